@@ -1,0 +1,117 @@
+/*
+ * polymer_fock.h -- C ABI of libpolymer_fock.so, the B200 direct J/K (Fock) build.
+ *
+ * Drop-in for SUBROUTINE FOURINDEX_ERI (src/pfourindexdirect.f90:1-814 of the
+ * polymer code), which has no dummy arguments and communicates through Fortran
+ * module globals.  pfe_args carries exactly the module state that subroutine
+ * reads (src/pmodules.f90: BASISSET 74-93, INTEGRAL 111-160, STRUCTURE 35-45,
+ * CONTROL DOPTN(12)/IOPTN(9), CONSTANTS MYID/NUMPROCS, FMT IGAMMA) and the two
+ * outputs it overwrites, C_C and X_C (src/pmodules.f90:114-115).
+ *
+ * Every array is Fortran column-major with the reference's bounds; pointers are
+ * borrowed for the duration of the call and never freed by the library.  All
+ * entry points return 0 on success and a negative PFE_E* code on failure;
+ * pfe_last_error() returns the message (the Fortran shim maps a non-zero code
+ * to PABORT, src/pmain.f90:75-103).
+ */
+#ifndef POLYMER_FOCK_H
+#define POLYMER_FOCK_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFE_OK 0
+#define PFE_EINVAL (-1)      /* malformed arguments (sizes, shell map, cutoffs) */
+#define PFE_ECUDA (-2)       /* a CUDA runtime / cuBLAS call failed */
+#define PFE_EUNSUPPORTED (-3)/* valid input outside what the kernels implement */
+#define PFE_ERANGE (-4)      /* Boys argument/order outside the IGAMMA table (reference: PABORT 'FMT CANNOT BE EVALUATED') */
+#define PFE_ENOMEM (-5)      /* device allocation failed */
+#define PFE_ETIMEOUT (-6)    /* a bounded device wait gave up */
+#define PFE_ENAN (-7)        /* non-finite density on input */
+
+#define PFE_PREC_FP64 0      /* every quartet in FP64 (parity path) */
+#define PFE_PREC_MIXED 1     /* quartets with Schwarz*|P|max below mixed_cutoff recur in FP32 */
+
+typedef struct pfe_args {
+  int32_t npgs, ncgs, npshell;       /* NPGS, NCGS, NPSHELL (module BASISSET)            */
+  int32_t lmax;                      /* BASIS_LMAX (3): P_SHELL is (npshell,0:lmax+1,...) */
+  const int32_t *p_shell;            /* P_SHELL(npshell,0:lmax+1,0:lmax+1,0:lmax+1), 1-based, -1 = none */
+  const int32_t *p_shell_ang;        /* P_SHELL_ANG(npshell)                              */
+  const double *pgsx, *pgsy, *pgsz;  /* PGSX/Y/Z(npgs), bohr                              */
+  const double *zt;                  /* ZT(npgs) exponents                                */
+  const double *cc;                  /* CC(ncgs,npgs)                                     */
+  const double *c2h;                 /* C2H(ncgs,ncgs,-(cel2x+cel1x):cel2x+cel1x); may be NULL if helix==0 */
+  const double *s_p;                 /* S_P(npgs,npgs,-cel1x:cel1x,-cel1y:cel1y,-cel1z:cel1z) */
+  const double *p_p;                 /* P_P, same layout as S_P                           */
+  const double *p_p_helix;           /* P_P_HELIX(npgs,npgs,-cel2x:cel2x,-(cel2x+cel1x):cel2x+cel1x); NULL if helix==0 */
+  const double *igamma;              /* IGAMMA(0:1700,0:27) (module FMT)                  */
+  int32_t cel1[3], cel2[3];          /* CEL1X/Y/Z, CEL2X/Y/Z                              */
+  int32_t reduced_cel1[3];           /* REDUCED_CEL1X/Y/Z (src/ponee.f90:359-409)         */
+  double period[3];                  /* PERIODX/Y/Z, bohr                                 */
+  double helix;                      /* HELIX, radians                                    */
+  double inttol;                     /* DOPTN(12) (INTTOL)                                */
+  int32_t print_level;               /* IOPTN(9) (PRINT); >=2 only affects the caller's dump */
+  int32_t myid, numprocs;            /* MPI rank and size: this call computes rank myid's share;
+                                        the caller sums C_C/X_C over ranks (MPI_ALLREDUCE)   */
+  int32_t precision_mode;            /* PFE_PREC_FP64 or PFE_PREC_MIXED                   */
+  double mixed_cutoff;               /* FP32 threshold on Schwarz(ij)*Schwarz(kl)*max|P|    */
+} pfe_args;
+
+/*
+ * Replaces FOURINDEX_ERI (src/pfourindexdirect.f90:1-814), called each SCF
+ * iteration from src/pselfconsistentfield.f90:42.  Host pointers in and out:
+ * c_c and x_c are C_C/X_C(ncgs,ncgs,-cel1x:cel1x,-cel1y:cel1y,-cel1z:cel1z),
+ * fully overwritten.  Static inputs (basis, S_P, IGAMMA, C2H, cutoffs) are
+ * cached on the device under a hash of their contents, so only P_P/P_P_HELIX
+ * are uploaded when they alone change between calls.
+ */
+int32_t pfe_fourindex_eri(const pfe_args *a, double *c_c, double *x_c);
+
+/* Message of the most recent failure in this thread (NUL-terminated). Returns its length. */
+int32_t pfe_last_error(char *buf, int32_t len);
+
+/* ---- device-resident interface (no host round trip per SCF iteration) ---- */
+
+typedef struct pfe_context pfe_context;
+
+/* Create a context on CUDA device `device`; *out receives it. Builds nothing yet. */
+int32_t pfe_context_create(int32_t device, pfe_context **out);
+int32_t pfe_context_destroy(pfe_context *ctx);
+
+/*
+ * Upload static inputs and build the device pair lists / Schwarz bounds
+ * (src/pfourindexdirect.f90:260-462 hoisted out of the SCF loop).  Only the
+ * p_p / p_p_helix members of `a` are ignored.
+ */
+int32_t pfe_context_setup(pfe_context *ctx, const pfe_args *a);
+
+/*
+ * One Fock build with device pointers: d_p_p (and d_p_p_helix when helix != 0)
+ * laid out as in pfe_args; d_c_c, d_x_c receive C_C/X_C.  `stream` is a
+ * cudaStream_t (NULL = legacy default).  Asynchronous: returns after enqueueing.
+ */
+int32_t pfe_context_fock(pfe_context *ctx, const double *d_p_p, const double *d_p_p_helix,
+                         double *d_c_c, double *d_x_c, void *stream);
+
+/* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */
+typedef struct pfe_census {
+  double quartets;          /* screened primitive-shell quartets computed per build   */
+  double quartets_ref;      /* the same work counted the reference's way (no symmetry) */
+  double flops;             /* FP64/FP32 recursion + digestion flops per build        */
+  double quartets_fp32;     /* quartets routed to FP32 recursion (mixed mode)          */
+  int64_t pairs;            /* significant primitive-shell pairs kept                 */
+  int32_t kernel_launches;  /* kernels launched by one pfe_context_fock call          */
+} pfe_census;
+int32_t pfe_context_census(pfe_context *ctx, pfe_census *out);
+
+/* Library version string. */
+const char *pfe_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLYMER_FOCK_H */

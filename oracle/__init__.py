@@ -1,0 +1,130 @@
+"""CPU oracle: the checker for the CUDA Fock build.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package.  It wraps oracle/oracle.c, a plain-C restatement of the
+reference's FOURINDEX_ERI, OVERLAP_KINETIC, NUCLEAR_ATTRACTION and
+FMT_PRELIMINARY (see that file's header for the file:line map), through the
+same pfe_args C-ABI block the product takes.
+
+Pinned against the reference's recorded outputs in tests/test_oracle_golden.py
+(SCF energies and components of data/H2O_CCSD_ccpVDZ_out, data/BH_MBGF_out,
+data/FH_finiteT_MBPT_*_out, and the helical-polyethylene overlap/lattice
+numbers of data/Polyethylene_B3LYP_631G_out).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, '_build', 'liboracle.so')
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class OneeArgs(ctypes.Structure):
+    _fields_ = [('npgs', ctypes.c_int32), ('npshell', ctypes.c_int32), ('natom', ctypes.c_int32),
+                ('p_shell', _ip), ('p_shell_ang', _ip), ('pgs_atom', _ip),
+                ('pgsx', _dp), ('pgsy', _dp), ('pgsz', _dp), ('zt', _dp),
+                ('iatom', _ip), ('atomx', _dp), ('atomy', _dp), ('atomz', _dp),
+                ('cel1', ctypes.c_int32 * 3), ('cel2', ctypes.c_int32 * 3),
+                ('period', ctypes.c_double * 3), ('helix', ctypes.c_double),
+                ('igamma', _dp)]
+
+
+def build():
+    """Compile oracle.c with gcc (make) into oracle/_build/liboracle.so."""
+    subprocess.run(['make', '-s', '-C', HERE], check=True)
+
+
+_L = None
+
+
+def lib():
+    global _L
+    if _L is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, 'oracle.c')):
+            build()
+        from polymer_b200.capi import PfeArgs
+        L = ctypes.CDLL(LIB)
+        L.oracle_fourindex_eri.argtypes = [ctypes.POINTER(PfeArgs), _dp, _dp]
+        L.oracle_fourindex_eri.restype = ctypes.c_int32
+        L.oracle_fmt_table.argtypes = [_dp]
+        L.oracle_overlap_kinetic.argtypes = [ctypes.POINTER(OneeArgs), _dp, _dp]
+        L.oracle_overlap_kinetic.restype = ctypes.c_int32
+        L.oracle_nuclear_attraction.argtypes = [ctypes.POINTER(OneeArgs), _dp]
+        L.oracle_nuclear_attraction.restype = ctypes.c_int32
+        _L = L
+    return _L
+
+
+def fmt_table() -> np.ndarray:
+    out = np.zeros((1701, 28), order='F')
+    lib().oracle_fmt_table(out.ctypes.data_as(_dp))
+    return out
+
+
+def onee(sysm):
+    """(S_P, T_P, N_P) cell-major, from the oracle's OVERLAP_KINETIC / NUCLEAR_ATTRACTION."""
+    from polymer_b200.system import from_fortran
+    b, d = sysm.basis, sysm.deck
+    keep = dict(p_shell=np.asfortranarray(b.p_shell.astype(np.int32)),
+                ang=b.p_shell_ang.astype(np.int32), atom=b.pgs_atom.astype(np.int32),
+                x=np.ascontiguousarray(b.pgs[:, 0]), y=np.ascontiguousarray(b.pgs[:, 1]),
+                z=np.ascontiguousarray(b.pgs[:, 2]), zt=np.ascontiguousarray(b.zt),
+                iatom=np.array(d.atoms, dtype=np.int32),
+                ax=np.array([c[0] for c in d.coords]), ay=np.array([c[1] for c in d.coords]),
+                az=np.array([c[2] for c in d.coords]), ig=np.asfortranarray(sysm.igamma))
+    a = OneeArgs()
+    a.npgs, a.npshell, a.natom = b.npgs, b.npshell, d.natom
+    a.p_shell = keep['p_shell'].ctypes.data_as(_ip)
+    a.p_shell_ang = keep['ang'].ctypes.data_as(_ip)
+    a.pgs_atom = keep['atom'].ctypes.data_as(_ip)
+    a.pgsx, a.pgsy, a.pgsz = (keep[k].ctypes.data_as(_dp) for k in ('x', 'y', 'z'))
+    a.zt = keep['zt'].ctypes.data_as(_dp)
+    a.iatom = keep['iatom'].ctypes.data_as(_ip)
+    a.atomx, a.atomy, a.atomz = (keep[k].ctypes.data_as(_dp) for k in ('ax', 'ay', 'az'))
+    for k in range(3):
+        a.cel1[k], a.cel2[k], a.period[k] = d.cel1[k], d.cel2[k], d.period[k]
+    a.helix = d.helix
+    a.igamma = keep['ig'].ctypes.data_as(_dp)
+    nc = sysm.ncell1
+    s = np.zeros(b.npgs * b.npgs * nc)
+    t = np.zeros_like(s)
+    n = np.zeros_like(s)
+    L = lib()
+    assert L.oracle_overlap_kinetic(ctypes.byref(a), s.ctypes.data_as(_dp), t.ctypes.data_as(_dp)) == 0
+    assert L.oracle_nuclear_attraction(ctypes.byref(a), n.ctypes.data_as(_dp)) == 0
+    return (from_fortran(s, (nc,), b.npgs).copy(), from_fortran(t, (nc,), b.npgs).copy(),
+            from_fortran(n, (nc,), b.npgs).copy())
+
+
+def fourindex_eri(sysm, p_p: np.ndarray, p_p_helix=None, **kw):
+    """(C_C, X_C) cell-major for cell-major P_P (and P_P_HELIX when helical)."""
+    from polymer_b200.system import from_fortran
+    b = sysm.basis
+    a, keep = sysm.pfe_args(p_p, p_p_helix, **kw)
+    nc = sysm.ncell1
+    c = np.zeros(b.ncgs * b.ncgs * nc)
+    x = np.zeros_like(c)
+    rc = lib().oracle_fourindex_eri(ctypes.byref(a), c.ctypes.data_as(_dp), x.ctypes.data_as(_dp))
+    if rc != 0:
+        raise RuntimeError('oracle_fourindex_eri failed with %d' % rc)
+    return from_fortran(c, (nc,), b.ncgs).copy(), from_fortran(x, (nc,), b.ncgs).copy()
+
+
+def fock_builder(sysm):
+    """A FockBuilder for polymer_b200.scf.run_scf backed by the oracle (CPU)."""
+    import torch
+
+    def f(p_p, p_ph):
+        pp = p_p.detach().cpu().numpy()
+        ph = p_ph.detach().cpu().numpy() if p_ph is not None else None
+        c, x = fourindex_eri(sysm, pp, ph)
+        return (torch.tensor(c, dtype=torch.float64, device=p_p.device),
+                torch.tensor(x, dtype=torch.float64, device=p_p.device))
+    return f

@@ -1,0 +1,119 @@
+"""ctypes mirror of include/polymer_fock.h and the loader of libpolymer_fock.so.
+
+The library is built in-tree (``polymer_b200/_build/libpolymer_fock.so``) by
+``polymer_b200.build``.  There is no fallback: if the shared object is missing
+or fails to load, :func:`lib` raises, so a Fock build never silently runs
+anywhere but the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, '_build', 'libpolymer_fock.so')
+
+PFE_OK = 0
+PFE_PREC_FP64 = 0
+PFE_PREC_MIXED = 1
+_ERRNAMES = {-1: 'PFE_EINVAL', -2: 'PFE_ECUDA', -3: 'PFE_EUNSUPPORTED', -4: 'PFE_ERANGE',
+             -5: 'PFE_ENOMEM', -6: 'PFE_ETIMEOUT', -7: 'PFE_ENAN'}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class PfeArgs(ctypes.Structure):
+    _fields_ = [
+        ('npgs', ctypes.c_int32), ('ncgs', ctypes.c_int32), ('npshell', ctypes.c_int32),
+        ('lmax', ctypes.c_int32),
+        ('p_shell', _ip), ('p_shell_ang', _ip),
+        ('pgsx', _dp), ('pgsy', _dp), ('pgsz', _dp), ('zt', _dp),
+        ('cc', _dp), ('c2h', _dp), ('s_p', _dp), ('p_p', _dp), ('p_p_helix', _dp),
+        ('igamma', _dp),
+        ('cel1', ctypes.c_int32 * 3), ('cel2', ctypes.c_int32 * 3),
+        ('reduced_cel1', ctypes.c_int32 * 3),
+        ('period', ctypes.c_double * 3), ('helix', ctypes.c_double),
+        ('inttol', ctypes.c_double),
+        ('print_level', ctypes.c_int32), ('myid', ctypes.c_int32), ('numprocs', ctypes.c_int32),
+        ('precision_mode', ctypes.c_int32), ('mixed_cutoff', ctypes.c_double),
+    ]
+
+
+class PfeCensus(ctypes.Structure):
+    _fields_ = [('quartets', ctypes.c_double), ('quartets_ref', ctypes.c_double),
+                ('flops', ctypes.c_double), ('quartets_fp32', ctypes.c_double),
+                ('pairs', ctypes.c_int64), ('kernel_launches', ctypes.c_int32)]
+
+
+class FockError(RuntimeError):
+    """A non-zero status from the library (the reference would PABORT)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__('%s (%d): %s' % (_ERRNAMES.get(code, 'PFE_E?'), code, msg))
+        self.code = code
+
+
+def dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return ctypes.cast(None, _dp)
+    assert a.dtype == np.float64 and a.flags['F_CONTIGUOUS'] or a.flags['C_CONTIGUOUS']
+    return a.ctypes.data_as(_dp)
+
+
+def iptr(a: Optional[np.ndarray]):
+    if a is None:
+        return ctypes.cast(None, _ip)
+    assert a.dtype == np.int32
+    return a.ctypes.data_as(_ip)
+
+
+_LIB = None
+
+
+def lib(path: str = LIB_PATH):
+    """Load libpolymer_fock.so; raises if it is absent (no CPU fallback exists)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError('libpolymer_fock.so not built at %s: run python -c "import polymer_b200.build as b; b.build()"' % path)
+    L = ctypes.CDLL(path)
+    L.pfe_fourindex_eri.argtypes = [ctypes.POINTER(PfeArgs), _dp, _dp]
+    L.pfe_fourindex_eri.restype = ctypes.c_int32
+    L.pfe_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int32]
+    L.pfe_last_error.restype = ctypes.c_int32
+    L.pfe_context_create.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+    L.pfe_context_create.restype = ctypes.c_int32
+    L.pfe_context_destroy.argtypes = [ctypes.c_void_p]
+    L.pfe_context_destroy.restype = ctypes.c_int32
+    L.pfe_context_setup.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeArgs)]
+    L.pfe_context_setup.restype = ctypes.c_int32
+    L.pfe_context_fock.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.pfe_context_fock.restype = ctypes.c_int32
+    L.pfe_context_census.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeCensus)]
+    L.pfe_context_census.restype = ctypes.c_int32
+    L.pfe_version.argtypes = []
+    L.pfe_version.restype = ctypes.c_char_p
+    _LIB = L
+    return L
+
+
+def last_error(L) -> str:
+    buf = ctypes.create_string_buffer(1024)
+    L.pfe_last_error(buf, 1024)
+    return buf.value.decode(errors='replace')
+
+
+def check(L, code: int) -> None:
+    if code != PFE_OK:
+        raise FockError(code, last_error(L))
+
+
+# Exported symbols declared in include/polymer_fock.h (checked by the CPU tests).
+EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_context_destroy',
+           'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_version']
