@@ -107,6 +107,25 @@ typedef struct pfe_census {
 } pfe_census;
 int32_t pfe_context_census(pfe_context *ctx, pfe_census *out);
 
+/* ---- caller-side set-up integrals (outside FOURINDEX_ERI) ----
+ * The Fortran caller computes these before the SCF (src/psinglepoint.f90:184,212);
+ * they are provided on the device so a host driver needs no CPU integral code. */
+typedef struct pfe_onee_args {
+  int32_t npgs, npshell, natom;
+  const int32_t *p_shell, *p_shell_ang, *pgs_atom; /* as in pfe_args; PGS_ATOM(npgs) 1-based */
+  const double *pgsx, *pgsy, *pgsz, *zt;
+  const int32_t *iatom;                           /* IATOM(natom) nuclear charges          */
+  const double *atomx, *atomy, *atomz;            /* ATOMX/Y/Z(natom), bohr                 */
+  int32_t cel1[3], cel2[3];
+  double period[3], helix;
+  const double *igamma;                           /* IGAMMA(0:1700,0:27)                    */
+} pfe_onee_args;
+
+/* OVERLAP_KINETIC(0) (src/ponee.f90:1-160): S_P and T_P(npgs,npgs,cells1), host out. */
+int32_t pfe_overlap_kinetic(const pfe_onee_args *a, double *s_p, double *t_p);
+/* NUCLEAR_ATTRACTION(0) (src/ponee.f90:418-603): N_P(npgs,npgs,cells1), host out. */
+int32_t pfe_nuclear_attraction(const pfe_onee_args *a, double *n_p);
+
 /* Library version string. */
 const char *pfe_version(void);
 

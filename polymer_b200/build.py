@@ -1,0 +1,71 @@
+"""Build libpolymer_fock.so in-tree for sm_100a with nvcc.
+
+Sources: polymer_b200/csrc/*.cu; the class-specialised ERI header is
+regenerated from gen_eri.py first.  Output: polymer_b200/_build/.
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, 'csrc')
+OUT = os.path.join(HERE, '_build')
+LIB = os.path.join(OUT, 'libpolymer_fock.so')
+SOURCES = ['pfe_api.cu', 'pfe_eri.cu', 'pfe_lattice.cu', 'pfe_onee.cu']
+NVCC = os.environ.get('NVCC', 'nvcc')
+ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
+FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550']
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError('command failed: %s\n%s\n%s' % (' '.join(cmd), r.stdout[-4000:], r.stderr[-8000:]))
+    return r.stdout + r.stderr
+
+
+def generate():
+    gen = os.path.join(CSRC, 'gen_eri.py')
+    out = os.path.join(CSRC, 'generated', 'eri_classes.cuh')
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    if (not os.path.exists(out)) or os.path.getmtime(out) < os.path.getmtime(gen):
+        _run([sys.executable, gen, out, '2'])
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile every CUDA source and link the shared library; returns its path."""
+    generate()
+    os.makedirs(OUT, exist_ok=True)
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cu', '.cuh'))]
+    deps += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
+             os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h')]
+    newest = max(os.path.getmtime(d) for d in deps if os.path.exists(d))
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not ptxas_info:
+        return LIB
+
+    def compile_one(src):
+        obj = os.path.join(OUT, src.replace('.cu', '.o'))
+        cmd = [NVCC] + ARCH + FLAGS + (['-Xptxas', '-v'] if ptxas_info else []) + \
+            ['-c', os.path.join(CSRC, src), '-o', obj]
+        log = _run(cmd)
+        if ptxas_info:
+            with open(os.path.join(OUT, src.replace('.cu', '.ptxas.txt')), 'w') as fh:
+                fh.write(log)
+        return obj
+
+    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    with cf.ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+        objs = list(ex.map(compile_one, srcs))
+    tmp = LIB + '.tmp'
+    _run([NVCC] + ARCH + ['-shared', '-o', tmp] + objs + ['-lcublas'])
+    os.replace(tmp, LIB)
+    if verbose:
+        print('built', LIB)
+    return LIB
+
+
+if __name__ == '__main__':
+    print(build(verbose=True, ptxas_info='--ptxas' in sys.argv))

@@ -43,6 +43,16 @@ class PfeArgs(ctypes.Structure):
     ]
 
 
+class PfeOneeArgs(ctypes.Structure):
+    _fields_ = [('npgs', ctypes.c_int32), ('npshell', ctypes.c_int32), ('natom', ctypes.c_int32),
+                ('p_shell', _ip), ('p_shell_ang', _ip), ('pgs_atom', _ip),
+                ('pgsx', _dp), ('pgsy', _dp), ('pgsz', _dp), ('zt', _dp),
+                ('iatom', _ip), ('atomx', _dp), ('atomy', _dp), ('atomz', _dp),
+                ('cel1', ctypes.c_int32 * 3), ('cel2', ctypes.c_int32 * 3),
+                ('period', ctypes.c_double * 3), ('helix', ctypes.c_double),
+                ('igamma', _dp)]
+
+
 class PfeCensus(ctypes.Structure):
     _fields_ = [('quartets', ctypes.c_double), ('quartets_ref', ctypes.c_double),
                 ('flops', ctypes.c_double), ('quartets_fp32', ctypes.c_double),
@@ -97,6 +107,10 @@ def lib(path: str = LIB_PATH):
     L.pfe_context_fock.restype = ctypes.c_int32
     L.pfe_context_census.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeCensus)]
     L.pfe_context_census.restype = ctypes.c_int32
+    L.pfe_overlap_kinetic.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp, _dp]
+    L.pfe_overlap_kinetic.restype = ctypes.c_int32
+    L.pfe_nuclear_attraction.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp]
+    L.pfe_nuclear_attraction.restype = ctypes.c_int32
     L.pfe_version.argtypes = []
     L.pfe_version.restype = ctypes.c_char_p
     _LIB = L
@@ -116,4 +130,5 @@ def check(L, code: int) -> None:
 
 # Exported symbols declared in include/polymer_fock.h (checked by the CPU tests).
 EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_context_destroy',
-           'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_version']
+           'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_overlap_kinetic',
+           'pfe_nuclear_attraction', 'pfe_version']

@@ -1,0 +1,436 @@
+// C ABI of libpolymer_fock (include/polymer_fock.h): argument validation, the
+// static-input cache, host <-> device staging and context lifetime.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pfe_common.cuh"
+#include "pfe_context.cuh"
+#include "generated/eri_classes.cuh"
+
+namespace pfe {
+
+// ------------------------------------------------------------------ helpers
+
+__global__ void k_gather_u8(const unsigned char* __restrict__ src, const int* __restrict__ perm,
+                            unsigned char* __restrict__ dst, long long n) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n) dst[t] = src[perm[t]];
+}
+
+void thrust_gather_u8(const unsigned char* src, const int* perm, unsigned char* dst, long long n, cudaStream_t s) {
+  k_gather_u8<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, perm, dst, n);
+}
+
+int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n) {
+  for (int k = 0; k < 3; ++k) {
+    PFE_CUDA(ctx->alloc((void**)&pa->P[k], sizeof(double) * n));
+    PFE_CUDA(ctx->alloc((void**)&pa->PA[k], sizeof(double) * n));
+    PFE_CUDA(ctx->alloc((void**)&pa->AB[k], sizeof(double) * n));
+  }
+  PFE_CUDA(ctx->alloc((void**)&pa->zeta, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->S, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->schwarz, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->si, sizeof(int) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->sj, sizeof(int) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->cls, n));
+  PFE_CUDA(ctx->alloc((void**)&pa->key, sizeof(unsigned long long) * n));
+  return PFE_OK;
+}
+
+void free_pairs(pfe_context* ctx, PairArrays* pa) {
+  for (int k = 0; k < 3; ++k) {
+    ctx->free_now(pa->P[k]);
+    ctx->free_now(pa->PA[k]);
+    ctx->free_now(pa->AB[k]);
+  }
+  ctx->free_now(pa->zeta);
+  ctx->free_now(pa->S);
+  ctx->free_now(pa->schwarz);
+  ctx->free_now(pa->si);
+  ctx->free_now(pa->sj);
+  ctx->free_now(pa->cls);
+  ctx->free_now(pa->key);
+  *pa = PairArrays{};
+}
+
+// Per primitive-shell-quartet flops of class (bra cb, ket ck) counted by the
+// roofline: generated recursion + Boys (table Taylor, 13 per order) + quartet
+// geometry (~40) + digestion (6 FMAs per integral = 12 flops).
+double class_flops(int cb, int ck) {
+  static const int L[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  const int la = L[cb][0], lb = L[cb][1], lc = L[ck][0], ld = L[ck][1];
+  const double ni = (double)(ncum(la) * ncum(lb) * ncum(lc) * ncum(ld));
+  const int lt = la + lb + lc + ld;
+  return eri_recursion_flops(la, lb, lc, ld) + 13.0 * (lt + 1) + 40.0 + 12.0 * ni;
+}
+
+static uint64_t fnv(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = (const unsigned char*)p;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ull;
+  }
+  return h;
+}
+
+static inline size_t psh_index(int npshell, int s, int i1, int i2, int i3) {
+  return (size_t)s + (size_t)npshell * (i1 + NPOW * (i2 + NPOW * i3));
+}
+
+// Validate the argument block and derive the shell table on the host.
+struct HostShells {
+  std::vector<double> x, y, z, zeta;
+  std::vector<int> L, prim, head;
+  int lmax = 0;
+};
+
+static int build_host_shells(const pfe_args* a, HostShells* hs) {
+  if (!a) { set_error("null argument block"); return PFE_EINVAL; }
+  if (a->npgs <= 0 || a->ncgs <= 0 || a->npshell <= 0) { set_error("npgs, ncgs and npshell must be positive"); return PFE_EINVAL; }
+  if (a->lmax != 3) { set_error("lmax must be BASIS_LMAX = 3 (P_SHELL layout)"); return PFE_EINVAL; }
+  if (!a->p_shell || !a->p_shell_ang || !a->pgsx || !a->pgsy || !a->pgsz || !a->zt || !a->cc || !a->s_p || !a->igamma) {
+    set_error("a required array pointer is null");
+    return PFE_EINVAL;
+  }
+  for (int k = 0; k < 3; ++k) {
+    if (a->cel1[k] < 0 || a->cel2[k] < 0 || a->reduced_cel1[k] < 0 || a->reduced_cel1[k] > a->cel1[k]) {
+      set_error("invalid CUTOFF parameters");
+      return PFE_EINVAL;
+    }
+  }
+  if (a->numprocs < 1 || a->myid < 0 || a->myid >= a->numprocs) { set_error("invalid myid/numprocs"); return PFE_EINVAL; }
+  if (a->helix != 0.0 && (a->cel1[1] | a->cel1[2] | a->cel2[1] | a->cel2[2])) {
+    set_error("HELICAL SYMMETRY FOR 1D CRYSTAL ONLY");
+    return PFE_EINVAL;
+  }
+  if (a->helix != 0.0 && (!a->c2h)) { set_error("helix != 0 needs C2H"); return PFE_EINVAL; }
+  const int n = a->npshell;
+  hs->x.resize(n); hs->y.resize(n); hs->z.resize(n); hs->zeta.resize(n);
+  hs->L.resize(n); hs->prim.assign((size_t)n * MAXCOMP, -1); hs->head.resize(n);
+  for (int s = 0; s < n; ++s) {
+    const int L = a->p_shell_ang[s];
+    if (L < 0 || L > 3) { set_error("P_SHELL_ANG out of range"); return PFE_EINVAL; }
+    if (L > LMAX_SUPPORTED) {
+      set_error("f shells (P_SHELL_ANG = 3) are not implemented by the CUDA kernels");
+      return PFE_EUNSUPPORTED;
+    }
+    hs->lmax = std::max(hs->lmax, L);
+    int c = 0;
+    for (int i1 = 0; i1 <= L; ++i1)
+      for (int i2 = 0; i2 <= L - i1; ++i2)
+        for (int i3 = 0; i3 <= L - i1 - i2; ++i3) {
+          const int p = a->p_shell[psh_index(n, s, i1, i2, i3)];
+          if (p < 1 || p > a->npgs) {
+            set_error("P_SHELL refers to a missing primitive: the shell is not cumulative");
+            return PFE_EINVAL;
+          }
+          hs->prim[(size_t)s * MAXCOMP + c++] = p - 1;
+        }
+    const int h = hs->prim[(size_t)s * MAXCOMP];
+    hs->head[s] = h;
+    hs->x[s] = a->pgsx[h];
+    hs->y[s] = a->pgsy[h];
+    hs->z[s] = a->pgsz[h];
+    hs->zeta[s] = a->zt[h];
+    hs->L[s] = L;
+    if (!(a->zt[h] > 0.0) || !std::isfinite(a->zt[h])) { set_error("non-positive exponent"); return PFE_EINVAL; }
+  }
+  return PFE_OK;
+}
+
+static uint64_t static_key(const pfe_args* a, const HostShells& hs) {
+  uint64_t h = 1469598103934665603ull;
+  h = fnv(h, &a->npgs, sizeof(int) * 4);
+  h = fnv(h, hs.x.data(), sizeof(double) * hs.x.size());
+  h = fnv(h, hs.y.data(), sizeof(double) * hs.y.size());
+  h = fnv(h, hs.z.data(), sizeof(double) * hs.z.size());
+  h = fnv(h, hs.zeta.data(), sizeof(double) * hs.zeta.size());
+  h = fnv(h, hs.prim.data(), sizeof(int) * hs.prim.size());
+  h = fnv(h, a->cc, sizeof(double) * (size_t)a->ncgs * a->npgs);
+  h = fnv(h, a->igamma, sizeof(double) * 64);
+  h = fnv(h, a->cel1, sizeof(int) * 9);
+  h = fnv(h, a->period, sizeof(double) * 5);
+  h = fnv(h, &a->myid, sizeof(int) * 3);
+  h = fnv(h, &a->mixed_cutoff, sizeof(double));
+  // the s-s overlaps of the shell heads are the only part of S_P the kernels read
+  const int n = a->npshell;
+  const int n1x = 2 * a->cel1[0] + 1, n1y = 2 * a->cel1[1] + 1, n1z = 2 * a->cel1[2] + 1;
+  const size_t pp = (size_t)a->npgs * a->npgs;
+  for (int c = 0; c < n1x * n1y * n1z; ++c)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const double v = a->s_p[(size_t)hs.head[i] + (size_t)a->npgs * hs.head[j] + pp * c];
+        h = fnv(h, &v, sizeof v);
+      }
+  if (a->helix != 0.0 && a->c2h) {
+    const int nq = 2 * (a->cel2[0] + a->cel1[0]) + 1;
+    h = fnv(h, a->c2h, sizeof(double) * (size_t)a->ncgs * a->ncgs * nq);
+  }
+  return h;
+}
+
+static void reset_context(pfe_context* ctx) {
+  if (ctx->lattice) lattice_release(ctx);
+  ctx->release_all();
+  ctx->shells = DevShells{};
+  ctx->pairs = PairArrays{};
+  ctx->d_sss = ctx->d_boys = ctx->d_maxc = ctx->d_cc = ctx->d_c2h = nullptr;
+  ctx->d_jp = ctx->d_kp = ctx->d_w1 = ctx->d_w2 = nullptr;
+  ctx->d_pp = ctx->d_pph = ctx->d_out_c = ctx->d_out_x = nullptr;
+  ctx->pp_bytes = ctx->pph_bytes = ctx->out_bytes = 0;
+  ctx->nlaunch = 0;
+  ctx->ready = false;
+}
+
+static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs, uint64_t key) {
+  int rc;
+  PFE_CUDA(cudaSetDevice(ctx->device));
+  if ((rc = upload_constants(ctx->device)) != PFE_OK) return rc;
+  reset_context(ctx);
+  ctx->npgs = a->npgs;
+  ctx->ncgs = a->ncgs;
+  ctx->npshell = a->npshell;
+  for (int k = 0; k < 3; ++k) {
+    ctx->cel1[k] = a->cel1[k];
+    ctx->cel2[k] = a->cel2[k];
+    ctx->rc1[k] = a->reduced_cel1[k];
+    ctx->period[k] = a->period[k];
+  }
+  ctx->ncell1 = (2 * a->cel1[0] + 1) * (2 * a->cel1[1] + 1) * (2 * a->cel1[2] + 1);
+  ctx->helix = a->helix;
+  ctx->inttol = a->inttol;
+  ctx->myid = a->myid;
+  ctx->numprocs = a->numprocs;
+  ctx->precision = a->precision_mode;
+  ctx->mixed_cutoff = a->mixed_cutoff;
+  ctx->molecular = (ctx->ncell1 == 1 && a->cel2[0] == 0 && a->cel2[1] == 0 && a->cel2[2] == 0 && a->helix == 0.0);
+  cudaStream_t s = ctx->stream;
+  const int n = a->npshell;
+  // shells
+  DevShells& sh = ctx->shells;
+  sh.n = n;
+  PFE_CUDA(ctx->alloc((void**)&sh.x, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&sh.y, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&sh.z, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&sh.zeta, sizeof(double) * n));
+  PFE_CUDA(ctx->alloc((void**)&sh.L, sizeof(int) * n));
+  PFE_CUDA(ctx->alloc((void**)&sh.prim, sizeof(int) * n * MAXCOMP));
+  PFE_CUDA(cudaMemcpyAsync(sh.x, hs.x.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaMemcpyAsync(sh.y, hs.y.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaMemcpyAsync(sh.z, hs.z.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaMemcpyAsync(sh.zeta, hs.zeta.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaMemcpyAsync(sh.L, hs.L.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaMemcpyAsync(sh.prim, hs.prim.data(), sizeof(int) * n * MAXCOMP, cudaMemcpyHostToDevice, s));
+  // s-s overlaps of the shell heads per cell, [cell][J][I]
+  {
+    std::vector<double> sss((size_t)n * n * ctx->ncell1);
+    const size_t pp = (size_t)a->npgs * a->npgs;
+    for (int c = 0; c < ctx->ncell1; ++c)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i)
+          sss[(size_t)i + (size_t)n * j + (size_t)n * n * c] = a->s_p[(size_t)hs.head[i] + (size_t)a->npgs * hs.head[j] + pp * c];
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_sss, sizeof(double) * sss.size()));
+    PFE_CUDA(cudaMemcpyAsync(ctx->d_sss, sss.data(), sizeof(double) * sss.size(), cudaMemcpyHostToDevice, s));
+    PFE_CUDA(cudaStreamSynchronize(s));
+  }
+  // Boys table, row-major [T][m]
+  {
+    std::vector<double> tab((size_t)NIG_T * NIG_M);
+    for (int t = 0; t < NIG_T; ++t)
+      for (int m = 0; m < NIG_M; ++m) tab[(size_t)t * NIG_M + m] = a->igamma[t + (size_t)NIG_T * m];
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_boys, sizeof(double) * tab.size()));
+    PFE_CUDA(cudaMemcpyAsync(ctx->d_boys, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, s));
+    PFE_CUDA(cudaStreamSynchronize(s));
+  }
+  // MAXC and CC
+  {
+    std::vector<double> maxc(a->npgs, 0.0);
+    for (int p = 0; p < a->npgs; ++p)
+      for (int r = 0; r < a->ncgs; ++r) maxc[p] = std::max(maxc[p], std::fabs(a->cc[r + (size_t)a->ncgs * p]));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_maxc, sizeof(double) * a->npgs));
+    PFE_CUDA(cudaMemcpy(ctx->d_maxc, maxc.data(), sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_cc, sizeof(double) * (size_t)a->ncgs * a->npgs));
+    PFE_CUDA(cudaMemcpy(ctx->d_cc, a->cc, sizeof(double) * (size_t)a->ncgs * a->npgs, cudaMemcpyHostToDevice));
+  }
+  if (a->helix != 0.0) {
+    const int nq = 2 * (a->cel2[0] + a->cel1[0]) + 1;
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_c2h, sizeof(double) * (size_t)a->ncgs * a->ncgs * nq));
+    PFE_CUDA(cudaMemcpy(ctx->d_c2h, a->c2h, sizeof(double) * (size_t)a->ncgs * a->ncgs * nq, cudaMemcpyHostToDevice));
+  }
+  // accumulators and GEMM scratch
+  const size_t pp = (size_t)a->npgs * a->npgs * ctx->ncell1;
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_jp, sizeof(double) * pp));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_kp, sizeof(double) * pp));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_w1, sizeof(double) * (size_t)a->ncgs * a->npgs * ctx->ncell1));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_w2, sizeof(double) * (size_t)a->ncgs * a->ncgs * ctx->ncell1));
+  rc = ctx->molecular ? molecular_setup(ctx, a) : lattice_setup(ctx, a);
+  if (rc != PFE_OK) return rc;
+  ctx->key = key;
+  ctx->ready = true;
+  return PFE_OK;
+}
+
+static int check_density(const double* p, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) {
+      set_error("non-finite density element in P_P");
+      return PFE_ENAN;
+    }
+  return PFE_OK;
+}
+
+}  // namespace pfe
+
+using namespace pfe;
+
+extern "C" {
+
+const char* pfe_version(void) { return "polymer_fock 0.1 (sm_100a, cumulative s/p/d shells)"; }
+
+int32_t pfe_last_error(char* buf, int32_t len) {
+  const char* m = last_error_cstr();
+  const int32_t n = (int32_t)strlen(m);
+  if (buf && len > 0) {
+    const int32_t k = n < len - 1 ? n : len - 1;
+    memcpy(buf, m, k);
+    buf[k] = 0;
+  }
+  return n;
+}
+
+int32_t pfe_context_create(int32_t device, pfe_context** out) {
+  if (!out) { set_error("null output handle"); return PFE_EINVAL; }
+  int ndev = 0;
+  PFE_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) { set_error("no such CUDA device"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(device));
+  pfe_context* ctx = new pfe_context();
+  ctx->device = device;
+  cudaDeviceProp prop;
+  PFE_CUDA(cudaGetDeviceProperties(&prop, device));
+  ctx->num_sms = prop.multiProcessorCount;
+  PFE_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) {
+    set_error("cublasCreate failed");
+    delete ctx;
+    return PFE_ECUDA;
+  }
+  *out = ctx;
+  return PFE_OK;
+}
+
+int32_t pfe_context_destroy(pfe_context* ctx) {
+  if (!ctx) return PFE_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  reset_context(ctx);
+  if (ctx->blas) cublasDestroy(ctx->blas);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return PFE_OK;
+}
+
+int32_t pfe_context_setup(pfe_context* ctx, const pfe_args* a) {
+  if (!ctx) { set_error("null context"); return PFE_EINVAL; }
+  HostShells hs;
+  int rc = build_host_shells(a, &hs);
+  if (rc != PFE_OK) return rc;
+  const uint64_t key = static_key(a, hs);
+  if (ctx->ready && ctx->key == key) return PFE_OK;
+  rc = setup_impl(ctx, a, hs, key);
+  if (rc != PFE_OK) ctx->ready = false;
+  return rc;
+}
+
+int32_t pfe_context_fock(pfe_context* ctx, const double* d_p_p, const double* d_p_p_helix, double* d_c_c, double* d_x_c,
+                         void* stream) {
+  if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
+  if (!d_p_p || !d_c_c || !d_x_c) { set_error("null device pointer"); return PFE_EINVAL; }
+  if (ctx->helix != 0.0 && !d_p_p_helix) { set_error("helix != 0 needs P_P_HELIX"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  return ctx->molecular ? molecular_fock(ctx, d_p_p, d_c_c, d_x_c, s)
+                        : lattice_fock(ctx, d_p_p, d_p_p_helix, d_c_c, d_x_c, s);
+}
+
+int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
+  if (!ctx || !out) { set_error("null argument"); return PFE_EINVAL; }
+  out->quartets = ctx->census_quartets;
+  out->quartets_ref = ctx->census_ref;
+  out->flops = ctx->census_flops;
+  out->quartets_fp32 = ctx->census_fp32;
+  out->pairs = ctx->npairs;
+  out->kernel_launches = ctx->nlaunch + (ctx->molecular ? 2 : 3);
+  return PFE_OK;
+}
+
+static std::mutex g_default_mu;
+static pfe_context* g_default[64] = {nullptr};
+
+int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
+  std::lock_guard<std::mutex> lock(g_default_mu);
+  if (!c_c || !x_c) { set_error("null output array"); return PFE_EINVAL; }
+  int dev = 0;
+  PFE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_error("device index out of range"); return PFE_EINVAL; }
+  if (!g_default[dev]) {
+    int rc = pfe_context_create(dev, &g_default[dev]);
+    if (rc != PFE_OK) return rc;
+  }
+  pfe_context* ctx = g_default[dev];
+  HostShells hs;
+  int rc = build_host_shells(a, &hs);
+  if (rc != PFE_OK) return rc;
+  if (!a->p_p) { set_error("P_P is null"); return PFE_EINVAL; }
+  const size_t ncell1 = (size_t)(2 * a->cel1[0] + 1) * (2 * a->cel1[1] + 1) * (2 * a->cel1[2] + 1);
+  const size_t npp = (size_t)a->npgs * a->npgs * ncell1;
+  if ((rc = check_density(a->p_p, npp)) != PFE_OK) return rc;
+  const uint64_t key = static_key(a, hs);
+  if (!(ctx->ready && ctx->key == key)) {
+    if ((rc = setup_impl(ctx, a, hs, key)) != PFE_OK) { ctx->ready = false; return rc; }
+  }
+  cudaStream_t s = ctx->stream;
+  const size_t out_bytes = sizeof(double) * (size_t)a->ncgs * a->ncgs * ncell1;
+  if (ctx->pp_bytes < npp * sizeof(double)) {
+    ctx->free_now(ctx->d_pp);
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_pp, npp * sizeof(double)));
+    ctx->pp_bytes = npp * sizeof(double);
+  }
+  if (ctx->out_bytes < out_bytes) {
+    ctx->free_now(ctx->d_out_c);
+    ctx->free_now(ctx->d_out_x);
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_out_c, out_bytes));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_out_x, out_bytes));
+    ctx->out_bytes = out_bytes;
+  }
+  PFE_CUDA(cudaMemcpyAsync(ctx->d_pp, a->p_p, npp * sizeof(double), cudaMemcpyHostToDevice, s));
+  const double* d_pph = nullptr;
+  if (a->helix != 0.0) {
+    if (!a->p_p_helix) { set_error("helix != 0 needs P_P_HELIX"); return PFE_EINVAL; }
+    const size_t nh = (size_t)a->npgs * a->npgs * (2 * a->cel2[0] + 1) * (2 * (a->cel2[0] + a->cel1[0]) + 1);
+    if ((rc = check_density(a->p_p_helix, nh)) != PFE_OK) return rc;
+    if (ctx->pph_bytes < nh * sizeof(double)) {
+      ctx->free_now(ctx->d_pph);
+      PFE_CUDA(ctx->alloc((void**)&ctx->d_pph, nh * sizeof(double)));
+      ctx->pph_bytes = nh * sizeof(double);
+    }
+    PFE_CUDA(cudaMemcpyAsync(ctx->d_pph, a->p_p_helix, nh * sizeof(double), cudaMemcpyHostToDevice, s));
+    d_pph = ctx->d_pph;
+  }
+  rc = ctx->molecular ? molecular_fock(ctx, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, s)
+                      : lattice_fock(ctx, ctx->d_pp, d_pph, ctx->d_out_c, ctx->d_out_x, s);
+  if (rc != PFE_OK) return rc;
+  PFE_CUDA(cudaMemcpyAsync(c_c, ctx->d_out_c, out_bytes, cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaMemcpyAsync(x_c, ctx->d_out_x, out_bytes, cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaStreamSynchronize(s));
+  return PFE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,81 @@
+// Shared device helpers of libpolymer_fock: constants, error plumbing, the
+// tabulated Boys function and the cumulative-shell component counts.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/polymer_fock.h"
+#include "generated/eri_classes.cuh"
+
+namespace pfe {
+
+// The reference's own constant (src/pmodules.f90:7), used wherever it enters
+// normalisation/prefactors so that integrals agree with it to the last digits.
+constexpr double REF_PI = 3.14159265358979;
+constexpr int LMAX_SUPPORTED = 2;   // cumulative s, sp, spd shells (what the workloads use)
+constexpr int NPOW = 5;             // P_SHELL power extent 0..BASIS_LMAX+1
+constexpr int MAXCOMP = 10;         // components of a cumulative d shell
+constexpr int NIG_T = 1701;         // IGAMMA rows (T = 0..85 step 0.05)
+constexpr int NIG_M = 28;           // IGAMMA orders 0..27
+
+__host__ __device__ constexpr int ncum(int L) { return (L + 1) * (L + 2) * (L + 3) / 6; }
+
+void set_error(const std::string& msg);
+
+#define PFE_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      ::pfe::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));             \
+      return (e_ == cudaErrorMemoryAllocation) ? PFE_ENOMEM : PFE_ECUDA;               \
+    }                                                                                    \
+  } while (0)
+
+// Switch points of the asymptotic Boys form, TF(0:21) (src/pmodules.f90:156-159).
+static __constant__ const double c_TF[22] = {33, 37, 41, 43, 46, 49, 51, 54, 56, 58, 61,
+                                             63, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84};
+
+// F_m(T)*pref for m = 0..L exactly as the reference evaluates it
+// (src/pfourindexdirect.f90:543-553): below TF(m) a 6-term Taylor series about
+// the nearest tabulated point of IGAMMA (row-major [T][m] here), above it the
+// asymptotic form.  The asymptotic power T^(-m-1/2) is formed as
+// rsqrt(T)*(1/T)^m instead of exp((-m-1/2) log T): same function, rounding
+// differs in the last bit.
+template <int L>
+__device__ __forceinline__ void boys_tab(double T, double pref, const double* __restrict__ tab,
+                                         double* __restrict__ F) {
+  if (T < c_TF[L]) {
+    const int ts = (int)floor(T * 20.0 + 0.5);  // NINT for T >= 0
+    const double h = 0.05 * (double)ts - T;
+    const double* g = tab + ts * NIG_M;
+    double gv[L + 7];
+#pragma unroll
+    for (int k = 0; k < L + 7; ++k) gv[k] = __ldg(g + k);
+#pragma unroll
+    for (int m = 0; m <= L; ++m) {
+      if (T < c_TF[m]) {
+        F[m] = ((((((gv[m + 6] * h * 0.166666666666667 + gv[m + 5]) * h * 0.2 + gv[m + 4]) * h * 0.25 +
+                   gv[m + 3]) * h * 0.333333333333333 + gv[m + 2]) * h * 0.5 + gv[m + 1]) * h + gv[m]) * pref;
+      } else {
+        // asymptotic prefactor F1(m) = (2m-1)!!/2^m * sqrt(PI)/2 (src/pfourindexdirect.f90:75-81)
+        double v = pref * PFE_F1_0 * rsqrt(T);
+        const double it = 1.0 / T;
+        for (int k = 1; k <= m; ++k) v *= it * (0.5 * (double)(2 * k - 1));
+        F[m] = v;
+      }
+    }
+  } else {
+    const double it = 1.0 / T;
+    double v = pref * PFE_F1_0 * rsqrt(T);
+    F[0] = v;
+#pragma unroll
+    for (int m = 1; m <= L; ++m) {
+      v *= it * (0.5 * (double)(2 * m - 1));
+      F[m] = v;
+    }
+  }
+}
+
+}  // namespace pfe

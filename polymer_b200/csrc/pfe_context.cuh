@@ -1,0 +1,156 @@
+// Device-side state of one Fock-build context (struct pfe_context of the C ABI).
+#pragma once
+
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "pfe_common.cuh"
+
+namespace pfe {
+
+// Primitive-shell table, struct of arrays (n shells).
+struct DevShells {
+  int n;
+  double *x, *y, *z, *zeta;
+  int* L;
+  int* prim;  // n * MAXCOMP, 0-based primitive of each cumulative component (-1 ghost/absent)
+};
+
+// Shell-pair records, struct of arrays; sorted by (class, Schwarz descending) after setup.
+struct PairArrays {
+  double* P[3];
+  double* PA[3];
+  double* AB[3];
+  double* zeta;
+  double* S;        // S_P of the two s components (the reference's OV / C1 factor)
+  double* schwarz;  // the reference's IJIJ/KLKL bound
+  int* si;
+  int* sj;
+  unsigned char* cls;
+  unsigned long long* key;
+};
+
+// One launch of the quartet kernel: a (bra class, ket class) pair and its chunks.
+struct ClassLaunch {
+  int cb, ck;
+  int nchunks_host;
+  int* d_nchunks;
+  int4* chunks;  // (bra pair, first ket, end ket, 0)
+  double quartets;
+  // interpreted classes: level-scheduled op table and its shared-memory size
+  bool big;
+  const unsigned short* ops;
+  const int* levels;
+  const unsigned short* out;
+  int nlevels, nout, nslots;
+  size_t smem;
+};
+
+struct QuartetLaunch {
+  PairArrays pairs;
+  const int* prim;
+  const double* boys;     // IGAMMA row-major [T][m]
+  const double* density;  // P_P (npgs x npgs, column-major)
+  double* jp;             // J' accumulator (primitive, column-major)
+  double* kp;             // K' accumulator
+  const int4* chunks;
+  const int* nchunks;
+  int npgs;
+  int myid, numprocs;
+};
+
+}  // namespace pfe
+
+// The opaque handle of the C ABI.
+struct pfe_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t blas = nullptr;
+  bool ready = false;
+  uint64_t key = 0;
+  bool molecular = true;
+  int npgs = 0, ncgs = 0, npshell = 0, ncell1 = 1;
+  int cel1[3] = {0, 0, 0}, cel2[3] = {0, 0, 0}, rc1[3] = {0, 0, 0};
+  double period[3] = {0, 0, 0};
+  double helix = 0.0;
+  double inttol = 0.0;
+  int myid = 0, numprocs = 1;
+  int precision = 0;
+  double mixed_cutoff = 0.0;
+
+  // device data
+  pfe::DevShells shells{};
+  double* d_sss = nullptr;   // S_P(head I, head J, cell) for shell heads, [cell][J][I]
+  double* d_boys = nullptr;
+  double* d_maxc = nullptr;  // max_i |CC(i, p)| per primitive
+  double* d_cc = nullptr;    // CC (ncgs x npgs, column-major)
+  double* d_c2h = nullptr;
+  double* d_jp = nullptr;
+  double* d_kp = nullptr;
+  double* d_w1 = nullptr;
+  double* d_w2 = nullptr;
+  pfe::PairArrays pairs{};
+  long long npairs = 0;
+  int class_off[8] = {0}, class_n[8] = {0};
+  pfe::ClassLaunch launches[64];
+  int nlaunch = 0;
+  double census_quartets = 0.0, census_flops = 0.0, census_ref = 0.0, census_fp32 = 0.0;
+
+  // host-path staging (pfe_fourindex_eri)
+  double* d_pp = nullptr;
+  double* d_pph = nullptr;
+  double* d_out_c = nullptr;
+  double* d_out_x = nullptr;
+  size_t pp_bytes = 0, pph_bytes = 0, out_bytes = 0;
+
+  // lattice path state lives in pfe_lattice.cu
+  void* lattice = nullptr;
+
+  std::vector<void*> owned;    // freed on reset/destroy
+  std::vector<void*> pending;  // scratch freed at the end of setup
+
+  cudaError_t alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e == cudaSuccess) owned.push_back(*p);
+    return e;
+  }
+  void free_now(void* p) {
+    if (!p) return;
+    for (size_t i = 0; i < owned.size(); ++i)
+      if (owned[i] == p) {
+        owned.erase(owned.begin() + i);
+        break;
+      }
+    cudaFree(p);
+  }
+  void free_later(void* p) { pending.push_back(p); }
+  void free_pending() {
+    for (void* p : pending) free_now(p);
+    pending.clear();
+  }
+  void release_all() {
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+    pending.clear();
+  }
+};
+
+namespace pfe {
+int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n);
+void free_pairs(pfe_context* ctx, PairArrays* pa);
+void thrust_gather_u8(const unsigned char* src, const int* perm, unsigned char* dst, long long n, cudaStream_t s);
+int upload_constants(int device);
+int molecular_setup(pfe_context* ctx, const pfe_args* a);
+int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s);
+int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, double* d_cc, double* d_xc,
+                     bool symmetrize, int ncell, cudaStream_t s);
+int lattice_setup(pfe_context* ctx, const pfe_args* a);
+int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, double* d_cc, double* d_xc,
+                 cudaStream_t s);
+void lattice_release(pfe_context* ctx);
+const char* last_error_cstr();
+}  // namespace pfe

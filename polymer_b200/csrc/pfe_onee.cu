@@ -1,0 +1,343 @@
+// One-electron integrals on the device: S_P and T_P (OVERLAP_KINETIC(0),
+// src/ponee.f90:1-160) and N_P (NUCLEAR_ATTRACTION(0), src/ponee.f90:418-603)
+// over primitive shells, per lattice cell, with the helical image of the second
+// centre.  These are set-up inputs of the Fock build (S_P feeds its pair
+// prefactors), computed once per geometry.  One thread per (shell pair, cell);
+// the Obara-Saika recursions are those of the reference, the Boys function is
+// the same tabulated evaluation as the two-electron kernels.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "pfe_common.cuh"
+
+namespace pfe {
+
+// storage index of a Cartesian power triple of total <= 2 (10 slots)
+__device__ __forceinline__ int cidx(int a, int b, int c) {
+  // order: 000 001 002 010 011 020 100 101 110 200
+  const int s = a * 100 + b * 10 + c;
+  switch (s) {
+    case 0: return 0;
+    case 1: return 1;
+    case 2: return 2;
+    case 10: return 3;
+    case 11: return 4;
+    case 20: return 5;
+    case 100: return 6;
+    case 101: return 7;
+    case 110: return 8;
+    default: return 9;  // 200
+  }
+}
+
+struct OneeDev {
+  int npgs, npshell, natom;
+  const int* p_shell;  // Fortran P_SHELL(npshell,0:4,0:4,0:4), 1-based
+  const int* ang;
+  const double *x, *y, *z, *zt;
+  const int* iatom;
+  const double *ax, *ay, *az;
+  int cel1[3], cel2[3];
+  double period[3], helix;
+  const double* boys;  // row-major [T][m]
+};
+
+__device__ __forceinline__ int psh(const OneeDev& a, int s, int i1, int i2, int i3) {
+  return a.p_shell[s + a.npshell * (i1 + NPOW * (i2 + NPOW * i3))] - 1;
+}
+
+__global__ void k_overlap_kinetic(OneeDev a, double* __restrict__ s_p, double* __restrict__ t_p) {
+  const int n1x = 2 * a.cel1[0] + 1, n1y = 2 * a.cel1[1] + 1, n1z = 2 * a.cel1[2] + 1;
+  const long long total = (long long)a.npshell * a.npshell * n1x * n1y * n1z;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int I = (int)(t % a.npshell), J = (int)((t / a.npshell) % a.npshell);
+  const long long cell = t / ((long long)a.npshell * a.npshell);
+  const int kx = (int)(cell % n1x) - a.cel1[0];
+  const int ky = (int)((cell / n1x) % n1y) - a.cel1[1];
+  const int kz = (int)(cell / ((long long)n1x * n1y)) - a.cel1[2];
+  const double qx = kx * a.period[0], qy = ky * a.period[1], qz = kz * a.period[2];
+  const double ang = kx * a.helix, cs = cos(ang), sn = sin(ang);
+  const int ii = psh(a, I, 0, 0, 0), jj = psh(a, J, 0, 0, 0);
+  const double Ax = a.x[ii], Ay = a.y[ii], Az = a.z[ii];
+  const double Bx = a.x[jj] + qx, By = a.y[jj] * cs - a.z[jj] * sn + qy, Bz = a.y[jj] * sn + a.z[jj] * cs + qz;
+  const double r = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+  const double z1 = a.zt[ii] + a.zt[jj], z2 = sqrt(z1 * z1 * z1), gzi = a.zt[ii] * a.zt[jj] / z1;
+  const double pisub = sqrt(REF_PI * REF_PI * REF_PI);
+  double S1[10][10], T1[10][10];
+  S1[0][0] = pisub / z2 * exp(-gzi * r);
+  T1[0][0] = gzi * (3.0 - 2.0 * gzi * r) * S1[0][0];
+  const double Px = (Ax * a.zt[ii] + Bx * a.zt[jj]) / z1, Py = (Ay * a.zt[ii] + By * a.zt[jj]) / z1,
+               Pz = (Az * a.zt[ii] + Bz * a.zt[jj]) / z1;
+  const double PA[3] = {Px - Ax, Py - Ay, Pz - Az}, PB[3] = {Px - Bx, Py - By, Pz - Bz};
+  const int LI = a.ang[I], LJ = a.ang[J];
+  for (int i1 = 0; i1 <= LI; ++i1)
+    for (int i2 = 0; i2 <= LI - i1; ++i2)
+      for (int i3 = 0; i3 <= LI - i1 - i2; ++i3)
+        for (int j1 = 0; j1 <= LJ; ++j1)
+          for (int j2 = 0; j2 <= LJ - j1; ++j2)
+            for (int j3 = 0; j3 <= LJ - j1 - j2; ++j3) {
+              if (i1 + i2 + i3 + j1 + j2 + j3 == 0) continue;
+              int A[3] = {i1, i2, i3}, B[3] = {j1, j2, j3};
+              int ax = -1;
+              bool onA = false;
+              for (int k = 0; k < 3 && ax < 0; ++k) if (A[k] >= 1) { ax = k; onA = true; }
+              for (int k = 0; k < 3 && ax < 0; ++k) if (B[k] >= 1) { ax = k; onA = false; }
+              const int ci = cidx(i1, i2, i3), cj = cidx(j1, j2, j3);
+              if (onA) {
+                int A1[3] = {i1, i2, i3};
+                A1[ax]--;
+                const int c1 = cidx(A1[0], A1[1], A1[2]);
+                double s = PA[ax] * S1[c1][cj];
+                double sm2 = 0.0, tm2 = 0.0, sb = 0.0, tb = 0.0;
+                if (A[ax] >= 2) {
+                  int A2[3] = {A1[0], A1[1], A1[2]};
+                  A2[ax]--;
+                  const int c2 = cidx(A2[0], A2[1], A2[2]);
+                  sm2 = S1[c2][cj];
+                  tm2 = T1[c2][cj];
+                  s += 0.5 * (double)(A[ax] - 1) / z1 * sm2;
+                }
+                if (B[ax] >= 1) {
+                  int B2[3] = {j1, j2, j3};
+                  B2[ax]--;
+                  const int cb = cidx(B2[0], B2[1], B2[2]);
+                  sb = S1[c1][cb];
+                  tb = T1[c1][cb];
+                  s += 0.5 * (double)B[ax] / z1 * sb;
+                }
+                S1[ci][cj] = s;
+                double tv = 2.0 * gzi * s + PA[ax] * T1[c1][cj];
+                if (A[ax] >= 2) tv += 0.5 * (double)(A[ax] - 1) / z1 * tm2 - (double)(A[ax] - 1) * gzi / a.zt[ii] * sm2;
+                if (B[ax] >= 1) tv += 0.5 * (double)B[ax] / z1 * tb;
+                T1[ci][cj] = tv;
+              } else {
+                int B1[3] = {j1, j2, j3};
+                B1[ax]--;
+                const int c1 = cidx(B1[0], B1[1], B1[2]);
+                double s = PB[ax] * S1[ci][c1];
+                double sm2 = 0.0, tm2 = 0.0;
+                if (B[ax] >= 2) {
+                  int B2[3] = {B1[0], B1[1], B1[2]};
+                  B2[ax]--;
+                  const int c2 = cidx(B2[0], B2[1], B2[2]);
+                  sm2 = S1[ci][c2];
+                  tm2 = T1[ci][c2];
+                  s += 0.5 * (double)(B[ax] - 1) / z1 * sm2;
+                }
+                S1[ci][cj] = s;
+                double tv = 2.0 * gzi * s + PB[ax] * T1[ci][c1];
+                if (B[ax] >= 2) tv += 0.5 * (double)(B[ax] - 1) / z1 * tm2 - (double)(B[ax] - 1) * gzi / a.zt[jj] * sm2;
+                T1[ci][cj] = tv;
+              }
+            }
+  const size_t pp = (size_t)a.npgs * a.npgs;
+  for (int i1 = 0; i1 <= LI; ++i1)
+    for (int i2 = 0; i2 <= LI - i1; ++i2)
+      for (int i3 = 0; i3 <= LI - i1 - i2; ++i3)
+        for (int j1 = 0; j1 <= LJ; ++j1)
+          for (int j2 = 0; j2 <= LJ - j1; ++j2)
+            for (int j3 = 0; j3 <= LJ - j1 - j2; ++j3) {
+              const size_t o = (size_t)psh(a, I, i1, i2, i3) + (size_t)a.npgs * psh(a, J, j1, j2, j3) + pp * cell;
+              s_p[o] = S1[cidx(i1, i2, i3)][cidx(j1, j2, j3)];
+              t_p[o] = T1[cidx(i1, i2, i3)][cidx(j1, j2, j3)];
+            }
+}
+
+__global__ void k_nuclear(OneeDev a, double* __restrict__ n_p) {
+  const int n1x = 2 * a.cel1[0] + 1, n1y = 2 * a.cel1[1] + 1, n1z = 2 * a.cel1[2] + 1;
+  const long long total = (long long)a.npshell * a.npshell * n1x * n1y * n1z;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int I = (int)(t % a.npshell), J = (int)((t / a.npshell) % a.npshell);
+  const long long cell = t / ((long long)a.npshell * a.npshell);
+  const int k1x = (int)(cell % n1x) - a.cel1[0];
+  const int k1y = (int)((cell / n1x) % n1y) - a.cel1[1];
+  const int k1z = (int)(cell / ((long long)n1x * n1y)) - a.cel1[2];
+  const double q1x = k1x * a.period[0], q1y = k1y * a.period[1], q1z = k1z * a.period[2];
+  const double ang = k1x * a.helix, cs = cos(ang), sn = sin(ang);
+  const int ii = psh(a, I, 0, 0, 0), jj = psh(a, J, 0, 0, 0);
+  const double Ax = a.x[ii], Ay = a.y[ii], Az = a.z[ii];
+  const double Bx = a.x[jj] + q1x, By = a.y[jj] * cs - a.z[jj] * sn + q1y, Bz = a.y[jj] * sn + a.z[jj] * cs + q1z;
+  const double comz = a.zt[ii] + a.zt[jj];
+  const double Px = (Ax * a.zt[ii] + Bx * a.zt[jj]) / comz, Py = (Ay * a.zt[ii] + By * a.zt[jj]) / comz,
+               Pz = (Az * a.zt[ii] + Bz * a.zt[jj]) / comz;
+  const double r = (Ax - Bx) * (Ax - Bx) + (Ay - By) * (Ay - By) + (Az - Bz) * (Az - Bz);
+  const double sab = sqrt(REF_PI * REF_PI * REF_PI) / sqrt(comz * comz * comz) * exp(-a.zt[ii] * a.zt[jj] / comz * r);
+  const double e1 = 2.0 / sqrt(REF_PI) * sqrt(comz) * sab;
+  const double PA[3] = {Px - Ax, Py - Ay, Pz - Az}, PB[3] = {Px - Bx, Py - By, Pz - Bz};
+  const int LI = a.ang[I], LJ = a.ang[J];
+  double N1[10][10][5];
+  double N2[10][10];
+  for (int x = 0; x < 10; ++x)
+    for (int y = 0; y < 10; ++y) N2[x][y] = 0.0;
+  for (int k2x = -a.cel2[0]; k2x <= a.cel2[0]; ++k2x)
+    for (int k2y = -a.cel2[1]; k2y <= a.cel2[1]; ++k2y)
+      for (int k2z = -a.cel2[2]; k2z <= a.cel2[2]; ++k2z) {
+        const double q2x = k2x * a.period[0], q2y = k2y * a.period[1], q2z = k2z * a.period[2];
+        const double ang2 = k2x * a.helix, cs2 = cos(ang2), sn2 = sin(ang2);
+        for (int k = 0; k < a.natom; ++k) {
+          const double e2 = -(double)a.iatom[k] * e1;
+          const double Cx = a.ax[k] + q2x, Cy = a.ay[k] * cs2 - a.az[k] * sn2 + q2y, Cz = a.ay[k] * sn2 + a.az[k] * cs2 + q2z;
+          const double T = comz * ((Px - Cx) * (Px - Cx) + (Py - Cy) * (Py - Cy) + (Pz - Cz) * (Pz - Cz));
+          const double PC[3] = {Px - Cx, Py - Cy, Pz - Cz};
+          double F[5];
+          switch (LI + LJ) {
+            case 0: boys_tab<0>(T, e2, a.boys, F); break;
+            case 1: boys_tab<1>(T, e2, a.boys, F); break;
+            case 2: boys_tab<2>(T, e2, a.boys, F); break;
+            case 3: boys_tab<3>(T, e2, a.boys, F); break;
+            default: boys_tab<4>(T, e2, a.boys, F); break;
+          }
+          for (int m = 0; m <= LI + LJ; ++m) N1[0][0][m] = F[m];
+          N2[0][0] += N1[0][0][0];
+          for (int i1 = 0; i1 <= LI; ++i1)
+            for (int i2 = 0; i2 <= LI - i1; ++i2)
+              for (int i3 = 0; i3 <= LI - i1 - i2; ++i3)
+                for (int j1 = 0; j1 <= LJ; ++j1)
+                  for (int j2 = 0; j2 <= LJ - j1; ++j2)
+                    for (int j3 = 0; j3 <= LJ - j1 - j2; ++j3) {
+                      const int mmax = LI + LJ - i1 - i2 - i3 - j1 - j2 - j3;
+                      if (i1 + i2 + i3 + j1 + j2 + j3 == 0 || mmax < 0) continue;
+                      int A[3] = {i1, i2, i3}, B[3] = {j1, j2, j3};
+                      int ax = -1;
+                      bool onA = false;
+                      for (int q = 0; q < 3 && ax < 0; ++q) if (A[q] >= 1) { ax = q; onA = true; }
+                      for (int q = 0; q < 3 && ax < 0; ++q) if (B[q] >= 1) { ax = q; onA = false; }
+                      const int ci = cidx(i1, i2, i3), cj = cidx(j1, j2, j3);
+                      for (int m = 0; m <= mmax; ++m) {
+                        double v;
+                        if (onA) {
+                          int A1[3] = {i1, i2, i3};
+                          A1[ax]--;
+                          const int c1 = cidx(A1[0], A1[1], A1[2]);
+                          v = PA[ax] * N1[c1][cj][m] - PC[ax] * N1[c1][cj][m + 1];
+                          if (A[ax] >= 2) {
+                            int A2[3] = {A1[0], A1[1], A1[2]};
+                            A2[ax]--;
+                            const int c2 = cidx(A2[0], A2[1], A2[2]);
+                            v += 0.5 * (double)(A[ax] - 1) / comz * (N1[c2][cj][m] - N1[c2][cj][m + 1]);
+                          }
+                          if (B[ax] >= 1) {
+                            int B2[3] = {j1, j2, j3};
+                            B2[ax]--;
+                            const int cb = cidx(B2[0], B2[1], B2[2]);
+                            v += 0.5 * (double)B[ax] / comz * (N1[c1][cb][m] - N1[c1][cb][m + 1]);
+                          }
+                        } else {
+                          int B1[3] = {j1, j2, j3};
+                          B1[ax]--;
+                          const int c1 = cidx(B1[0], B1[1], B1[2]);
+                          v = PB[ax] * N1[ci][c1][m] - PC[ax] * N1[ci][c1][m + 1];
+                          if (B[ax] >= 2) {
+                            int B2[3] = {B1[0], B1[1], B1[2]};
+                            B2[ax]--;
+                            const int c2 = cidx(B2[0], B2[1], B2[2]);
+                            v += 0.5 * (double)(B[ax] - 1) / comz * (N1[ci][c2][m] - N1[ci][c2][m + 1]);
+                          }
+                        }
+                        N1[ci][cj][m] = v;
+                      }
+                      N2[ci][cj] += N1[ci][cj][0];
+                    }
+        }
+      }
+  const size_t pp = (size_t)a.npgs * a.npgs;
+  for (int i1 = 0; i1 <= LI; ++i1)
+    for (int i2 = 0; i2 <= LI - i1; ++i2)
+      for (int i3 = 0; i3 <= LI - i1 - i2; ++i3)
+        for (int j1 = 0; j1 <= LJ; ++j1)
+          for (int j2 = 0; j2 <= LJ - j1; ++j2)
+            for (int j3 = 0; j3 <= LJ - j1 - j2; ++j3)
+              n_p[(size_t)psh(a, I, i1, i2, i3) + (size_t)a.npgs * psh(a, J, j1, j2, j3) + pp * cell] =
+                  N2[cidx(i1, i2, i3)][cidx(j1, j2, j3)];
+}
+
+template <typename T>
+static int upload(std::vector<void*>& owned, const T* h, size_t n, T** d) {
+  PFE_CUDA(cudaMalloc((void**)d, sizeof(T) * (n ? n : 1)));
+  owned.push_back(*d);
+  PFE_CUDA(cudaMemcpy(*d, h, sizeof(T) * n, cudaMemcpyHostToDevice));
+  return PFE_OK;
+}
+
+static int onee_run(const pfe_onee_args* a, double* s_p, double* t_p, double* n_p) {
+  if (!a || a->npgs <= 0 || a->npshell <= 0 || a->natom <= 0) { set_error("invalid one-electron arguments"); return PFE_EINVAL; }
+  for (int s = 0; s < a->npshell; ++s)
+    if (a->p_shell_ang[s] > LMAX_SUPPORTED) {
+      set_error("f shells are not implemented by the one-electron kernels");
+      return PFE_EUNSUPPORTED;
+    }
+  std::vector<void*> owned;
+  OneeDev d{};
+  int rc = PFE_OK;
+  const size_t psz = (size_t)a->npshell * NPOW * NPOW * NPOW;
+  const int n1 = (2 * a->cel1[0] + 1) * (2 * a->cel1[1] + 1) * (2 * a->cel1[2] + 1);
+  const size_t out_n = (size_t)a->npgs * a->npgs * n1;
+  double *ds = nullptr, *dt = nullptr, *dn = nullptr;
+  std::vector<double> tab((size_t)NIG_T * NIG_M);
+  for (int t = 0; t < NIG_T; ++t)
+    for (int m = 0; m < NIG_M; ++m) tab[(size_t)t * NIG_M + m] = a->igamma[t + (size_t)NIG_T * m];
+  int* dps = nullptr; int* dang = nullptr; int* diat = nullptr;
+  double *dx = nullptr, *dy = nullptr, *dz = nullptr, *dzt = nullptr, *dax = nullptr, *day = nullptr, *daz = nullptr, *dboys = nullptr;
+  if ((rc = upload(owned, a->p_shell, psz, &dps)) || (rc = upload(owned, a->p_shell_ang, (size_t)a->npshell, &dang)) ||
+      (rc = upload(owned, a->pgsx, (size_t)a->npgs, &dx)) || (rc = upload(owned, a->pgsy, (size_t)a->npgs, &dy)) ||
+      (rc = upload(owned, a->pgsz, (size_t)a->npgs, &dz)) || (rc = upload(owned, a->zt, (size_t)a->npgs, &dzt)) ||
+      (rc = upload(owned, a->iatom, (size_t)a->natom, &diat)) || (rc = upload(owned, a->atomx, (size_t)a->natom, &dax)) ||
+      (rc = upload(owned, a->atomy, (size_t)a->natom, &day)) || (rc = upload(owned, a->atomz, (size_t)a->natom, &daz)) ||
+      (rc = upload(owned, tab.data(), tab.size(), &dboys)))
+    goto done;
+  d.npgs = a->npgs; d.npshell = a->npshell; d.natom = a->natom;
+  d.p_shell = dps; d.ang = dang; d.x = dx; d.y = dy; d.z = dz; d.zt = dzt;
+  d.iatom = diat; d.ax = dax; d.ay = day; d.az = daz; d.boys = dboys;
+  for (int k = 0; k < 3; ++k) { d.cel1[k] = a->cel1[k]; d.cel2[k] = a->cel2[k]; d.period[k] = a->period[k]; }
+  d.helix = a->helix;
+  {
+    const long long total = (long long)a->npshell * a->npshell * n1;
+    const unsigned grid = (unsigned)((total + 127) / 128);
+    if (s_p || t_p) {
+      if (cudaMalloc(&ds, sizeof(double) * out_n) != cudaSuccess || cudaMalloc(&dt, sizeof(double) * out_n) != cudaSuccess) {
+        set_error("cudaMalloc failed");
+        rc = PFE_ENOMEM;
+        goto done;
+      }
+      owned.push_back(ds);
+      owned.push_back(dt);
+      cudaMemset(ds, 0, sizeof(double) * out_n);
+      cudaMemset(dt, 0, sizeof(double) * out_n);
+      k_overlap_kinetic<<<grid, 128>>>(d, ds, dt);
+      if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("k_overlap_kinetic failed");
+        rc = PFE_ECUDA;
+        goto done;
+      }
+      if (s_p) cudaMemcpy(s_p, ds, sizeof(double) * out_n, cudaMemcpyDeviceToHost);
+      if (t_p) cudaMemcpy(t_p, dt, sizeof(double) * out_n, cudaMemcpyDeviceToHost);
+    }
+    if (n_p) {
+      if (cudaMalloc(&dn, sizeof(double) * out_n) != cudaSuccess) { set_error("cudaMalloc failed"); rc = PFE_ENOMEM; goto done; }
+      owned.push_back(dn);
+      cudaMemset(dn, 0, sizeof(double) * out_n);
+      k_nuclear<<<grid, 128>>>(d, dn);
+      if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("k_nuclear failed");
+        rc = PFE_ECUDA;
+        goto done;
+      }
+      cudaMemcpy(n_p, dn, sizeof(double) * out_n, cudaMemcpyDeviceToHost);
+    }
+  }
+done:
+  for (void* p : owned) cudaFree(p);
+  return rc;
+}
+
+}  // namespace pfe
+
+extern "C" {
+int32_t pfe_overlap_kinetic(const pfe_onee_args* a, double* s_p, double* t_p) { return pfe::onee_run(a, s_p, t_p, nullptr); }
+int32_t pfe_nuclear_attraction(const pfe_onee_args* a, double* n_p) { return pfe::onee_run(a, nullptr, nullptr, n_p); }
+}

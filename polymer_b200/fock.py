@@ -1,0 +1,133 @@
+"""Python side of libpolymer_fock: the FOURINDEX_ERI call and the device context.
+
+* :func:`fourindex_eri` is the reference-facing call: host arrays in, host
+  C_C/X_C out, through ``pfe_fourindex_eri`` (the entry point a Fortran
+  ISO_C_BINDING shim binds).
+* :class:`DeviceFock` keeps a ``pfe_context`` and runs Fock builds on
+  device-resident torch tensors (``pfe_context_fock`` on torch's current
+  stream) -- the form the GPU SCF loop uses.
+* :func:`onee` computes the caller-side S_P/T_P/N_P on the device.
+
+All of it needs the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import capi
+from .capi import PfeCensus, PfeOneeArgs, check, lib
+from .system import System, from_fortran, to_fortran
+
+
+def onee(sysm: System):
+    """(S_P, T_P, N_P) cell-major from the device kernels (OVERLAP_KINETIC / NUCLEAR_ATTRACTION)."""
+    L = lib()
+    b, d = sysm.basis, sysm.deck
+    keep = dict(p_shell=np.asfortranarray(b.p_shell.astype(np.int32)),
+                ang=np.ascontiguousarray(b.p_shell_ang.astype(np.int32)),
+                atom=np.ascontiguousarray(b.pgs_atom.astype(np.int32)),
+                x=np.ascontiguousarray(b.pgs[:, 0]), y=np.ascontiguousarray(b.pgs[:, 1]),
+                z=np.ascontiguousarray(b.pgs[:, 2]), zt=np.ascontiguousarray(b.zt),
+                iatom=np.array(d.atoms, dtype=np.int32),
+                ax=np.array([c[0] for c in d.coords]), ay=np.array([c[1] for c in d.coords]),
+                az=np.array([c[2] for c in d.coords]), ig=np.asfortranarray(sysm.igamma))
+    a = PfeOneeArgs()
+    a.npgs, a.npshell, a.natom = b.npgs, b.npshell, d.natom
+    a.p_shell = capi.iptr(keep['p_shell'])
+    a.p_shell_ang = capi.iptr(keep['ang'])
+    a.pgs_atom = capi.iptr(keep['atom'])
+    a.pgsx, a.pgsy, a.pgsz = capi.dptr(keep['x']), capi.dptr(keep['y']), capi.dptr(keep['z'])
+    a.zt = capi.dptr(keep['zt'])
+    a.iatom = capi.iptr(keep['iatom'])
+    a.atomx, a.atomy, a.atomz = capi.dptr(keep['ax']), capi.dptr(keep['ay']), capi.dptr(keep['az'])
+    for k in range(3):
+        a.cel1[k], a.cel2[k], a.period[k] = d.cel1[k], d.cel2[k], d.period[k]
+    a.helix = d.helix
+    a.igamma = capi.dptr(keep['ig'])
+    nc = sysm.ncell1
+    n = b.npgs * b.npgs * nc
+    s, t, v = np.zeros(n), np.zeros(n), np.zeros(n)
+    check(L, L.pfe_overlap_kinetic(ctypes.byref(a), capi.dptr(s), capi.dptr(t)))
+    check(L, L.pfe_nuclear_attraction(ctypes.byref(a), capi.dptr(v)))
+    return (from_fortran(s, (nc,), b.npgs).copy(), from_fortran(t, (nc,), b.npgs).copy(),
+            from_fortran(v, (nc,), b.npgs).copy())
+
+
+def fourindex_eri(sysm: System, p_p: np.ndarray, p_p_helix: Optional[np.ndarray] = None,
+                  **kw) -> Tuple[np.ndarray, np.ndarray]:
+    """FOURINDEX_ERI through the C ABI with host buffers: cell-major P_P -> (C_C, X_C)."""
+    L = lib()
+    a, keep = sysm.pfe_args(p_p, p_p_helix, **kw)
+    nc = sysm.ncell1
+    n = sysm.basis.ncgs
+    c = np.zeros(n * n * nc)
+    x = np.zeros_like(c)
+    check(L, L.pfe_fourindex_eri(ctypes.byref(a), capi.dptr(c), capi.dptr(x)))
+    return from_fortran(c, (nc,), n).copy(), from_fortran(x, (nc,), n).copy()
+
+
+class DeviceFock:
+    """A pfe_context bound to one System; callable as the SCF's FockBuilder."""
+
+    def __init__(self, sysm: System, device: int = 0, **kw):
+        self.L = lib()
+        self.sys = sysm
+        self.device = device
+        h = ctypes.c_void_p()
+        check(self.L, self.L.pfe_context_create(device, ctypes.byref(h)))
+        self.ctx = h
+        a, keep = sysm.pfe_args(None, None, **kw)
+        check(self.L, self.L.pfe_context_setup(self.ctx, ctypes.byref(a)))
+        nc, n = sysm.ncell1, sysm.basis.ncgs
+        dev = torch.device('cuda', device)
+        self.out_c = torch.empty((nc, n, n), dtype=torch.float64, device=dev)
+        self.out_x = torch.empty((nc, n, n), dtype=torch.float64, device=dev)
+
+    def census(self) -> dict:
+        c = PfeCensus()
+        check(self.L, self.L.pfe_context_census(self.ctx, ctypes.byref(c)))
+        return {'quartets': c.quartets, 'quartets_ref': c.quartets_ref, 'flops': c.flops,
+                'quartets_fp32': c.quartets_fp32, 'pairs': c.pairs, 'kernel_launches': c.kernel_launches}
+
+    def run_fortran(self, d_pp: torch.Tensor, d_pph: Optional[torch.Tensor], out_c: torch.Tensor,
+                    out_x: torch.Tensor, stream=None) -> None:
+        """Raw call on Fortran-layout device buffers (no layout conversion)."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        check(self.L, self.L.pfe_context_fock(self.ctx, ctypes.c_void_p(d_pp.data_ptr()),
+                                              ctypes.c_void_p(d_pph.data_ptr()) if d_pph is not None else None,
+                                              ctypes.c_void_p(out_c.data_ptr()),
+                                              ctypes.c_void_p(out_x.data_ptr()), ctypes.c_void_p(s)))
+
+    def __call__(self, p_p: torch.Tensor, p_ph: Optional[torch.Tensor] = None):
+        """Cell-major device P_P (and P_P_HELIX) -> cell-major device (C_C, X_C)."""
+        pp = p_p.transpose(-1, -2).contiguous()
+        ph = p_ph.transpose(-1, -2).contiguous() if p_ph is not None else None
+        self.run_fortran(pp, ph, self.out_c, self.out_x)
+        return self.out_c.transpose(-1, -2).clone(), self.out_x.transpose(-1, -2).clone()
+
+    def close(self):
+        if self.ctx is not None:
+            self.L.pfe_context_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def host_fock_builder(sysm: System, **kw):
+    """A FockBuilder going through the host C ABI each call (the drop-in path)."""
+
+    def f(p_p, p_ph):
+        pp = p_p.detach().cpu().numpy()
+        ph = p_ph.detach().cpu().numpy() if p_ph is not None else None
+        c, x = fourindex_eri(sysm, pp, ph, **kw)
+        return (torch.tensor(c, dtype=torch.float64, device=p_p.device),
+                torch.tensor(x, dtype=torch.float64, device=p_p.device))
+    return f

@@ -1,0 +1,56 @@
+"""C-ABI surface checks that need no GPU.
+
+* every entry point include/polymer_fock.h declares is exported by the built
+  libpolymer_fock.so (no compute call is made);
+* the ctypes mirrors of pfe_args / pfe_onee_args / pfe_census have exactly the
+  C layout (offsets measured by compiling a probe against the header).
+"""
+import ctypes
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from polymer_b200 import build, capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, 'include', 'polymer_fock.h')
+
+
+def _declared():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r'\b(pfe_[a-z_]+)\s*\(', txt)))
+
+
+def test_header_declares_the_exports():
+    assert _declared() == sorted(capi.EXPORTS)
+
+
+def test_library_exports_every_symbol():
+    lib = build.build()
+    out = subprocess.run(['nm', '-D', '--defined-only', lib], capture_output=True, text=True, check=True).stdout
+    exported = set(ln.split()[-1] for ln in out.splitlines() if ln.strip())
+    missing = [s for s in capi.EXPORTS if s not in exported]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize('cname,pyt', [('pfe_args', capi.PfeArgs), ('pfe_onee_args', capi.PfeOneeArgs),
+                                       ('pfe_census', capi.PfeCensus)])
+def test_struct_layout_matches_header(cname, pyt):
+    fields = [f[0] for f in pyt._fields_]
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "%s"' % HEADER, 'int main(void){',
+           'printf("%%zu\\n", sizeof(%s));' % cname]
+    for f in fields:
+        src.append('printf("%%zu\\n", offsetof(%s, %s));' % (cname, f))
+    src.append('return 0;}')
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, 'probe.c')
+        exe = os.path.join(d, 'probe')
+        open(c, 'w').write('\n'.join(src))
+        subprocess.run(['gcc', '-o', exe, c], check=True)
+        vals = [int(v) for v in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(pyt)
+    for f, off in zip(fields, vals[1:]):
+        assert getattr(pyt, f).offset == off, f
