@@ -1,0 +1,378 @@
+#!/usr/bin/env python
+"""Fock-build throughput of the CUDA library on the alkane workload.
+
+One step = one direct J/K build (FOURINDEX_ERI) of all-trans C20H42 in
+6-31G** (seeded jitter 0.02 A, INTTOL 1e-10, FP64) with a fixed density.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value: Fock builds/s with P_P resident in HBM (pfe_context_fock), CUDA
+  events on the launch stream, L2 flushed (256 MiB write) before every step.
+* e2e: the same metric through the reference-facing C ABI pfe_fourindex_eri
+  with pinned host buffers (P_P upload and C_C/X_C download inside the step).
+* roofline: the kernel with the largest time share, its algorithmic FP64 flops
+  over its event-timed duration, against the FP64 FMA-pipe peak measured here.
+* cpu_baseline: the CPU oracle (a restatement of the reference loop) on a
+  bounded sample of bra shells, extrapolated to one full build, one core.
+* N > 1 (torchrun): every rank computes its share of the quartet chunks and the
+  J/K matrices are summed with one NCCL all-reduce -- the reference's
+  MPI_ALLREDUCE of J/K; total work is fixed (strong scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = 'Fock builds/s & time-to-converged SCF (1e-8 Eh) vs plain FP64 GPU, 1 B200'
+N_ALKANE = 20
+INTTOL = 1.0e-10
+
+
+def workload_name(n=N_ALKANE):
+    return 'C%dH%d 6-31G** all-trans alkane (seeded jitter 0.02 A), molecule, INTTOL %.0e' % (n, 2 * n + 2, INTTOL)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.th = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        mhz, mx, reasons = [], 0.0, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(',')]
+            if len(p) < 9:
+                continue
+            try:
+                mhz.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(nm)
+        return {'sm_mhz': statistics.median(mhz) if mhz else None, 'sm_max_mhz': mx or None,
+                'reasons': sorted(reasons), 'samples': len(mhz)}
+
+
+def build_problem(device: int):
+    import numpy as np
+    import torch
+    from polymer_b200 import fock, geometry, scf, system
+    deck = geometry.alkane_deck(N_ALKANE, inttol=INTTOL)
+    sysm = system.build_system(deck, fock.onee)
+    # a realistic density: one SCF iteration from the nuclear-charge guess
+    st = scf.HostState(sysm, 'cuda:%d' % device)
+    p_c = torch.tensor(scf.guess_density(sysm), dtype=torch.float64, device=st.device)
+    p_p = scf.decontract(st, p_c)
+    df0 = fock.DeviceFock(sysm, device)
+    c_c, x_c = df0(p_p)
+    p_out, _, _, _ = scf.fock_build(st, st.t_c + st.n_c + c_c - 0.5 * x_c)
+    p_p = scf.decontract(st, p_out)
+    df0.close()
+    return sysm, p_p
+
+
+def measure_fp64_peak(device: int) -> float:
+    import ctypes
+    from polymer_b200 import capi
+    L = capi.lib()
+    v = ctypes.c_double(0.0)
+    capi.check(L, L.pfe_measure_fp64_peak(device, ctypes.byref(v)))
+    return v.value
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes of the dominant kernel from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, 'profiles', 'roofline_traffic.json')
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline(sysm, p_p_np, budget_s: float = 15.0):
+    """Oracle on bra shells I = 0 (mod stride), extrapolated to a full build, 1 thread."""
+    import oracle
+    n = sysm.basis.npshell
+    t0 = time.perf_counter()
+    oracle.fourindex_eri_sample(sysm, p_p_np, n + 1, n)   # no bra shell: the fixed KL/Schwarz part
+    t_fixed = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.fourindex_eri_sample(sysm, p_p_np, n, 0)       # one bra shell
+    t_one = time.perf_counter() - t0 - t_fixed
+    per = max(t_one, 1e-3)
+    nsamp = max(1, min(n, int((budget_s - t_fixed) / per)))
+    stride = max(1, n // nsamp)
+    t0 = time.perf_counter()
+    oracle.fourindex_eri_sample(sysm, p_p_np, stride, 0)
+    t_s = time.perf_counter() - t0
+    sampled = len(range(0, n, stride))
+    t_full = t_fixed + (t_s - t_fixed) * n / sampled
+    return {'value': 1.0 / t_full, 'unit': 'Fock builds/s', 'cores': 1, 'kind': 'port',
+            'sample': 'oracle FOURINDEX_ERI restatement over bra shells I = 0 mod %d (%d of %d), '
+                      'extrapolated: %.1f s per full build' % (stride, sampled, n, t_full),
+            'seconds_per_build': t_full}
+
+
+def _ref_system():
+    """The workload's System with the oracle's S_P (T/V are not needed by the Fock build)."""
+    import oracle
+    from polymer_b200 import geometry, system
+
+    def onee_s(sysm):
+        s_p, t_p, _ = oracle.onee_overlap(sysm)
+        return s_p, t_p, t_p * 0.0
+    return system.build_system(geometry.alkane_deck(N_ALKANE, inttol=INTTOL), onee_s)
+
+
+_REF_SYS = None
+
+
+def _ref_worker(args):
+    """Oracle FOURINDEX_ERI restricted to bra shells I = offset (mod stride)."""
+    global _REF_SYS
+    import numpy as np
+    import oracle
+    stride, offset = args
+    if _REF_SYS is None:
+        _REF_SYS = _ref_system()
+    n = _REF_SYS.basis.npgs
+    pp = np.zeros((1, n, n))
+    t0 = time.perf_counter()
+    oracle.fourindex_eri_sample(_REF_SYS, pp, stride, offset)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    """The reference's CPU algorithm (oracle port; Fortran is not buildable here) on all host cores."""
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    sysm = _ref_system()
+    n = sysm.basis.npshell
+    per_worker = 2
+    stride = max(1, n // per_worker)          # I = offset (mod stride): per_worker shells each
+    ctx = mp.get_context('spawn')
+    walls, fixed = [], []
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_worker, [(n + 1, n)] * cores)          # set-up of every worker
+        fixed = pool.map(_ref_worker, [(n + 1, n)] * cores)  # the per-build KL/Schwarz part alone
+        t_fixed = statistics.median(fixed)
+        for it in range(args.warmup + args.steps):
+            # every worker takes `per_worker` bra shells; the offsets rotate over the molecule
+            offs = [(stride, (it * cores + c) % stride) for c in range(cores)]
+            t0 = time.perf_counter()
+            ts = pool.map(_ref_worker, offs)
+            wall = time.perf_counter() - t0
+            if it >= args.warmup:
+                shells = sum(len(range(o, n, stride)) for _, o in offs)
+                walls.append((wall, max(ts), shells))
+    # a full build on `cores` processes: the fixed part once, the n bra shells spread over the cores
+    per_shell = statistics.mean((max(w[1] - t_fixed, 1e-6)) * cores / w[2] for w in walls)
+    t_full = t_fixed + per_shell * n / cores
+    value = 1.0 / t_full
+    line = {'metric': METRIC, 'value': value, 'unit': 'Fock builds/s', 'n_gpus': args.gpus, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * statistics.mean(w[0] for w in walls),
+            'higher_is_better': True, 'scaling': 'strong', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'impl': 'reference',
+            'config': {'workload': workload_name(), 'parallelism': 'cpu x%d processes' % cores},
+            'cpu_baseline': {'value': value, 'unit': 'Fock builds/s', 'cores': cores, 'kind': 'port',
+                             'sample': 'per step %d bra shells of %d on %d processes (stride %d), extrapolated '
+                                       'to one full build (%.1f s); the Fortran reference cannot be compiled here '
+                                       '(no gfortran/mpif90)' % (walls[0][2], n, cores, stride, t_full)},
+            'e2e': {'value': value, 'unit': 'Fock builds/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=10)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == 'reference':
+        return run_reference(args)
+
+    from polymer_b200 import build as _build
+    _build.build()   # no-op when the in-tree library is up to date
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from polymer_b200 import capi, fock, system
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    dev = torch.device('cuda', local)
+
+    sysm, p_p = build_problem(local)
+    df = fock.DeviceFock(sysm, local, myid=rank, numprocs=world)
+    cen = df.census()
+    nc, n = sysm.ncell1, sysm.basis.ncgs
+    pp_f = p_p.transpose(-1, -2).contiguous()
+    out_c = torch.empty((nc, n, n), dtype=torch.float64, device=dev)
+    out_x = torch.empty_like(out_c)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        df.run_fortran(pp_f, None, out_c, out_x)
+        if world > 1:
+            dist.all_reduce(out_c)
+            dist.all_reduce(out_x)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            step()
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_step = float(t.item()) / args.steps
+    value = 1000.0 / ms_step
+
+    # ---- roofline of the dominant kernel (one profiled build, untimed above)
+    L = capi.lib()
+    capi.check(L, L.pfe_context_profile(df.ctx, 1))
+    step()
+    torch.cuda.synchronize()
+    stats = (capi.PfeKernelStat * 64)()
+    nst = L.pfe_context_kernel_stats(df.ctx, stats, 64)
+    capi.check(L, L.pfe_context_profile(df.ctx, 0))
+    kern = [{'cls': '%04d' % s.cls, 'ms': s.ms, 'quartets': s.quartets, 'flops': s.flops} for s in stats[:max(nst, 0)]]
+    tot_ms = sum(k['ms'] for k in kern) or 1.0
+    dom = max(kern, key=lambda k: k['ms']) if kern else None
+    peak = measure_fp64_peak(local)
+    roof = None
+    if dom:
+        ach = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
+        traffic = ncu_traffic_per_launch()
+        roof = {'bound': 'fp64', 'kernel': 'k_quartets<%s>' % dom['cls'], 'achieved': ach, 'peak': peak,
+                'unit': 'TFLOP/s', 'frac': ach / peak if peak else None,
+                'peak_source': 'measured in this run: DFMA loop over all SMs (pfe_measure_fp64_peak); '
+                               'MEASURED_PEAKS.json has no FP64 figure',
+                'share_of_build': dom['ms'] / tot_ms,
+                'traffic': traffic.get(dom['cls']) if isinstance(traffic, dict) else None}
+        all_flops = sum(k['flops'] for k in kern)
+        roof['build_achieved'] = all_flops / (tot_ms * 1e-3) / 1e12
+
+    # ---- end to end through the host C ABI (pinned host buffers)
+    e2e = None
+    if world == 1:
+        pin_p = torch.empty(pp_f.numel(), dtype=torch.float64).pin_memory()
+        pin_p.copy_(pp_f.reshape(-1).cpu())
+        pin_c = torch.empty(nc * n * n, dtype=torch.float64).pin_memory()
+        pin_x = torch.empty_like(pin_c).pin_memory()
+        a, keep = sysm.pfe_args(None, None)
+        import ctypes
+        a.p_p = ctypes.cast(pin_p.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        cp = ctypes.cast(pin_c.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        xp = ctypes.cast(pin_x.data_ptr(), ctypes.POINTER(ctypes.c_double))
+        for _ in range(args.warmup):
+            capi.check(L, L.pfe_fourindex_eri(ctypes.byref(a), cp, xp))
+        walls = []
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            capi.check(L, L.pfe_fourindex_eri(ctypes.byref(a), cp, xp))
+            walls.append(time.perf_counter() - t0)
+        e2e = {'value': args.steps / sum(walls), 'unit': 'Fock builds/s',
+               'h2d_bytes_per_step': int(pin_p.numel() * 8), 'd2h_bytes_per_step': int(2 * pin_c.numel() * 8),
+               'ms_per_step': 1e3 * sum(walls) / args.steps,
+               'path': 'pfe_fourindex_eri (host pointers; static inputs cached on the device by content hash)'}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(sysm, p_p.cpu().numpy())
+
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': 'Fock builds/s', 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': ms_step, 'higher_is_better': True, 'scaling': 'strong',
+                'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': workload_name(), 'npgs': sysm.basis.npgs, 'ncgs': sysm.basis.ncgs,
+                           'npshell': sysm.basis.npshell, 'precision': 'fp64',
+                           'l2': 'flushed before every timed step (256 MiB write)',
+                           'parallelism': 'quartet chunks split over %d GPU(s), NCCL all-reduce of J/K' % world
+                           if world > 1 else 'single GPU'},
+                'quartets_per_build': cen['quartets'], 'quartets_per_s': cen['quartets'] * value,
+                'gpu_launches': args.steps * int(cen['kernel_launches']),
+                'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'cpu_baseline': cpu}
+        print(json.dumps(line))
+    df.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -107,6 +107,25 @@ typedef struct pfe_census {
 } pfe_census;
 int32_t pfe_context_census(pfe_context *ctx, pfe_census *out);
 
+/* Per-kernel timing of pfe_context_fock (diagnostics; no counterpart in the
+ * reference).  With profiling on, every quartet-class launch is bracketed by
+ * CUDA events on the caller's stream; pfe_context_kernel_stats() (after the
+ * stream is synchronised) returns, per launch of the last Fock build, the class
+ * code 1000*LA+100*LB+10*LC+LD, the milliseconds, the screened quartets and the
+ * algorithmic flops.  Returns the number of launches written. */
+int32_t pfe_context_profile(pfe_context *ctx, int32_t enable);
+typedef struct pfe_kernel_stat {
+  int32_t cls;
+  float ms;
+  double quartets;
+  double flops;
+} pfe_kernel_stat;
+int32_t pfe_context_kernel_stats(pfe_context *ctx, pfe_kernel_stat *out, int32_t cap);
+
+/* Measured FP64 FMA-pipe throughput of `device` in TFLOP/s (a dependent-chain
+ * free DFMA loop over all SMs; diagnostics for the roofline denominator). */
+int32_t pfe_measure_fp64_peak(int32_t device, double *tflops);
+
 /* ---- caller-side set-up integrals (outside FOURINDEX_ERI) ----
  * The Fortran caller computes these before the SCF (src/psinglepoint.f90:184,212);
  * they are provided on the device so a host driver needs no CPU integral code. */

@@ -53,6 +53,8 @@ def lib():
         L = ctypes.CDLL(LIB)
         L.oracle_fourindex_eri.argtypes = [ctypes.POINTER(PfeArgs), _dp, _dp]
         L.oracle_fourindex_eri.restype = ctypes.c_int32
+        L.oracle_fourindex_eri_sample.argtypes = [ctypes.POINTER(PfeArgs), _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+        L.oracle_fourindex_eri_sample.restype = ctypes.c_int32
         L.oracle_fmt_table.argtypes = [_dp]
         L.oracle_overlap_kinetic.argtypes = [ctypes.POINTER(OneeArgs), _dp, _dp]
         L.oracle_overlap_kinetic.restype = ctypes.c_int32
@@ -70,6 +72,10 @@ def fmt_table() -> np.ndarray:
 
 def onee(sysm):
     """(S_P, T_P, N_P) cell-major, from the oracle's OVERLAP_KINETIC / NUCLEAR_ATTRACTION."""
+    return _onee(sysm, with_v=True)
+
+
+def _onee(sysm, with_v):
     from polymer_b200.system import from_fortran
     b, d = sysm.basis, sysm.deck
     keep = dict(p_shell=np.asfortranarray(b.p_shell.astype(np.int32)),
@@ -98,9 +104,16 @@ def onee(sysm):
     n = np.zeros_like(s)
     L = lib()
     assert L.oracle_overlap_kinetic(ctypes.byref(a), s.ctypes.data_as(_dp), t.ctypes.data_as(_dp)) == 0
-    assert L.oracle_nuclear_attraction(ctypes.byref(a), n.ctypes.data_as(_dp)) == 0
+    if with_v:
+        assert L.oracle_nuclear_attraction(ctypes.byref(a), n.ctypes.data_as(_dp)) == 0
     return (from_fortran(s, (nc,), b.npgs).copy(), from_fortran(t, (nc,), b.npgs).copy(),
             from_fortran(n, (nc,), b.npgs).copy())
+
+
+def onee_overlap(sysm):
+    """(S_P, T_P) only -- what the Fock build needs from the one-electron set-up."""
+    s, t, _ = _onee(sysm, with_v=False)
+    return s, t, None
 
 
 def fourindex_eri(sysm, p_p: np.ndarray, p_p_helix=None, **kw):
@@ -114,6 +127,21 @@ def fourindex_eri(sysm, p_p: np.ndarray, p_p_helix=None, **kw):
     rc = lib().oracle_fourindex_eri(ctypes.byref(a), c.ctypes.data_as(_dp), x.ctypes.data_as(_dp))
     if rc != 0:
         raise RuntimeError('oracle_fourindex_eri failed with %d' % rc)
+    return from_fortran(c, (nc,), b.ncgs).copy(), from_fortran(x, (nc,), b.ncgs).copy()
+
+
+def fourindex_eri_sample(sysm, p_p: np.ndarray, stride: int, offset: int, **kw):
+    """The oracle restricted to bra shells I = offset (mod stride): a bounded CPU sample."""
+    from polymer_b200.system import from_fortran
+    b = sysm.basis
+    a, keep = sysm.pfe_args(p_p, None, **kw)
+    nc = sysm.ncell1
+    c = np.zeros(b.ncgs * b.ncgs * nc)
+    x = np.zeros_like(c)
+    rc = lib().oracle_fourindex_eri_sample(ctypes.byref(a), c.ctypes.data_as(_dp), x.ctypes.data_as(_dp),
+                                           stride, offset)
+    if rc != 0:
+        raise RuntimeError('oracle_fourindex_eri_sample failed with %d' % rc)
     return from_fortran(c, (nc,), b.ncgs).copy(), from_fortran(x, (nc,), b.ncgs).copy()
 
 

@@ -257,6 +257,21 @@ static inline double boys_tab(const double *ig, int m, double T, double c2, cons
 }
 
 /* ---------------------------------------------------------- FOURINDEX_ERI */
+/* Bra-shell sampling for the bounded CPU baseline: only I with I % g_stride ==
+ * g_offset are processed (1/0 = the whole loop, the reference's semantics). */
+static int g_stride = 1, g_offset = 0;
+
+int32_t oracle_fourindex_eri(const pfe_args *a, double *c_c, double *x_c);
+
+int32_t oracle_fourindex_eri_sample(const pfe_args *a, double *c_c, double *x_c, int32_t stride, int32_t offset) {
+  g_stride = stride > 0 ? stride : 1;
+  g_offset = offset;
+  int32_t rc = oracle_fourindex_eri(a, c_c, x_c);
+  g_stride = 1;
+  g_offset = 0;
+  return rc;
+}
+
 int32_t oracle_fourindex_eri(const pfe_args *a, double *c_c, double *x_c) {
   build_types();
   if (!g_eri) g_eri = (double *)malloc(sizeof(double) * MDIM * (NCMP + 1) * (NCMP + 1));
@@ -344,6 +359,7 @@ int32_t oracle_fourindex_eri(const pfe_args *a, double *c_c, double *x_c) {
         }
       }
       for (int I = 0; I < nsh; ++I) {
+        if (I % g_stride != g_offset) continue;
         int ii = head[I];
         double ax = X[ii], ay = Y[ii], az = Z[ii];
         for (int J = 0; J < nsh; ++J) {

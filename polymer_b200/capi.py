@@ -59,6 +59,11 @@ class PfeCensus(ctypes.Structure):
                 ('pairs', ctypes.c_int64), ('kernel_launches', ctypes.c_int32)]
 
 
+class PfeKernelStat(ctypes.Structure):
+    _fields_ = [('cls', ctypes.c_int32), ('ms', ctypes.c_float), ('quartets', ctypes.c_double),
+                ('flops', ctypes.c_double)]
+
+
 class FockError(RuntimeError):
     """A non-zero status from the library (the reference would PABORT)."""
 
@@ -111,6 +116,12 @@ def lib(path: str = LIB_PATH):
     L.pfe_overlap_kinetic.restype = ctypes.c_int32
     L.pfe_nuclear_attraction.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp]
     L.pfe_nuclear_attraction.restype = ctypes.c_int32
+    L.pfe_context_profile.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.pfe_context_profile.restype = ctypes.c_int32
+    L.pfe_context_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeKernelStat), ctypes.c_int32]
+    L.pfe_context_kernel_stats.restype = ctypes.c_int32
+    L.pfe_measure_fp64_peak.argtypes = [ctypes.c_int32, _dp]
+    L.pfe_measure_fp64_peak.restype = ctypes.c_int32
     L.pfe_version.argtypes = []
     L.pfe_version.restype = ctypes.c_char_p
     _LIB = L
@@ -131,4 +142,5 @@ def check(L, code: int) -> None:
 # Exported symbols declared in include/polymer_fock.h (checked by the CPU tests).
 EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_context_destroy',
            'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_overlap_kinetic',
-           'pfe_nuclear_attraction', 'pfe_version']
+           'pfe_nuclear_attraction', 'pfe_context_profile', 'pfe_context_kernel_stats',
+           'pfe_measure_fp64_peak', 'pfe_version']

@@ -71,9 +71,18 @@ double class_flops(int cb, int ck) {
   return eri_recursion_flops(la, lb, lc, ld) + 13.0 * (lt + 1) + 40.0 + 12.0 * ni;
 }
 
+// 64-bit-word mixing hash of the static inputs (detects any change of them).
 static uint64_t fnv(uint64_t h, const void* p, size_t n) {
   const unsigned char* b = (const unsigned char*)p;
-  for (size_t i = 0; i < n; ++i) {
+  size_t i = 0;
+  for (; i + 8 <= n; i += 8) {
+    uint64_t w;
+    memcpy(&w, b + i, 8);
+    h ^= w;
+    h *= 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+  }
+  for (; i < n; ++i) {
     h ^= b[i];
     h *= 1099511628211ull;
   }
@@ -369,6 +378,32 @@ int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
   out->pairs = ctx->npairs;
   out->kernel_launches = ctx->nlaunch + (ctx->molecular ? 2 : 3);
   return PFE_OK;
+}
+
+int32_t pfe_context_profile(pfe_context* ctx, int32_t enable) {
+  if (!ctx) { set_error("null context"); return PFE_EINVAL; }
+  ctx->profile = enable != 0;
+  return PFE_OK;
+}
+
+int32_t pfe_context_kernel_stats(pfe_context* ctx, pfe_kernel_stat* out, int32_t cap) {
+  if (!ctx || !out) { set_error("null argument"); return PFE_EINVAL; }
+  if (!ctx->profile) { set_error("profiling is off"); return PFE_EINVAL; }
+  int n = 0;
+  for (int i = 0; i < ctx->nprof && n < cap; ++i, ++n) {
+    float ms = 0.f;
+    PFE_CUDA(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
+    out[n].cls = ctx->ev_cls[i];
+    out[n].ms = ms;
+    out[n].quartets = ctx->ev_quartets[i];
+    out[n].flops = ctx->ev_flops[i];
+  }
+  return n;
+}
+
+int32_t pfe_measure_fp64_peak(int32_t device, double* tflops) {
+  if (!tflops) { set_error("null output"); return PFE_EINVAL; }
+  return measure_fp64_peak(device, tflops);
 }
 
 static std::mutex g_default_mu;

@@ -110,6 +110,14 @@ struct pfe_context {
   // lattice path state lives in pfe_lattice.cu
   void* lattice = nullptr;
 
+  // per-launch timing (pfe_context_profile)
+  bool profile = false;
+  cudaEvent_t ev[130] = {};
+  int nev = 0;
+  int ev_cls[64] = {0};
+  double ev_quartets[64] = {0}, ev_flops[64] = {0};
+  int nprof = 0;
+
   std::vector<void*> owned;    // freed on reset/destroy
   std::vector<void*> pending;  // scratch freed at the end of setup
 
@@ -153,4 +161,5 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
                  cudaStream_t s);
 void lattice_release(pfe_context* ctx);
 const char* last_error_cstr();
+int measure_fp64_peak(int device, double* tflops);
 }  // namespace pfe

@@ -838,6 +838,12 @@ int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d
   ql.npgs = ctx->npgs;
   ql.myid = ctx->myid;
   ql.numprocs = ctx->numprocs;
+  if (ctx->profile) {
+    for (int i = 0; i <= ctx->nlaunch && i < 64; ++i)
+      if (!ctx->ev[i]) PFE_CUDA(cudaEventCreate(&ctx->ev[i]));
+    ctx->nprof = ctx->nlaunch;
+    PFE_CUDA(cudaEventRecord(ctx->ev[0], s));
+  }
   for (int i = 0; i < ctx->nlaunch; ++i) {
     const ClassLaunch& cl = ctx->launches[i];
     ql.chunks = cl.chunks;
@@ -856,6 +862,12 @@ int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d
       launcher(cl.cb, cl.ck)(ql, grid, s);
     }
     PFE_CUDA(cudaGetLastError());
+    if (ctx->profile) {
+      PFE_CUDA(cudaEventRecord(ctx->ev[i + 1], s));
+      ctx->ev_cls[i] = 1000 * kClassL[cl.cb][0] + 100 * kClassL[cl.cb][1] + 10 * kClassL[cl.ck][0] + kClassL[cl.ck][1];
+      ctx->ev_quartets[i] = cl.quartets;
+      ctx->ev_flops[i] = cl.quartets * class_flops(cl.cb, cl.ck);
+    }
   }
   return contract_outputs(ctx, ctx->d_jp, ctx->d_kp, d_cc, d_xc, /*symmetrize=*/true, 1, s);
 }
@@ -887,5 +899,48 @@ int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, doubl
 }
 
 const char* last_error_cstr() { return g_err.c_str(); }
+
+// Independent FMA chains: 8 accumulators per thread, no memory traffic.
+__global__ void k_dfma_peak(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+      x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+    }
+  }
+  const double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (r == 1.2345) out[0] = r;  // keeps the chains live
+}
+
+int measure_fp64_peak(int device, double* tflops) {
+  PFE_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  PFE_CUDA(cudaGetDeviceProperties(&prop, device));
+  double* d = nullptr;
+  PFE_CUDA(cudaMalloc(&d, sizeof(double)));
+  const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 4096;
+  cudaEvent_t e0, e1;
+  PFE_CUDA(cudaEventCreate(&e0));
+  PFE_CUDA(cudaEventCreate(&e1));
+  k_dfma_peak<<<blocks, threads>>>(d, 64, 0.999999, 1e-7);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; ++r) {
+    PFE_CUDA(cudaEventRecord(e0));
+    k_dfma_peak<<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+    PFE_CUDA(cudaEventRecord(e1));
+    PFE_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    best = std::min(best, ms);
+  }
+  const double flops = 2.0 * 8.0 * 16.0 * (double)iters * blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d);
+  return PFE_OK;
+}
 
 }  // namespace pfe

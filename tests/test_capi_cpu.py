@@ -21,7 +21,7 @@ HEADER = os.path.join(ROOT, 'include', 'polymer_fock.h')
 
 def _declared():
     txt = open(HEADER).read()
-    return sorted(set(re.findall(r'\b(pfe_[a-z_]+)\s*\(', txt)))
+    return sorted(set(re.findall(r'\b(pfe_[a-z0-9_]+)\s*\(', txt)))
 
 
 def test_header_declares_the_exports():
