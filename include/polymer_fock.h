@@ -116,11 +116,23 @@ int32_t pfe_context_census(pfe_context *ctx, pfe_census *out);
 int32_t pfe_context_profile(pfe_context *ctx, int32_t enable);
 typedef struct pfe_kernel_stat {
   int32_t cls;
+  int32_t variant;    /* 0 straight-line thread/quartet, 1 warp/quartet, 2 block/quartet */
   float ms;
+  float tuned_ms[3];  /* autotuner timing of each variant, 0 where not run */
   double quartets;
   double flops;
 } pfe_kernel_stat;
 int32_t pfe_context_kernel_stats(pfe_context *ctx, pfe_kernel_stat *out, int32_t cap);
+
+/* Schedule autotuning (no counterpart in the reference): time every execution
+ * variant of every quartet class on this context's screened work lists with the
+ * device density d_p_p, keep the fastest for later builds.  Synchronous.  The
+ * host entry point pfe_fourindex_eri runs it on its first call after a set-up. */
+int32_t pfe_context_autotune(pfe_context *ctx, const double *d_p_p, const double *d_p_p_helix, void *stream);
+
+/* Force execution variant v (0/1/2 as in pfe_kernel_stat) on every quartet
+ * class that has it; the others keep theirs (diagnostics and tests). */
+int32_t pfe_context_force_variant(pfe_context *ctx, int32_t variant);
 
 /* Measured FP64 FMA-pipe throughput of `device` in TFLOP/s (a dependent-chain
  * free DFMA loop over all SMs; diagnostics for the roofline denominator). */

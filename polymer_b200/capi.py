@@ -60,8 +60,8 @@ class PfeCensus(ctypes.Structure):
 
 
 class PfeKernelStat(ctypes.Structure):
-    _fields_ = [('cls', ctypes.c_int32), ('ms', ctypes.c_float), ('quartets', ctypes.c_double),
-                ('flops', ctypes.c_double)]
+    _fields_ = [('cls', ctypes.c_int32), ('variant', ctypes.c_int32), ('ms', ctypes.c_float),
+                ('tuned_ms', ctypes.c_float * 3), ('quartets', ctypes.c_double), ('flops', ctypes.c_double)]
 
 
 class FockError(RuntimeError):
@@ -120,6 +120,10 @@ def lib(path: str = LIB_PATH):
     L.pfe_context_profile.restype = ctypes.c_int32
     L.pfe_context_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeKernelStat), ctypes.c_int32]
     L.pfe_context_kernel_stats.restype = ctypes.c_int32
+    L.pfe_context_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.pfe_context_autotune.restype = ctypes.c_int32
+    L.pfe_context_force_variant.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.pfe_context_force_variant.restype = ctypes.c_int32
     L.pfe_measure_fp64_peak.argtypes = [ctypes.c_int32, _dp]
     L.pfe_measure_fp64_peak.restype = ctypes.c_int32
     L.pfe_version.argtypes = []
@@ -143,4 +147,5 @@ def check(L, code: int) -> None:
 EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_context_destroy',
            'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_overlap_kinetic',
            'pfe_nuclear_attraction', 'pfe_context_profile', 'pfe_context_kernel_stats',
-           'pfe_measure_fp64_peak', 'pfe_version']
+           'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
+           'pfe_version']

@@ -271,7 +271,7 @@ def emit_optable(LA, LB, LC, LD):
     ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD)
     name = 'op_%d%d%d%d' % (LA, LB, LC, LD)
     lines = ['// (%d%d|%d%d): %d ops in %d levels, %d slots' % (LA, LB, LC, LD, len(ops), len(lev) - 1, nslots)]
-    flat = [v for op in ops for v in op]
+    flat = [v for op in ops for v in op] or [0] * 6
     lines.append('static const unsigned short %s_ops[%d] = {%s};' % (name, len(flat), ','.join(map(str, flat))))
     lines.append('static const int %s_levels[%d] = {%s};' % (name, len(lev), ','.join(map(str, lev))))
     lines.append('static const unsigned short %s_out[%d] = {%s};' % (name, len(outs), ','.join(map(str, outs))))
@@ -343,10 +343,10 @@ def main():
             if ik > ib and not both:
                 continue   # the kernels put the higher pair class on the bra side
             n = ncomp_class = (len(comps(LA)) * len(comps(LB)) * len(comps(LC)) * len(comps(LD)))
+            big.append(emit_optable(LA, LB, LC, LD))   # every class can run interpreted
             if n > OPS_THRESHOLD:
                 g = Gen(LA, LB, LC, LD)
                 g.build()
-                big.append(emit_optable(LA, LB, LC, LD))
                 table['%d%d%d%d' % (LA, LB, LC, LD)] = {'integrals': n, 'recursion_flops': g.flops, 'interpreted': True}
                 continue
             code, n, fl = gen_class(LA, LB, LC, LD)

@@ -196,6 +196,7 @@ static void reset_context(pfe_context* ctx) {
   ctx->pp_bytes = ctx->pph_bytes = ctx->out_bytes = 0;
   ctx->nlaunch = 0;
   ctx->ready = false;
+  ctx->tuned = false;
 }
 
 static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs, uint64_t key) {
@@ -394,11 +395,35 @@ int32_t pfe_context_kernel_stats(pfe_context* ctx, pfe_kernel_stat* out, int32_t
     float ms = 0.f;
     PFE_CUDA(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
     out[n].cls = ctx->ev_cls[i];
+    out[n].variant = ctx->ev_variant[i];
+    for (int v = 0; v < 3; ++v) out[n].tuned_ms[v] = ctx->ev_tuned[i][v];
     out[n].ms = ms;
     out[n].quartets = ctx->ev_quartets[i];
     out[n].flops = ctx->ev_flops[i];
   }
   return n;
+}
+
+int32_t pfe_context_autotune(pfe_context* ctx, const double* d_p_p, const double* d_p_p_helix, void* stream) {
+  if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
+  if (!d_p_p) { set_error("null density"); return PFE_EINVAL; }
+  (void)d_p_p_helix;
+  PFE_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->molecular) return PFE_OK;  // the lattice path has a single schedule
+  return autotune(ctx, d_p_p, (cudaStream_t)stream);
+}
+
+int32_t pfe_context_force_variant(pfe_context* ctx, int32_t variant) {
+  if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
+  if (variant < 0 || variant > 2) { set_error("variant must be 0, 1 or 2"); return PFE_EINVAL; }
+  for (int i = 0; i < ctx->nlaunch; ++i) {
+    ClassLaunch& cl = ctx->launches[i];
+    if (variant == 0 && cl.has_straight) cl.variant = 0;
+    if (variant == 1 && cl.has_table && sizeof(double) * (size_t)cl.per_warp <= 200 * 1024) cl.variant = 1;
+    if (variant == 2 && cl.has_table) cl.variant = 2;
+  }
+  ctx->tuned = true;
+  return PFE_OK;
 }
 
 int32_t pfe_measure_fp64_peak(int32_t device, double* tflops) {
@@ -458,6 +483,9 @@ int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
     }
     PFE_CUDA(cudaMemcpyAsync(ctx->d_pph, a->p_p_helix, nh * sizeof(double), cudaMemcpyHostToDevice, s));
     d_pph = ctx->d_pph;
+  }
+  if (ctx->molecular && !ctx->tuned) {
+    if ((rc = autotune(ctx, ctx->d_pp, s)) != PFE_OK) return rc;
   }
   rc = ctx->molecular ? molecular_fock(ctx, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, s)
                       : lattice_fock(ctx, ctx->d_pp, d_pph, ctx->d_out_c, ctx->d_out_x, s);

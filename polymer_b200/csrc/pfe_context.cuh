@@ -40,13 +40,17 @@ struct ClassLaunch {
   int* d_nchunks;
   int4* chunks;  // (bra pair, first ket, end ket, 0)
   double quartets;
-  // interpreted classes: level-scheduled op table and its shared-memory size
-  bool big;
+  // execution variant: 0 = straight-line thread per quartet, 1 = warp per
+  // quartet on the op table, 2 = block per quartet on the op table
+  int variant;
+  bool has_straight, has_table;
   const unsigned short* ops;
   const int* levels;
   const unsigned short* out;
   int nlevels, nout, nslots;
-  size_t smem;
+  int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
+  size_t smem_big, smem_warp;
+  float tuned_ms[3];         // autotuner timings per variant (0 = not run)
 };
 
 struct QuartetLaunch {
@@ -112,9 +116,12 @@ struct pfe_context {
 
   // per-launch timing (pfe_context_profile)
   bool profile = false;
+  bool tuned = false;
   cudaEvent_t ev[130] = {};
   int nev = 0;
   int ev_cls[64] = {0};
+  int ev_variant[64] = {0};
+  float ev_tuned[64][3] = {};
   double ev_quartets[64] = {0}, ev_flops[64] = {0};
   int nprof = 0;
 
@@ -156,6 +163,11 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a);
 int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s);
 int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, double* d_cc, double* d_xc,
                      bool symmetrize, int ncell, cudaStream_t s);
+int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s);
+struct OpTableDev;
+const struct OpTableHost* host_optable(int cb, int ck);
+int upload_optable(pfe_context* ctx, const struct OpTableHost* h, OpTableDev* d);
+double class_flops(int cb, int ck);
 int lattice_setup(pfe_context* ctx, const pfe_args* a);
 int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, double* d_cc, double* d_xc,
                  cudaStream_t s);

@@ -29,6 +29,7 @@
 
 #include "pfe_common.cuh"
 #include "pfe_context.cuh"
+#include "pfe_interp.cuh"
 #include "generated/eri_classes.cuh"
 
 namespace pfe {
@@ -41,40 +42,6 @@ int upload_constants(int) { return PFE_OK; }  // constants are static-initialise
 // ------------------------------------------------------------------ pair build
 
 // class index of a canonical pair (LA >= LB): 00,10,11,20,21,22
-__host__ __device__ inline int pair_class(int la, int lb) { return la * (la + 1) / 2 + lb; }
-
-template <int LA, int LB>
-__device__ double schwarz_pair(const double* __restrict__ tab, double zeta, double S, const double PA[3],
-                               const double AB[3], const int* __restrict__ pa, const int* __restrict__ pb,
-                               const double* __restrict__ maxc) {
-  constexpr int NA = ncum(LA), NB = ncum(LB);
-  // (ab|ab) at T = 0: F_m = C2/(2m+1), C2 = 2 sqrt(rho/PI) S^2, rho = zeta/2
-  const double rho = 0.5 * zeta;
-  const double c2 = 2.0 * sqrt(rho / REF_PI) * S * S;
-  if (LA + LB == 0) return sqrt(c2 * maxc[pa[0]] * maxc[pb[0]]);
-  double F[2 * (LA + LB) + 1];
-#pragma unroll
-  for (int m = 0; m <= 2 * (LA + LB); ++m) F[m] = c2 / (double)(2 * m + 1);
-  EriGeom<double> g;
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    g.PA[k] = PA[k]; g.QC[k] = PA[k]; g.AB[k] = AB[k]; g.CD[k] = AB[k]; g.WP[k] = 0.0; g.WQ[k] = 0.0;
-  }
-  g.oz = 0.5 / zeta; g.oe = 0.5 / zeta; g.oze = 0.25 / zeta; g.roz = 0.5; g.roe = 0.5;
-  double out[NA * NB * NA * NB];
-  eri_dispatch<LA, LB, LA, LB>(F, g, out);
-  double best = 0.0;
-#pragma unroll 1
-  for (int a = 0; a < NA; ++a)
-    for (int b = 0; b < NB; ++b) {
-      if (a == 0 && b == 0) continue;  // component 1 is excluded (src/pfourindexdirect.f90:356,455)
-      const int ia = pa[a], ib = pb[b];
-      const double ma = ia >= 0 ? maxc[ia] : 0.0, mb = ib >= 0 ? maxc[ib] : 0.0;
-      const double v = sqrt(out[((a * NB + b) * NA + a) * NB + b] * ma * mb);
-      if (v > best) best = v;
-    }
-  return best;
-}
 
 // One thread per unordered shell pair t in [0, n(n+1)/2).
 __global__ void k_build_pairs(DevShells sh, const double* __restrict__ sss, const double* __restrict__ tab,
@@ -183,9 +150,6 @@ struct Digest {
   double jab[NA * NB], jcd[NC * ND], kad[NA * ND], kbd[NB * ND], kac[NA * NC], kbc[NB * NC];
 };
 
-__device__ __forceinline__ double dens_at(const double* __restrict__ D, int npgs, int i, int j) {
-  return (i >= 0 && j >= 0) ? __ldg(D + i + (size_t)npgs * j) : 0.0;
-}
 
 // One primitive-shell quartet per lane; a warp shares one bra pair.
 template <int LA, int LB, int LC, int LD>
@@ -321,49 +285,6 @@ __global__ void __launch_bounds__(128) k_quartets(QuartetLaunch ql) {
 
 // ---------------------------------------------- interpreted (large) classes
 
-struct OpTableDev {
-  const unsigned short* ops;
-  const int* levels;
-  const unsigned short* out;
-  int nlevels, nout, nslots;
-};
-
-// Geometry multipliers of the four op kinds, in shared memory.
-struct OpGeom {
-  double G1[4][3], G2[4][3];
-  double X[4], Y[4], Z;
-};
-
-__device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restrict__ v, const OpGeom& geo,
-                                            int base) {
-  for (int l = 0; l < t.nlevels; ++l) {
-    const int o0 = t.levels[l], o1 = t.levels[l + 1];
-    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-      const unsigned short* op = t.ops + 6 * o;
-      const int h = op[0];
-      const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-      double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-      if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-      if (cB) val += (double)cB * geo.Z * v[op[5]];
-      v[base + o] = val;
-    }
-    __syncthreads();
-  }
-}
-
-__device__ inline void set_geom(OpGeom& g, const double PA[3], const double WP[3], const double QC[3],
-                                const double WQ[3], const double AB[3], const double CD[3], double oz, double oe,
-                                double oze, double roz, double roe) {
-  for (int k = 0; k < 3; ++k) {
-    g.G1[0][k] = PA[k]; g.G2[0][k] = WP[k];
-    g.G1[1][k] = QC[k]; g.G2[1][k] = WQ[k];
-    g.G1[2][k] = 1.0;   g.G2[2][k] = AB[k];
-    g.G1[3][k] = 1.0;   g.G2[3][k] = CD[k];
-  }
-  g.X[0] = oz; g.Y[0] = roz; g.X[1] = oe; g.Y[1] = roe; g.X[2] = g.X[3] = 0.0; g.Y[2] = g.Y[3] = 0.0;
-  g.Z = oze;
-}
-
 // One quartet at a time per block; ops of a dependency level run in parallel.
 template <int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(256) k_quartets_big(QuartetLaunch ql, OpTableDev tab) {
@@ -489,50 +410,152 @@ __global__ void __launch_bounds__(256) k_quartets_big(QuartetLaunch ql, OpTableD
   }
 }
 
-// Schwarz bound of the (21) and (22) pair classes on the interpreter: one block per pair.
-template <int LA, int LB>
-__global__ void __launch_bounds__(256) k_schwarz_big(PairArrays pr, const int* __restrict__ prim,
-                                                     const double* __restrict__ maxc, const int* __restrict__ list,
-                                                     int n, OpTableDev tab) {
-  constexpr int NA = ncum(LA), NB = ncum(LB);
+// One quartet per warp, several warps per block: the level-scheduled op table
+// runs across the 32 lanes with __syncwarp between dependency levels; the
+// Boys values are computed one order per lane; digestion targets are spread
+// over the lanes.  Per-warp shared memory: the op-table slots and the six
+// density blocks.
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(256) k_quartets_warp(QuartetLaunch ql, OpTableDev tab, int per_warp) {
+  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
+  constexpr int LT = LA + LB + LC + LD;
+  constexpr int NT = NA * NB + NC * ND + (NA + NB) * (NC + ND);
+  constexpr int NPRM = NA + NB + NC + ND;
   extern __shared__ double smem[];
-  double* v = smem;
-  __shared__ OpGeom geo;
-  __shared__ double best[256];
-  for (int w = blockIdx.x; w < n; w += gridDim.x) {
-    const int t = list[w];
-    const double z = pr.zeta[t], S = pr.S[t];
-    if (threadIdx.x == 0) {
-      const double rho = 0.5 * z, c2 = 2.0 * sqrt(rho / REF_PI) * S * S;
-      v[0] = 0.0;
-      for (int m = 0; m <= 2 * (LA + LB); ++m) v[1 + m] = c2 / (double)(2 * m + 1);
-      double PA[3], AB[3], Z0[3] = {0.0, 0.0, 0.0};
-      for (int k = 0; k < 3; ++k) { PA[k] = pr.PA[k][t]; AB[k] = pr.AB[k][t]; }
-      set_geom(geo, PA, Z0, PA, Z0, AB, AB, 0.5 / z, 0.5 / z, 0.25 / z, 0.5, 0.5);
+  __shared__ OpGeom s_geo[8];
+  __shared__ int s_prm[8][NPRM];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  double* v = smem + (size_t)wid * per_warp;
+  double* Pab = v + tab.nslots;
+  double* Pcd = Pab + NA * NB;
+  double* Pac = Pcd + NC * ND;
+  double* Pad = Pac + NA * NC;
+  double* Pbc = Pad + NA * ND;
+  double* Pbd = Pbc + NB * NC;
+  OpGeom& geo = s_geo[wid];
+  int* pa = s_prm[wid];
+  int* pb = pa + NA;
+  int* pc = pb + NB;
+  int* pd = pc + NC;
+  const PairArrays pr = ql.pairs;
+  const int npgs = ql.npgs;
+  const double* __restrict__ D = ql.density;
+  const int nchunks = *ql.nchunks;
+  const double c2pi = 2.0 / sqrt(REF_PI);
+  const int base = LT + 2;
+  const int stride = gridDim.x * wpb * ql.numprocs;
+  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
+    const int4 ch = ql.chunks[c];
+    const int p = ch.x;
+    const int I = pr.si[p], J = pr.sj[p];
+    for (int x = lane; x < NA; x += 32) pa[x] = ql.prim[I * MAXCOMP + x];
+    for (int x = lane; x < NB; x += 32) pb[x] = ql.prim[J * MAXCOMP + x];
+    __syncwarp();
+    for (int t = lane; t < NA * NB; t += 32) Pab[t] = dens_at(D, npgs, pa[t / NB], pb[t % NB]);
+    const double zb = pr.zeta[p];
+    const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
+    for (int qq = ch.y; qq < ch.z; ++qq) {
+      const double ze = pr.zeta[qq];
+      const double Qx = pr.P[0][qq], Qy = pr.P[1][qq], Qz = pr.P[2][qq];
+      const double zz = zb + ze, rho = zb * ze / zz;
+      const double T = rho * ((Px - Qx) * (Px - Qx) + (Py - Qy) * (Py - Qy) + (Pz - Qz) * (Pz - Qz));
+      const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
+      const int K = pr.si[qq], L = pr.sj[qq];
+      if (lane == 0) {
+        double F[LT + 1];
+        boys_tab<LT>(T, pref, ql.boys, F);
+        v[0] = 0.0;
+#pragma unroll
+        for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
+      } else if (lane == 1) {
+        const double W[3] = {(zb * Px + ze * Qx) / zz, (zb * Py + ze * Qy) / zz, (zb * Pz + ze * Qz) / zz};
+        const double Pv[3] = {Px, Py, Pz}, Qv[3] = {Qx, Qy, Qz};
+        double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
+        for (int k = 0; k < 3; ++k) {
+          PA[k] = pr.PA[k][p]; QC[k] = pr.PA[k][qq]; AB[k] = pr.AB[k][p]; CD[k] = pr.AB[k][qq];
+          WP[k] = W[k] - Pv[k]; WQ[k] = W[k] - Qv[k];
+        }
+        set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
+      }
+      for (int x = lane; x < NC; x += 32) pc[x] = ql.prim[K * MAXCOMP + x];
+      for (int x = lane; x < ND; x += 32) pd[x] = ql.prim[L * MAXCOMP + x];
+      __syncwarp();
+      for (int t = lane; t < NC * ND; t += 32) Pcd[t] = dens_at(D, npgs, pc[t / ND], pd[t % ND]);
+      for (int t = lane; t < NA * NC; t += 32) Pac[t] = dens_at(D, npgs, pa[t / NC], pc[t % NC]);
+      for (int t = lane; t < NA * ND; t += 32) Pad[t] = dens_at(D, npgs, pa[t / ND], pd[t % ND]);
+      for (int t = lane; t < NB * NC; t += 32) Pbc[t] = dens_at(D, npgs, pb[t / NC], pc[t % NC]);
+      for (int t = lane; t < NB * ND; t += 32) Pbd[t] = dens_at(D, npgs, pb[t / ND], pd[t % ND]);
+      for (int l = 0; l < tab.nlevels; ++l) {
+        const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
+        for (int o = o0 + lane; o < o1; o += 32) {
+          const unsigned short* op = tab.ops + 6 * o;
+          const int h = op[0];
+          const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
+          double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
+          if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
+          if (cB) val += (double)cB * geo.Z * v[op[5]];
+          v[base + o] = val;
+        }
+        __syncwarp();
+      }
+      const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
+      const double wj = 0.25 * deg, wk = 0.125 * deg;
+      const unsigned short* __restrict__ out = tab.out;
+      for (int t = lane; t < NT; t += 32) {
+        double acc = 0.0;
+        int r = t;
+        if (r < NA * NB) {
+          const int a = r / NB, b = r % NB;
+          for (int cc = 0; cc < NC; ++cc)
+            for (int d = 0; d < ND; ++d) acc += Pcd[cc * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pa[a] >= 0 && pb[b] >= 0) atomicAdd(ql.jp + pa[a] + (size_t)npgs * pb[b], acc * wj);
+          continue;
+        }
+        r -= NA * NB;
+        if (r < NC * ND) {
+          const int cc = r / ND, d = r % ND;
+          for (int a = 0; a < NA; ++a)
+            for (int b = 0; b < NB; ++b) acc += Pab[a * NB + b] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pc[cc] >= 0 && pd[d] >= 0) atomicAdd(ql.jp + pc[cc] + (size_t)npgs * pd[d], acc * wj);
+          continue;
+        }
+        r -= NC * ND;
+        if (r < NA * ND) {
+          const int a = r / ND, d = r % ND;
+          for (int b = 0; b < NB; ++b)
+            for (int cc = 0; cc < NC; ++cc) acc += Pbc[b * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pa[a] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pd[d], acc * wk);
+          continue;
+        }
+        r -= NA * ND;
+        if (r < NB * ND) {
+          const int b = r / ND, d = r % ND;
+          for (int a = 0; a < NA; ++a)
+            for (int cc = 0; cc < NC; ++cc) acc += Pac[a * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pb[b] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pd[d], acc * wk);
+          continue;
+        }
+        r -= NB * ND;
+        if (r < NA * NC) {
+          const int a = r / NC, cc = r % NC;
+          for (int b = 0; b < NB; ++b)
+            for (int d = 0; d < ND; ++d) acc += Pbd[b * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pa[a] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pc[cc], acc * wk);
+          continue;
+        }
+        r -= NA * NC;
+        {
+          const int b = r / NC, cc = r % NC;
+          for (int a = 0; a < NA; ++a)
+            for (int d = 0; d < ND; ++d) acc += Pad[a * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
+          if (pb[b] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pc[cc], acc * wk);
+        }
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    run_optable(tab, v, geo, 2 * (LA + LB) + 2);
-    const int I = pr.si[t], J = pr.sj[t];
-    double b = 0.0;
-    for (int x = threadIdx.x; x < NA * NB; x += blockDim.x) {
-      const int a = x / NB, bb = x % NB;
-      if (a == 0 && bb == 0) continue;
-      const int ia = prim[I * MAXCOMP + a], ib = prim[J * MAXCOMP + bb];
-      const double ma = ia >= 0 ? maxc[ia] : 0.0, mb = ib >= 0 ? maxc[ib] : 0.0;
-      const double val = sqrt(v[tab.out[((a * NB + bb) * NA + a) * NB + bb]] * ma * mb);
-      b = fmax(b, val);
-    }
-    best[threadIdx.x] = b;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0.0;
-      for (int k = 0; k < (int)blockDim.x; ++k) m = fmax(m, best[k]);
-      pr.schwarz[t] = m;
-      pr.key[t] = ~(unsigned long long)__double_as_longlong(m);
-    }
-    __syncthreads();
   }
 }
+
 
 // M (+)= A + A^T for n x n column-major matrices, batched over cells
 __global__ void k_symmetrize(const double* __restrict__ a, double* __restrict__ out, int n, int ncell) {
@@ -567,21 +590,36 @@ static LaunchFn launcher(int cb, int ck) {
   return table[cb][ck];
 }
 
-static const OpTableHost* host_optable(int cb, int ck) {
+const OpTableHost* host_optable(int cb, int ck) {
   switch (cb * 8 + ck) {
+    case 1 * 8 + 0: return &op_1000;
+    case 1 * 8 + 1: return &op_1010;
+    case 2 * 8 + 0: return &op_1100;
+    case 2 * 8 + 1: return &op_1110;
+    case 2 * 8 + 2: return &op_1111;
+    case 3 * 8 + 0: return &op_2000;
+    case 3 * 8 + 1: return &op_2010;
+    case 3 * 8 + 2: return &op_2011;
+    case 3 * 8 + 3: return &op_2020;
+    case 4 * 8 + 0: return &op_2100;
+    case 4 * 8 + 1: return &op_2110;
     case 4 * 8 + 2: return &op_2111;
     case 4 * 8 + 3: return &op_2120;
     case 4 * 8 + 4: return &op_2121;
+    case 5 * 8 + 0: return &op_2200;
     case 5 * 8 + 1: return &op_2210;
     case 5 * 8 + 2: return &op_2211;
     case 5 * 8 + 3: return &op_2220;
     case 5 * 8 + 4: return &op_2221;
     case 5 * 8 + 5: return &op_2222;
+    case 0: return &op_0000;
     default: return nullptr;
   }
 }
 
 using BigFn = void (*)(const QuartetLaunch&, const OpTableDev&, int grid, size_t smem, cudaStream_t);
+using WarpFn = void (*)(const QuartetLaunch&, const OpTableDev&, int grid, int wpb, int per_warp, size_t smem,
+                        cudaStream_t);
 
 template <int LA, int LB, int LC, int LD>
 static void launch_big(const QuartetLaunch& ql, const OpTableDev& t, int grid, size_t smem, cudaStream_t s) {
@@ -589,47 +627,65 @@ static void launch_big(const QuartetLaunch& ql, const OpTableDev& t, int grid, s
 }
 
 template <int LA, int LB, int LC, int LD>
-static cudaError_t allow_smem(size_t smem) {
-  return cudaFuncSetAttribute(k_quartets_big<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+static void launch_warp(const QuartetLaunch& ql, const OpTableDev& t, int grid, int wpb, int per_warp, size_t smem,
+                        cudaStream_t s) {
+  k_quartets_warp<LA, LB, LC, LD><<<grid, 32 * wpb, smem, s>>>(ql, t, per_warp);
 }
 
-static BigFn big_launcher(int cb, int ck) {
-  switch (cb * 8 + ck) {
-    case 4 * 8 + 2: return &launch_big<2, 1, 1, 1>;
-    case 4 * 8 + 3: return &launch_big<2, 1, 2, 0>;
-    case 4 * 8 + 4: return &launch_big<2, 1, 2, 1>;
-    case 5 * 8 + 1: return &launch_big<2, 2, 1, 0>;
-    case 5 * 8 + 2: return &launch_big<2, 2, 1, 1>;
-    case 5 * 8 + 3: return &launch_big<2, 2, 2, 0>;
-    case 5 * 8 + 4: return &launch_big<2, 2, 2, 1>;
-    case 5 * 8 + 5: return &launch_big<2, 2, 2, 2>;
-    default: return nullptr;
-  }
+template <int LA, int LB, int LC, int LD>
+static cudaError_t allow_smem_both(size_t big, size_t warp) {
+  cudaError_t e = cudaFuncSetAttribute(k_quartets_big<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_quartets_warp<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp);
 }
 
-static cudaError_t big_allow_smem(int cb, int ck, size_t smem) {
+struct Variants {
+  BigFn big;
+  WarpFn warp;
+  cudaError_t (*allow)(size_t, size_t);
+};
+
+static Variants variants(int cb, int ck) {
+#define V(A, B, C, D) Variants{&launch_big<A, B, C, D>, &launch_warp<A, B, C, D>, &allow_smem_both<A, B, C, D>}
   switch (cb * 8 + ck) {
-    case 4 * 8 + 2: return allow_smem<2, 1, 1, 1>(smem);
-    case 4 * 8 + 3: return allow_smem<2, 1, 2, 0>(smem);
-    case 4 * 8 + 4: return allow_smem<2, 1, 2, 1>(smem);
-    case 5 * 8 + 1: return allow_smem<2, 2, 1, 0>(smem);
-    case 5 * 8 + 2: return allow_smem<2, 2, 1, 1>(smem);
-    case 5 * 8 + 3: return allow_smem<2, 2, 2, 0>(smem);
-    case 5 * 8 + 4: return allow_smem<2, 2, 2, 1>(smem);
-    case 5 * 8 + 5: return allow_smem<2, 2, 2, 2>(smem);
-    default: return cudaSuccess;
+    case 0: return V(0, 0, 0, 0);
+    case 1 * 8 + 0: return V(1, 0, 0, 0);
+    case 1 * 8 + 1: return V(1, 0, 1, 0);
+    case 2 * 8 + 0: return V(1, 1, 0, 0);
+    case 2 * 8 + 1: return V(1, 1, 1, 0);
+    case 2 * 8 + 2: return V(1, 1, 1, 1);
+    case 3 * 8 + 0: return V(2, 0, 0, 0);
+    case 3 * 8 + 1: return V(2, 0, 1, 0);
+    case 3 * 8 + 2: return V(2, 0, 1, 1);
+    case 3 * 8 + 3: return V(2, 0, 2, 0);
+    case 4 * 8 + 0: return V(2, 1, 0, 0);
+    case 4 * 8 + 1: return V(2, 1, 1, 0);
+    case 4 * 8 + 2: return V(2, 1, 1, 1);
+    case 4 * 8 + 3: return V(2, 1, 2, 0);
+    case 4 * 8 + 4: return V(2, 1, 2, 1);
+    case 5 * 8 + 0: return V(2, 2, 0, 0);
+    case 5 * 8 + 1: return V(2, 2, 1, 0);
+    case 5 * 8 + 2: return V(2, 2, 1, 1);
+    case 5 * 8 + 3: return V(2, 2, 2, 0);
+    case 5 * 8 + 4: return V(2, 2, 2, 1);
+    case 5 * 8 + 5: return V(2, 2, 2, 2);
+    default: return Variants{nullptr, nullptr, nullptr};
   }
+#undef V
+}
+
+static int density_block_doubles(int cb, int ck) {
+  static const int Lc[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  const int NA = ncum(Lc[cb][0]), NB = ncum(Lc[cb][1]), NC = ncum(Lc[ck][0]), ND = ncum(Lc[ck][1]);
+  return NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
 }
 
 static size_t big_smem_bytes(int cb, int ck, const OpTableHost* h) {
-  static const int Lc[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
-  const int NA = ncum(Lc[cb][0]), NB = ncum(Lc[cb][1]), NC = ncum(Lc[ck][0]), ND = ncum(Lc[ck][1]);
-  const int np = NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
-  return sizeof(double) * ((size_t)h->nslots + np);
+  return sizeof(double) * ((size_t)h->nslots + density_block_doubles(cb, ck));
 }
 
 // Upload an op table once per context; returns the device view.
-static int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
+int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   unsigned short *ops = nullptr, *out = nullptr;
   int* lev = nullptr;
   PFE_CUDA(ctx->alloc((void**)&ops, sizeof(unsigned short) * 6 * h->nops));
@@ -788,15 +844,26 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
       ClassLaunch cl{};
       cl.cb = cb;
       cl.ck = ck;
+      cl.has_straight = launcher(cb, ck) != nullptr;
+      cl.has_table = false;
+      cl.variant = 0;
       if (const OpTableHost* h = host_optable(cb, ck)) {
         OpTableDev d{};
         if ((rc = upload_optable(ctx, h, &d)) != PFE_OK) return rc;
-        cl.big = true;
+        cl.has_table = true;
         cl.ops = d.ops; cl.levels = d.levels; cl.out = d.out;
         cl.nlevels = d.nlevels; cl.nout = d.nout; cl.nslots = d.nslots;
-        cl.smem = big_smem_bytes(cb, ck, h);
-        PFE_CUDA(big_allow_smem(cb, ck, cl.smem));
+        cl.smem_big = big_smem_bytes(cb, ck, h);
+        cl.per_warp = h->nslots + density_block_doubles(cb, ck);
+        const size_t limit = 200 * 1024;
+        cl.wpb = (int)std::max<size_t>(1, std::min<size_t>(8, limit / (sizeof(double) * cl.per_warp)));
+        cl.smem_warp = sizeof(double) * (size_t)cl.per_warp * cl.wpb;
+        PFE_CUDA(variants(cb, ck).allow(cl.smem_big, cl.smem_warp));
+        // default before tuning: straight-line for small classes, else one quartet per warp
+        const int ni = h->nout;
+        cl.variant = (cl.has_straight && ni <= 100) ? 0 : (sizeof(double) * cl.per_warp <= 100 * 1024 ? 1 : 2);
       }
+      for (int v = 0; v < 3; ++v) cl.tuned_ms[v] = 0.f;
       cl.nchunks_host = total;
       cl.quartets = (double)nq;
       PFE_CUDA(ctx->alloc((void**)&cl.chunks, sizeof(int4) * total));
@@ -824,6 +891,75 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
   return PFE_OK;
 }
 
+static void launch_class(pfe_context* ctx, const ClassLaunch& cl, const QuartetLaunch& ql, int variant, cudaStream_t s) {
+  const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
+  if (variant == 0 || !cl.has_table) {
+    int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
+    launcher(cl.cb, cl.ck)(ql, std::max(grid, 1), s);
+    return;
+  }
+  OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
+  if (variant == 1) {
+    int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
+    variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);
+  } else {
+    int grid = std::min(work, ctx->num_sms * 2);
+    variants(cl.cb, cl.ck).big(ql, t, std::max(grid, 1), cl.smem_big, s);
+  }
+}
+
+// Time every available variant of every class launch on the real chunk lists
+// and keep the fastest (run once per set-up, before the first timed build).
+int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
+  const size_t pp = (size_t)ctx->npgs * ctx->npgs;
+  QuartetLaunch ql{};
+  ql.pairs = ctx->pairs;
+  ql.prim = ctx->shells.prim;
+  ql.boys = ctx->d_boys;
+  ql.density = d_pp;
+  ql.jp = ctx->d_jp;
+  ql.kp = ctx->d_kp;
+  ql.npgs = ctx->npgs;
+  ql.myid = ctx->myid;
+  ql.numprocs = ctx->numprocs;
+  cudaEvent_t e0, e1;
+  PFE_CUDA(cudaEventCreate(&e0));
+  PFE_CUDA(cudaEventCreate(&e1));
+  for (int i = 0; i < ctx->nlaunch; ++i) {
+    ClassLaunch& cl = ctx->launches[i];
+    ql.chunks = cl.chunks;
+    ql.nchunks = cl.d_nchunks;
+    float best = 1e30f;
+    int bestv = cl.variant;
+    for (int v = 0; v < 3; ++v) {
+      if ((v == 0 && !cl.has_straight) || (v > 0 && !cl.has_table)) continue;
+      if (v == 1 && sizeof(double) * (size_t)cl.per_warp > 200 * 1024) continue;
+      launch_class(ctx, cl, ql, v, s);  // warm-up
+      float t = 1e30f;
+      for (int r = 0; r < 2; ++r) {
+        PFE_CUDA(cudaEventRecord(e0, s));
+        launch_class(ctx, cl, ql, v, s);
+        PFE_CUDA(cudaEventRecord(e1, s));
+        PFE_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t = std::min(t, ms);
+      }
+      PFE_CUDA(cudaGetLastError());
+      cl.tuned_ms[v] = t;
+      if (t < best) { best = t; bestv = v; }
+    }
+    cl.variant = bestv;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, sizeof(double) * pp, s));
+  PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, sizeof(double) * pp, s));
+  PFE_CUDA(cudaStreamSynchronize(s));
+  ctx->tuned = true;
+  return PFE_OK;
+}
+
 int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s) {
   const size_t pp = (size_t)ctx->npgs * ctx->npgs;
   PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, sizeof(double) * pp, s));
@@ -848,25 +984,15 @@ int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d
     const ClassLaunch& cl = ctx->launches[i];
     ql.chunks = cl.chunks;
     ql.nchunks = cl.d_nchunks;
-    const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
-    if (cl.big) {
-      OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
-      int grid = std::min(work, ctx->num_sms * 2);
-      if (grid < 1) grid = 1;
-      big_launcher(cl.cb, cl.ck)(ql, t, grid, cl.smem, s);
-    } else {
-      int grid = (work + 3) / 4;
-      const int cap = ctx->num_sms * 16;
-      if (grid > cap) grid = cap;
-      if (grid < 1) grid = 1;
-      launcher(cl.cb, cl.ck)(ql, grid, s);
-    }
+    launch_class(ctx, cl, ql, cl.variant, s);
     PFE_CUDA(cudaGetLastError());
     if (ctx->profile) {
       PFE_CUDA(cudaEventRecord(ctx->ev[i + 1], s));
       ctx->ev_cls[i] = 1000 * kClassL[cl.cb][0] + 100 * kClassL[cl.cb][1] + 10 * kClassL[cl.ck][0] + kClassL[cl.ck][1];
       ctx->ev_quartets[i] = cl.quartets;
       ctx->ev_flops[i] = cl.quartets * class_flops(cl.cb, cl.ck);
+      ctx->ev_variant[i] = cl.variant;
+      for (int v = 0; v < 3; ++v) ctx->ev_tuned[i][v] = cl.tuned_ms[v];
     }
   }
   return contract_outputs(ctx, ctx->d_jp, ctx->d_kp, d_cc, d_xc, /*symmetrize=*/true, 1, s);

@@ -93,6 +93,15 @@ class DeviceFock:
         return {'quartets': c.quartets, 'quartets_ref': c.quartets_ref, 'flops': c.flops,
                 'quartets_fp32': c.quartets_fp32, 'pairs': c.pairs, 'kernel_launches': c.kernel_launches}
 
+    def autotune(self, p_p: torch.Tensor) -> None:
+        """Pick the fastest execution variant per quartet class on this density (cell-major)."""
+        pp = p_p.transpose(-1, -2).contiguous()
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(self.L, self.L.pfe_context_autotune(self.ctx, ctypes.c_void_p(pp.data_ptr()), None, ctypes.c_void_p(s)))
+
+    def force_variant(self, v: int) -> None:
+        check(self.L, self.L.pfe_context_force_variant(self.ctx, v))
+
     def run_fortran(self, d_pp: torch.Tensor, d_pph: Optional[torch.Tensor], out_c: torch.Tensor,
                     out_x: torch.Tensor, stream=None) -> None:
         """Raw call on Fortran-layout device buffers (no layout conversion)."""

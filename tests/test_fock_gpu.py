@@ -70,6 +70,20 @@ def test_alkane_screened_matches_oracle(n, inttol):
     _assert_close(x_gpu, x_ref, 'X_C')
 
 
+@pytest.mark.parametrize('variant', [0, 1, 2])
+def test_every_execution_variant_matches_oracle(variant):
+    """Straight-line, warp-per-quartet and block-per-quartet schedules all agree."""
+    s = _sys(geometry.alkane_deck(2, inttol=1e-12))
+    _, pp = _random_density(s, seed=5)
+    c_ref, x_ref = oracle.fourindex_eri(s, pp)
+    df = fock.DeviceFock(s)
+    df.force_variant(variant)
+    c_d, x_d = df(torch.tensor(pp, device='cuda'))
+    torch.cuda.synchronize()
+    _assert_close(c_d.cpu().numpy(), c_ref, 'C_C variant %d' % variant)
+    _assert_close(x_d.cpu().numpy(), x_ref, 'X_C variant %d' % variant)
+
+
 def test_device_path_matches_host_path(water):
     pc, pp = _random_density(water, seed=3)
     c_h, x_h = fock.fourindex_eri(water, pp)
