@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -17,16 +18,6 @@
 namespace pfe {
 
 // ------------------------------------------------------------------ helpers
-
-__global__ void k_gather_u8(const unsigned char* __restrict__ src, const int* __restrict__ perm,
-                            unsigned char* __restrict__ dst, long long n) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t < n) dst[t] = src[perm[t]];
-}
-
-void thrust_gather_u8(const unsigned char* src, const int* perm, unsigned char* dst, long long n, cudaStream_t s) {
-  k_gather_u8<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, perm, dst, n);
-}
 
 int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n) {
   for (int k = 0; k < 3; ++k) {
@@ -41,6 +32,8 @@ int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n) {
   PFE_CUDA(ctx->alloc((void**)&pa->sj, sizeof(int) * n));
   PFE_CUDA(ctx->alloc((void**)&pa->cls, n));
   PFE_CUDA(ctx->alloc((void**)&pa->key, sizeof(unsigned long long) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->gid, sizeof(int) * n));
+  PFE_CUDA(ctx->alloc((void**)&pa->gmax, sizeof(double) * n));
   return PFE_OK;
 }
 
@@ -57,6 +50,8 @@ void free_pairs(pfe_context* ctx, PairArrays* pa) {
   ctx->free_now(pa->sj);
   ctx->free_now(pa->cls);
   ctx->free_now(pa->key);
+  ctx->free_now(pa->gid);
+  ctx->free_now(pa->gmax);
   *pa = PairArrays{};
 }
 
@@ -192,6 +187,9 @@ static void reset_context(pfe_context* ctx) {
   ctx->pairs = PairArrays{};
   ctx->d_sss = ctx->d_boys = ctx->d_maxc = ctx->d_cc = ctx->d_c2h = nullptr;
   ctx->d_jp = ctx->d_kp = ctx->d_w1 = ctx->d_w2 = nullptr;
+  ctx->d_tidx = nullptr;
+  ctx->d_tcoef = nullptr;
+  ctx->d_blk = nullptr;
   ctx->d_pp = ctx->d_pph = ctx->d_out_c = ctx->d_out_x = nullptr;
   ctx->pp_bytes = ctx->pph_bytes = ctx->out_bytes = 0;
   ctx->nlaunch = 0;
@@ -273,6 +271,57 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
     const int nq = 2 * (a->cel2[0] + a->cel1[0]) + 1;
     PFE_CUDA(ctx->alloc((void**)&ctx->d_c2h, sizeof(double) * (size_t)a->ncgs * a->ncgs * nq));
     PFE_CUDA(cudaMemcpy(ctx->d_c2h, a->c2h, sizeof(double) * (size_t)a->ncgs * a->ncgs * nq, cudaMemcpyHostToDevice));
+  }
+  // digestion targets and contracted blocks
+  {
+    std::vector<int> tidx(a->npgs, -1);
+    std::vector<double> tcoef(a->npgs, 0.0);
+    bool single = true;
+    for (int p = 0; p < a->npgs; ++p) {
+      int nz = 0;
+      for (int r = 0; r < a->ncgs; ++r) {
+        const double v = a->cc[r + (size_t)a->ncgs * p];
+        if (v != 0.0) {
+          ++nz;
+          tidx[p] = r;
+          tcoef[p] = v;
+        }
+      }
+      if (nz > 1) single = false;
+    }
+    ctx->contracted = single && ctx->molecular;
+    if (!ctx->contracted) {
+      for (int p = 0; p < a->npgs; ++p) {
+        const bool ghost = tidx[p] < 0;
+        tidx[p] = ghost ? -1 : p;
+        tcoef[p] = ghost ? 0.0 : 1.0;
+      }
+    }
+    ctx->nt = ctx->contracted ? a->ncgs : a->npgs;
+    // contracted block of a shell: the tuple of target rows of its components
+    std::map<std::vector<int>, int> keys;
+    std::vector<int> blk(a->npshell);
+    for (int sh = 0; sh < a->npshell; ++sh) {
+      std::vector<int> key;
+      key.push_back(hs.L[sh]);
+      for (int c = 0; c < ncum(hs.L[sh]); ++c) {
+        const int p = hs.prim[(size_t)sh * MAXCOMP + c];
+        key.push_back(ctx->contracted ? tidx[p] : p);
+      }
+      auto it = keys.emplace(key, (int)keys.size()).first;
+      blk[sh] = it->second;
+    }
+    ctx->nblk = (int)keys.size();
+    if ((long long)ctx->nblk * ctx->nblk > (1LL << 30)) {
+      set_error("too many shells for the block-pair index (more than 32768 distinct shells)");
+      return PFE_EINVAL;
+    }
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_tidx, sizeof(int) * a->npgs));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_tcoef, sizeof(double) * a->npgs));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_blk, sizeof(int) * a->npshell));
+    PFE_CUDA(cudaMemcpy(ctx->d_tidx, tidx.data(), sizeof(int) * a->npgs, cudaMemcpyHostToDevice));
+    PFE_CUDA(cudaMemcpy(ctx->d_tcoef, tcoef.data(), sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+    PFE_CUDA(cudaMemcpy(ctx->d_blk, blk.data(), sizeof(int) * a->npshell, cudaMemcpyHostToDevice));
   }
   // accumulators and GEMM scratch
   const size_t pp = (size_t)a->npgs * a->npgs * ctx->ncell1;

@@ -19,7 +19,7 @@ struct DevShells {
   int* prim;  // n * MAXCOMP, 0-based primitive of each cumulative component (-1 ghost/absent)
 };
 
-// Shell-pair records, struct of arrays; sorted by (class, Schwarz descending) after setup.
+// Shell-pair records, struct of arrays; sorted by class and bound after setup.
 struct PairArrays {
   double* P[3];
   double* PA[3];
@@ -31,6 +31,8 @@ struct PairArrays {
   int* sj;
   unsigned char* cls;
   unsigned long long* key;
+  int* gid;         // contracted block pair (molecules)
+  double* gmax;     // largest bound in the pair's block-pair group (molecules)
 };
 
 // One launch of the quartet kernel: a (bra class, ket class) pair and its chunks.
@@ -51,19 +53,6 @@ struct ClassLaunch {
   int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
   size_t smem_big, smem_warp;
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
-};
-
-struct QuartetLaunch {
-  PairArrays pairs;
-  const int* prim;
-  const double* boys;     // IGAMMA row-major [T][m]
-  const double* density;  // P_P (npgs x npgs, column-major)
-  double* jp;             // J' accumulator (primitive, column-major)
-  double* kp;             // K' accumulator
-  const int4* chunks;
-  const int* nchunks;
-  int npgs;
-  int myid, numprocs;
 };
 
 }  // namespace pfe
@@ -95,6 +84,14 @@ struct pfe_context {
   double* d_c2h = nullptr;
   double* d_jp = nullptr;
   double* d_kp = nullptr;
+  // digestion targets: contracted functions when every primitive feeds at most
+  // one contracted row of CC (the reference's READ3 bases), else primitives
+  bool contracted = false;
+  int nt = 0;                // target dimension (ncgs or npgs)
+  int* d_tidx = nullptr;     // primitive -> target row, -1 when it has no coefficient
+  double* d_tcoef = nullptr; // primitive -> coefficient (CC entry, or 1)
+  int* d_blk = nullptr;      // shell -> contracted block id
+  int nblk = 0;
   double* d_w1 = nullptr;
   double* d_w2 = nullptr;
   pfe::PairArrays pairs{};
@@ -157,7 +154,8 @@ struct pfe_context {
 namespace pfe {
 int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n);
 void free_pairs(pfe_context* ctx, PairArrays* pa);
-void thrust_gather_u8(const unsigned char* src, const int* perm, unsigned char* dst, long long n, cudaStream_t s);
+void launch_symmetrize(const double* a, double* out, int n, int ncell, cudaStream_t s);
+void launch_select_class(const unsigned char* cls, int want, int* list, int* count, long long n, cudaStream_t s);
 int upload_constants(int device);
 int molecular_setup(pfe_context* ctx, const pfe_args* a);
 int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s);

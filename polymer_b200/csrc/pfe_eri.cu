@@ -2,23 +2,12 @@
 // include/polymer_fock.h.  Replaces SUBROUTINE FOURINDEX_ERI
 // (src/pfourindexdirect.f90:1-814).
 //
-// Device pipeline (molecules, all cells 0, HELIX 0):
-//   setup  : primitive-shell table -> every unordered shell pair built on the
-//            device with its Schwarz bound (the reference's rule: max over
-//            components but the first of sqrt((ab|ab) maxc_a maxc_b),
-//            src/pfourindexdirect.f90:326-363) -> CUB sort by (class, bound
-//            descending) -> per class pair, the INTTOL-screened triangle of
-//            quartets cut into 32-ket chunks (src/pfourindexdirect.f90:529).
-//   build  : one kernel per quartet class (LA LB|LC LD) <= (22|22): a warp takes
-//            a chunk (one bra pair, up to 32 ket pairs), each lane one primitive
-//            shell quartet: tabulated Boys function, generated HGP recursion,
-//            digestion into primitive J'/K' with 8-fold permutational symmetry
-//            (bra J warp-reduced, the rest FP64 atomics), then
-//            C_C = CC (J'+J'^T) CC^T and X_C likewise on cuBLAS.
-// Lattices and helices take the general path of pfe_lattice.cu.
+// This file holds what both build paths share: the error string, the op-table
+// registry of the generated recursion, the CC contraction of primitive J'/K'
+// on cuBLAS, and the FP64 peak probe.  The molecular path is pfe_mol.cu, the
+// lattice / helical path pfe_lattice.cu.
 
 #include <cublas_v2.h>
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <cstdio>
@@ -39,526 +28,8 @@ void set_error(const std::string& msg) { g_err = msg; }
 
 int upload_constants(int) { return PFE_OK; }  // constants are static-initialised
 
-// ------------------------------------------------------------------ pair build
-
-// class index of a canonical pair (LA >= LB): 00,10,11,20,21,22
-
-// One thread per unordered shell pair t in [0, n(n+1)/2).
-__global__ void k_build_pairs(DevShells sh, const double* __restrict__ sss, const double* __restrict__ tab,
-                              const double* __restrict__ maxc, PairArrays out, int* __restrict__ class_count,
-                              long long npairs) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= npairs) return;
-  // decode t -> (i >= j)
-  long long i = (long long)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-  while ((i + 1) * (i + 2) / 2 <= t) ++i;
-  while (i * (i + 1) / 2 > t) --i;
-  int I = (int)i, J = (int)(t - i * (i + 1) / 2);
-  // canonical order: higher L on the first centre; equal L keeps I >= J
-  if (sh.L[J] > sh.L[I]) { int x = I; I = J; J = x; }
-  const double za = sh.zeta[I], zb = sh.zeta[J];
-  const double ax = sh.x[I], ay = sh.y[I], az = sh.z[I];
-  const double bx = sh.x[J], by = sh.y[J], bz = sh.z[J];
-  const double z = za + zb;
-  const double px = (ax * za + bx * zb) / z, py = (ay * za + by * zb) / z, pz = (az * za + bz * zb) / z;
-  const double S = sss[(size_t)I + (size_t)sh.n * J];  // S_P(head I, head J) at cell 0
-  const double PA[3] = {px - ax, py - ay, pz - az}, AB[3] = {ax - bx, ay - by, az - bz};
-  const int la = sh.L[I], lb = sh.L[J];
-  const int* pa = sh.prim + (size_t)I * MAXCOMP;
-  const int* pb = sh.prim + (size_t)J * MAXCOMP;
-  double sch = 0.0;
-  switch (pair_class(la, lb)) {
-    case 0: sch = schwarz_pair<0, 0>(tab, z, S, PA, AB, pa, pb, maxc); break;
-    case 1: sch = schwarz_pair<1, 0>(tab, z, S, PA, AB, pa, pb, maxc); break;
-    case 2: sch = schwarz_pair<1, 1>(tab, z, S, PA, AB, pa, pb, maxc); break;
-    case 3: sch = schwarz_pair<2, 0>(tab, z, S, PA, AB, pa, pb, maxc); break;
-    default: sch = 0.0; break;  // (21) and (22) pairs: k_schwarz_big fills the bound
-  }
-  out.P[0][t] = px; out.P[1][t] = py; out.P[2][t] = pz;
-  out.PA[0][t] = PA[0]; out.PA[1][t] = PA[1]; out.PA[2][t] = PA[2];
-  out.AB[0][t] = AB[0]; out.AB[1][t] = AB[1]; out.AB[2][t] = AB[2];
-  out.zeta[t] = z;
-  out.S[t] = S;
-  out.schwarz[t] = sch;
-  out.si[t] = I;
-  out.sj[t] = J;
-  const int cls = pair_class(la, lb);
-  out.cls[t] = (unsigned char)cls;
-  // descending bound as an ascending key: positive doubles order like their bits
-  out.key[t] = ~(unsigned long long)__double_as_longlong(sch);
-  atomicAdd(class_count + cls, 1);
-}
-
-__global__ void k_gather_pairs(PairArrays src, PairArrays dst, const int* __restrict__ perm, long long n) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int s = perm[t];
-  for (int k = 0; k < 3; ++k) {
-    dst.P[k][t] = src.P[k][s];
-    dst.PA[k][t] = src.PA[k][s];
-    dst.AB[k][t] = src.AB[k][s];
-  }
-  dst.zeta[t] = src.zeta[s];
-  dst.S[t] = src.S[s];
-  dst.schwarz[t] = src.schwarz[s];
-  dst.si[t] = src.si[s];
-  dst.sj[t] = src.sj[s];
-  dst.cls[t] = src.cls[s];
-}
-
-__global__ void k_iota(int* p, long long n) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t < n) p[t] = (int)t;
-}
-
-// ------------------------------------------------------------- chunk lists
-
-// For each bra pair p of class cb: number of ket pairs q of class ck (sorted by
-// descending bound) with bound_p*bound_q >= INTTOL -- the reference's screen
-// kept as the same floating-point product -- and, for cb == ck, q <= p.
-__global__ void k_count_chunks(const double* __restrict__ sch, int b0, int nb, int k0, int nk, bool same,
-                               double inttol, int* __restrict__ nvalid, int* __restrict__ nchunk) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nb) return;
-  const double sp = sch[b0 + p];
-  int lo = 0, hi = nk;  // first q with sp*sq < inttol
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (sp * sch[k0 + mid] < inttol) hi = mid; else lo = mid + 1;
-  }
-  int nv = lo;
-  if (same && nv > p + 1) nv = p + 1;
-  nvalid[p] = nv;
-  nchunk[p] = (nv + 31) >> 5;
-}
-
-__global__ void k_fill_chunks(const int* __restrict__ nvalid, const int* __restrict__ off, int b0, int k0, int nb,
-                              int4* __restrict__ chunks) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nb) return;
-  const int nv = nvalid[p];
-  int o = off[p];
-  for (int q = 0; q < nv; q += 32, ++o) chunks[o] = make_int4(b0 + p, k0 + q, k0 + min(q + 32, nv), 0);
-}
-
-// ------------------------------------------------------------- quartet kernel
-
-template <int NA, int NB, int NC, int ND>
-struct Digest {
-  // density sub-blocks the digestion reads, and the six partial sums it writes
-  double Pab[NA * NB], Pcd[NC * ND], Pac[NA * NC], Pad[NA * ND], Pbc[NB * NC], Pbd[NB * ND];
-  double jab[NA * NB], jcd[NC * ND], kad[NA * ND], kbd[NB * ND], kac[NA * NC], kbc[NB * NC];
-};
-
-
-// One primitive-shell quartet per lane; a warp shares one bra pair.
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) k_quartets(QuartetLaunch ql) {
-  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
-  constexpr int NI = NA * NB * NC * ND;
-  constexpr int LT = LA + LB + LC + LD;
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
-  const int nchunks = *ql.nchunks;
-  const int stride = gridDim.x * wpb * ql.numprocs;
-  const double c2pi = 2.0 / sqrt(REF_PI);
-  const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs;
-  const double* __restrict__ D = ql.density;
-  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
-    const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    const int q = ch.y + lane;
-    const bool act = q < ch.z;
-    const int qq = act ? q : ch.y;
-    const double zb = pr.zeta[p], ze = pr.zeta[qq];
-    const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-    const double Qx = pr.P[0][qq], Qy = pr.P[1][qq], Qz = pr.P[2][qq];
-    const double zz = zb + ze;
-    const double rho = zb * ze / zz;
-    const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
-    const double T = rho * (dx * dx + dy * dy + dz * dz);
-    const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-    double F[LT + 1];
-    boys_tab<LT>(T, pref, ql.boys, F);
-    double out[NI];
-    if constexpr (LT == 0) {
-      out[0] = F[0];
-    } else {
-      EriGeom<double> g;
-      const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
-      g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
-      g.QC[0] = pr.PA[0][qq]; g.QC[1] = pr.PA[1][qq]; g.QC[2] = pr.PA[2][qq];
-      g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
-      g.CD[0] = pr.AB[0][qq]; g.CD[1] = pr.AB[1][qq]; g.CD[2] = pr.AB[2][qq];
-      g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
-      g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
-      g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
-      eri_dispatch<LA, LB, LC, LD>(F, g, out);
-    }
-    // ---- digestion with 8-fold symmetry: weights deg/4 (J') and deg/8 (K')
-    const int I = pr.si[p], J = pr.sj[p], K = pr.si[qq], L = pr.sj[qq];
-    const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-    const double wj = act ? 0.25 * deg : 0.0, wk = act ? 0.125 * deg : 0.0;
-    int pa[NA], pb[NB], pc[NC], pd[ND];
-#pragma unroll
-    for (int x = 0; x < NA; ++x) pa[x] = ql.prim[I * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < NB; ++x) pb[x] = ql.prim[J * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < NC; ++x) pc[x] = ql.prim[K * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < ND; ++x) pd[x] = ql.prim[L * MAXCOMP + x];
-    Digest<NA, NB, NC, ND> dg;
-#pragma unroll
-    for (int a = 0; a < NA; ++a) {
-#pragma unroll
-      for (int b = 0; b < NB; ++b) { dg.Pab[a * NB + b] = dens_at(D, npgs, pa[a], pb[b]); dg.jab[a * NB + b] = 0.0; }
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc) { dg.Pac[a * NC + cc] = dens_at(D, npgs, pa[a], pc[cc]); dg.kac[a * NC + cc] = 0.0; }
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pad[a * ND + d] = dens_at(D, npgs, pa[a], pd[d]); dg.kad[a * ND + d] = 0.0; }
-    }
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc) { dg.Pbc[b * NC + cc] = dens_at(D, npgs, pb[b], pc[cc]); dg.kbc[b * NC + cc] = 0.0; }
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pbd[b * ND + d] = dens_at(D, npgs, pb[b], pd[d]); dg.kbd[b * ND + d] = 0.0; }
-    }
-#pragma unroll
-    for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pcd[cc * ND + d] = dens_at(D, npgs, pc[cc], pd[d]); dg.jcd[cc * ND + d] = 0.0; }
-#pragma unroll
-    for (int a = 0; a < NA; ++a)
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            const double v = out[((a * NB + b) * NC + cc) * ND + d];
-            dg.jab[a * NB + b] += dg.Pcd[cc * ND + d] * v;
-            dg.jcd[cc * ND + d] += dg.Pab[a * NB + b] * v;
-            dg.kad[a * ND + d] += dg.Pbc[b * NC + cc] * v;
-            dg.kbd[b * ND + d] += dg.Pac[a * NC + cc] * v;
-            dg.kac[a * NC + cc] += dg.Pbd[b * ND + d] * v;
-            dg.kbc[b * NC + cc] += dg.Pad[a * ND + d] * v;
-          }
-#pragma unroll
-    for (int a = 0; a < NA; ++a)
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-        double acc = dg.jab[a * NB + b] * wj;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0 && pa[a] >= 0 && pb[b] >= 0) atomicAdd(ql.jp + pa[a] + (size_t)npgs * pb[b], acc);
-      }
-    if (act) {
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-        for (int d = 0; d < ND; ++d)
-          if (pc[cc] >= 0 && pd[d] >= 0) atomicAdd(ql.jp + pc[cc] + (size_t)npgs * pd[d], dg.jcd[cc * ND + d] * wj);
-#pragma unroll
-      for (int a = 0; a < NA; ++a) {
-#pragma unroll
-        for (int d = 0; d < ND; ++d)
-          if (pa[a] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pd[d], dg.kad[a * ND + d] * wk);
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc)
-          if (pa[a] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pc[cc], dg.kac[a * NC + cc] * wk);
-      }
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-#pragma unroll
-        for (int d = 0; d < ND; ++d)
-          if (pb[b] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pd[d], dg.kbd[b * ND + d] * wk);
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc)
-          if (pb[b] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pc[cc], dg.kbc[b * NC + cc] * wk);
-      }
-    }
-  }
-}
-
-// ---------------------------------------------- interpreted (large) classes
-
-// One quartet at a time per block; ops of a dependency level run in parallel.
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(256) k_quartets_big(QuartetLaunch ql, OpTableDev tab) {
-  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
-  constexpr int LT = LA + LB + LC + LD;
-  constexpr int NT = NA * NB + NC * ND + (NA + NB) * (NC + ND);
-  extern __shared__ double smem[];
-  double* v = smem;                              // tab.nslots
-  double* P = smem + tab.nslots;                 // density blocks
-  double* Pab = P;
-  double* Pcd = Pab + NA * NB;
-  double* Pac = Pcd + NC * ND;
-  double* Pad = Pac + NA * NC;
-  double* Pbc = Pad + NA * ND;
-  double* Pbd = Pbc + NB * NC;
-  __shared__ OpGeom geo;
-  __shared__ int prm[NA + NB + NC + ND];
-  __shared__ double s_w[2];
-  const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs;
-  const double* __restrict__ D = ql.density;
-  const int nchunks = *ql.nchunks;
-  const double c2pi = 2.0 / sqrt(REF_PI);
-  const int base = LT + 2;
-  for (int c = blockIdx.x * ql.numprocs + ql.myid; c < nchunks; c += gridDim.x * ql.numprocs) {
-    const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    for (int qq = ch.y; qq < ch.z; ++qq) {
-      if (threadIdx.x == 0) {
-        const double zb = pr.zeta[p], ze = pr.zeta[qq];
-        const double Pv[3] = {pr.P[0][p], pr.P[1][p], pr.P[2][p]};
-        const double Qv[3] = {pr.P[0][qq], pr.P[1][qq], pr.P[2][qq]};
-        const double zz = zb + ze, rho = zb * ze / zz;
-        const double T = rho * ((Pv[0] - Qv[0]) * (Pv[0] - Qv[0]) + (Pv[1] - Qv[1]) * (Pv[1] - Qv[1]) +
-                                (Pv[2] - Qv[2]) * (Pv[2] - Qv[2]));
-        const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-        double F[LT + 1];
-        boys_tab<LT>(T, pref, ql.boys, F);
-        v[0] = 0.0;
-        for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
-        double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
-        for (int k = 0; k < 3; ++k) {
-          const double W = (zb * Pv[k] + ze * Qv[k]) / zz;
-          PA[k] = pr.PA[k][p]; QC[k] = pr.PA[k][qq]; AB[k] = pr.AB[k][p]; CD[k] = pr.AB[k][qq];
-          WP[k] = W - Pv[k]; WQ[k] = W - Qv[k];
-        }
-        set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
-        const int I = pr.si[p], J = pr.sj[p], K = pr.si[qq], L = pr.sj[qq];
-        const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-        s_w[0] = 0.25 * deg;
-        s_w[1] = 0.125 * deg;
-        for (int x = 0; x < NA; ++x) prm[x] = ql.prim[I * MAXCOMP + x];
-        for (int x = 0; x < NB; ++x) prm[NA + x] = ql.prim[J * MAXCOMP + x];
-        for (int x = 0; x < NC; ++x) prm[NA + NB + x] = ql.prim[K * MAXCOMP + x];
-        for (int x = 0; x < ND; ++x) prm[NA + NB + NC + x] = ql.prim[L * MAXCOMP + x];
-      }
-      __syncthreads();
-      const int* pa = prm;
-      const int* pb = prm + NA;
-      const int* pc = prm + NA + NB;
-      const int* pd = prm + NA + NB + NC;
-      for (int t = threadIdx.x; t < NA * NB; t += blockDim.x) Pab[t] = dens_at(D, npgs, pa[t / NB], pb[t % NB]);
-      for (int t = threadIdx.x; t < NC * ND; t += blockDim.x) Pcd[t] = dens_at(D, npgs, pc[t / ND], pd[t % ND]);
-      for (int t = threadIdx.x; t < NA * NC; t += blockDim.x) Pac[t] = dens_at(D, npgs, pa[t / NC], pc[t % NC]);
-      for (int t = threadIdx.x; t < NA * ND; t += blockDim.x) Pad[t] = dens_at(D, npgs, pa[t / ND], pd[t % ND]);
-      for (int t = threadIdx.x; t < NB * NC; t += blockDim.x) Pbc[t] = dens_at(D, npgs, pb[t / NC], pc[t % NC]);
-      for (int t = threadIdx.x; t < NB * ND; t += blockDim.x) Pbd[t] = dens_at(D, npgs, pb[t / ND], pd[t % ND]);
-      run_optable(tab, v, geo, base);  // ends with __syncthreads
-      const double wj = s_w[0], wk = s_w[1];
-      auto V = [&](int a, int b, int cc, int d) -> double { return v[tab.out[((a * NB + b) * NC + cc) * ND + d]]; };
-      for (int t = threadIdx.x; t < NT; t += blockDim.x) {
-        double acc = 0.0;
-        int r = t;
-        if (r < NA * NB) {               // J'(a,b) += P(c,d) v
-          const int a = r / NB, b = r % NB;
-          for (int cc = 0; cc < NC; ++cc)
-            for (int d = 0; d < ND; ++d) acc += Pcd[cc * ND + d] * V(a, b, cc, d);
-          if (pa[a] >= 0 && pb[b] >= 0) atomicAdd(ql.jp + pa[a] + (size_t)npgs * pb[b], acc * wj);
-          continue;
-        }
-        r -= NA * NB;
-        if (r < NC * ND) {               // J'(c,d) += P(a,b) v
-          const int cc = r / ND, d = r % ND;
-          for (int a = 0; a < NA; ++a)
-            for (int b = 0; b < NB; ++b) acc += Pab[a * NB + b] * V(a, b, cc, d);
-          if (pc[cc] >= 0 && pd[d] >= 0) atomicAdd(ql.jp + pc[cc] + (size_t)npgs * pd[d], acc * wj);
-          continue;
-        }
-        r -= NC * ND;
-        if (r < NA * ND) {               // K'(a,d) += P(b,c) v
-          const int a = r / ND, d = r % ND;
-          for (int b = 0; b < NB; ++b)
-            for (int cc = 0; cc < NC; ++cc) acc += Pbc[b * NC + cc] * V(a, b, cc, d);
-          if (pa[a] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pd[d], acc * wk);
-          continue;
-        }
-        r -= NA * ND;
-        if (r < NB * ND) {               // K'(b,d) += P(a,c) v
-          const int b = r / ND, d = r % ND;
-          for (int a = 0; a < NA; ++a)
-            for (int cc = 0; cc < NC; ++cc) acc += Pac[a * NC + cc] * V(a, b, cc, d);
-          if (pb[b] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pd[d], acc * wk);
-          continue;
-        }
-        r -= NB * ND;
-        if (r < NA * NC) {               // K'(a,c) += P(b,d) v
-          const int a = r / NC, cc = r % NC;
-          for (int b = 0; b < NB; ++b)
-            for (int d = 0; d < ND; ++d) acc += Pbd[b * ND + d] * V(a, b, cc, d);
-          if (pa[a] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pc[cc], acc * wk);
-          continue;
-        }
-        r -= NA * NC;                    // K'(b,c) += P(a,d) v
-        {
-          const int b = r / NC, cc = r % NC;
-          for (int a = 0; a < NA; ++a)
-            for (int d = 0; d < ND; ++d) acc += Pad[a * ND + d] * V(a, b, cc, d);
-          if (pb[b] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pc[cc], acc * wk);
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
-// One quartet per warp, several warps per block: the level-scheduled op table
-// runs across the 32 lanes with __syncwarp between dependency levels; the
-// Boys values are computed one order per lane; digestion targets are spread
-// over the lanes.  Per-warp shared memory: the op-table slots and the six
-// density blocks.
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(256) k_quartets_warp(QuartetLaunch ql, OpTableDev tab, int per_warp) {
-  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
-  constexpr int LT = LA + LB + LC + LD;
-  constexpr int NT = NA * NB + NC * ND + (NA + NB) * (NC + ND);
-  constexpr int NPRM = NA + NB + NC + ND;
-  extern __shared__ double smem[];
-  __shared__ OpGeom s_geo[8];
-  __shared__ int s_prm[8][NPRM];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  double* v = smem + (size_t)wid * per_warp;
-  double* Pab = v + tab.nslots;
-  double* Pcd = Pab + NA * NB;
-  double* Pac = Pcd + NC * ND;
-  double* Pad = Pac + NA * NC;
-  double* Pbc = Pad + NA * ND;
-  double* Pbd = Pbc + NB * NC;
-  OpGeom& geo = s_geo[wid];
-  int* pa = s_prm[wid];
-  int* pb = pa + NA;
-  int* pc = pb + NB;
-  int* pd = pc + NC;
-  const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs;
-  const double* __restrict__ D = ql.density;
-  const int nchunks = *ql.nchunks;
-  const double c2pi = 2.0 / sqrt(REF_PI);
-  const int base = LT + 2;
-  const int stride = gridDim.x * wpb * ql.numprocs;
-  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
-    const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    const int I = pr.si[p], J = pr.sj[p];
-    for (int x = lane; x < NA; x += 32) pa[x] = ql.prim[I * MAXCOMP + x];
-    for (int x = lane; x < NB; x += 32) pb[x] = ql.prim[J * MAXCOMP + x];
-    __syncwarp();
-    for (int t = lane; t < NA * NB; t += 32) Pab[t] = dens_at(D, npgs, pa[t / NB], pb[t % NB]);
-    const double zb = pr.zeta[p];
-    const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-    for (int qq = ch.y; qq < ch.z; ++qq) {
-      const double ze = pr.zeta[qq];
-      const double Qx = pr.P[0][qq], Qy = pr.P[1][qq], Qz = pr.P[2][qq];
-      const double zz = zb + ze, rho = zb * ze / zz;
-      const double T = rho * ((Px - Qx) * (Px - Qx) + (Py - Qy) * (Py - Qy) + (Pz - Qz) * (Pz - Qz));
-      const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-      const int K = pr.si[qq], L = pr.sj[qq];
-      if (lane == 0) {
-        double F[LT + 1];
-        boys_tab<LT>(T, pref, ql.boys, F);
-        v[0] = 0.0;
-#pragma unroll
-        for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
-      } else if (lane == 1) {
-        const double W[3] = {(zb * Px + ze * Qx) / zz, (zb * Py + ze * Qy) / zz, (zb * Pz + ze * Qz) / zz};
-        const double Pv[3] = {Px, Py, Pz}, Qv[3] = {Qx, Qy, Qz};
-        double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
-        for (int k = 0; k < 3; ++k) {
-          PA[k] = pr.PA[k][p]; QC[k] = pr.PA[k][qq]; AB[k] = pr.AB[k][p]; CD[k] = pr.AB[k][qq];
-          WP[k] = W[k] - Pv[k]; WQ[k] = W[k] - Qv[k];
-        }
-        set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
-      }
-      for (int x = lane; x < NC; x += 32) pc[x] = ql.prim[K * MAXCOMP + x];
-      for (int x = lane; x < ND; x += 32) pd[x] = ql.prim[L * MAXCOMP + x];
-      __syncwarp();
-      for (int t = lane; t < NC * ND; t += 32) Pcd[t] = dens_at(D, npgs, pc[t / ND], pd[t % ND]);
-      for (int t = lane; t < NA * NC; t += 32) Pac[t] = dens_at(D, npgs, pa[t / NC], pc[t % NC]);
-      for (int t = lane; t < NA * ND; t += 32) Pad[t] = dens_at(D, npgs, pa[t / ND], pd[t % ND]);
-      for (int t = lane; t < NB * NC; t += 32) Pbc[t] = dens_at(D, npgs, pb[t / NC], pc[t % NC]);
-      for (int t = lane; t < NB * ND; t += 32) Pbd[t] = dens_at(D, npgs, pb[t / ND], pd[t % ND]);
-      for (int l = 0; l < tab.nlevels; ++l) {
-        const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-        for (int o = o0 + lane; o < o1; o += 32) {
-          const unsigned short* op = tab.ops + 6 * o;
-          const int h = op[0];
-          const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-          double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-          if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-          if (cB) val += (double)cB * geo.Z * v[op[5]];
-          v[base + o] = val;
-        }
-        __syncwarp();
-      }
-      const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-      const double wj = 0.25 * deg, wk = 0.125 * deg;
-      const unsigned short* __restrict__ out = tab.out;
-      for (int t = lane; t < NT; t += 32) {
-        double acc = 0.0;
-        int r = t;
-        if (r < NA * NB) {
-          const int a = r / NB, b = r % NB;
-          for (int cc = 0; cc < NC; ++cc)
-            for (int d = 0; d < ND; ++d) acc += Pcd[cc * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pa[a] >= 0 && pb[b] >= 0) atomicAdd(ql.jp + pa[a] + (size_t)npgs * pb[b], acc * wj);
-          continue;
-        }
-        r -= NA * NB;
-        if (r < NC * ND) {
-          const int cc = r / ND, d = r % ND;
-          for (int a = 0; a < NA; ++a)
-            for (int b = 0; b < NB; ++b) acc += Pab[a * NB + b] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pc[cc] >= 0 && pd[d] >= 0) atomicAdd(ql.jp + pc[cc] + (size_t)npgs * pd[d], acc * wj);
-          continue;
-        }
-        r -= NC * ND;
-        if (r < NA * ND) {
-          const int a = r / ND, d = r % ND;
-          for (int b = 0; b < NB; ++b)
-            for (int cc = 0; cc < NC; ++cc) acc += Pbc[b * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pa[a] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pd[d], acc * wk);
-          continue;
-        }
-        r -= NA * ND;
-        if (r < NB * ND) {
-          const int b = r / ND, d = r % ND;
-          for (int a = 0; a < NA; ++a)
-            for (int cc = 0; cc < NC; ++cc) acc += Pac[a * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pb[b] >= 0 && pd[d] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pd[d], acc * wk);
-          continue;
-        }
-        r -= NB * ND;
-        if (r < NA * NC) {
-          const int a = r / NC, cc = r % NC;
-          for (int b = 0; b < NB; ++b)
-            for (int d = 0; d < ND; ++d) acc += Pbd[b * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pa[a] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pa[a] + (size_t)npgs * pc[cc], acc * wk);
-          continue;
-        }
-        r -= NA * NC;
-        {
-          const int b = r / NC, cc = r % NC;
-          for (int a = 0; a < NA; ++a)
-            for (int d = 0; d < ND; ++d) acc += Pad[a * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-          if (pb[b] >= 0 && pc[cc] >= 0) atomicAdd(ql.kp + pb[b] + (size_t)npgs * pc[cc], acc * wk);
-        }
-      }
-      __syncwarp();
-    }
-  }
-}
-
-
-// M (+)= A + A^T for n x n column-major matrices, batched over cells
-__global__ void k_symmetrize(const double* __restrict__ a, double* __restrict__ out, int n, int ncell) {
+// out = A + A^T for n x n column-major matrices, batched over cells
+__global__ void k_symmetrize_impl(const double* __restrict__ a, double* __restrict__ out, int n, int ncell) {
   const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long per = (long long)n * n;
   if (t >= per * ncell) return;
@@ -567,27 +38,20 @@ __global__ void k_symmetrize(const double* __restrict__ a, double* __restrict__ 
   out[t] = a[c * per + i + (long long)n * j] + a[c * per + j + (long long)n * i];
 }
 
-// ---------------------------------------------------------------- host side
-
-using LaunchFn = void (*)(const QuartetLaunch&, int grid, cudaStream_t);
-
-template <int LA, int LB, int LC, int LD>
-static void launch_q(const QuartetLaunch& ql, int grid, cudaStream_t s) {
-  k_quartets<LA, LB, LC, LD><<<grid, 128, 0, s>>>(ql);
+// list the pairs of one class (any order)
+__global__ void k_select_class_impl(const unsigned char* __restrict__ cls, int want, int* __restrict__ list,
+                                    int* __restrict__ count, long long n) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n && cls[t] == want) list[atomicAdd(count, 1)] = (int)t;
 }
 
-static LaunchFn launcher(int cb, int ck) {
-  // classes: 0=(0,0) 1=(1,0) 2=(1,1) 3=(2,0) 4=(2,1) 5=(2,2); cb >= ck; nullptr = interpreted
-#define Q(A, B, C, D) &launch_q<A, B, C, D>
-  static const LaunchFn table[6][6] = {
-      {Q(0, 0, 0, 0), nullptr, nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 0, 0, 0), Q(1, 0, 1, 0), nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 1, 0, 0), Q(1, 1, 1, 0), Q(1, 1, 1, 1), nullptr, nullptr, nullptr},
-      {Q(2, 0, 0, 0), Q(2, 0, 1, 0), Q(2, 0, 1, 1), Q(2, 0, 2, 0), nullptr, nullptr},
-      {Q(2, 1, 0, 0), Q(2, 1, 1, 0), nullptr, nullptr, nullptr, nullptr},
-      {Q(2, 2, 0, 0), nullptr, nullptr, nullptr, nullptr, nullptr}};
-#undef Q
-  return table[cb][ck];
+void launch_symmetrize(const double* a, double* out, int n, int ncell, cudaStream_t s) {
+  const long long t = (long long)n * n * ncell;
+  k_symmetrize_impl<<<(unsigned)((t + 255) / 256), 256, 0, s>>>(a, out, n, ncell);
+}
+
+void launch_select_class(const unsigned char* cls, int want, int* list, int* count, long long n, cudaStream_t s) {
+  k_select_class_impl<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cls, want, list, count, n);
 }
 
 const OpTableHost* host_optable(int cb, int ck) {
@@ -617,73 +81,6 @@ const OpTableHost* host_optable(int cb, int ck) {
   }
 }
 
-using BigFn = void (*)(const QuartetLaunch&, const OpTableDev&, int grid, size_t smem, cudaStream_t);
-using WarpFn = void (*)(const QuartetLaunch&, const OpTableDev&, int grid, int wpb, int per_warp, size_t smem,
-                        cudaStream_t);
-
-template <int LA, int LB, int LC, int LD>
-static void launch_big(const QuartetLaunch& ql, const OpTableDev& t, int grid, size_t smem, cudaStream_t s) {
-  k_quartets_big<LA, LB, LC, LD><<<grid, 256, smem, s>>>(ql, t);
-}
-
-template <int LA, int LB, int LC, int LD>
-static void launch_warp(const QuartetLaunch& ql, const OpTableDev& t, int grid, int wpb, int per_warp, size_t smem,
-                        cudaStream_t s) {
-  k_quartets_warp<LA, LB, LC, LD><<<grid, 32 * wpb, smem, s>>>(ql, t, per_warp);
-}
-
-template <int LA, int LB, int LC, int LD>
-static cudaError_t allow_smem_both(size_t big, size_t warp) {
-  cudaError_t e = cudaFuncSetAttribute(k_quartets_big<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_quartets_warp<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp);
-}
-
-struct Variants {
-  BigFn big;
-  WarpFn warp;
-  cudaError_t (*allow)(size_t, size_t);
-};
-
-static Variants variants(int cb, int ck) {
-#define V(A, B, C, D) Variants{&launch_big<A, B, C, D>, &launch_warp<A, B, C, D>, &allow_smem_both<A, B, C, D>}
-  switch (cb * 8 + ck) {
-    case 0: return V(0, 0, 0, 0);
-    case 1 * 8 + 0: return V(1, 0, 0, 0);
-    case 1 * 8 + 1: return V(1, 0, 1, 0);
-    case 2 * 8 + 0: return V(1, 1, 0, 0);
-    case 2 * 8 + 1: return V(1, 1, 1, 0);
-    case 2 * 8 + 2: return V(1, 1, 1, 1);
-    case 3 * 8 + 0: return V(2, 0, 0, 0);
-    case 3 * 8 + 1: return V(2, 0, 1, 0);
-    case 3 * 8 + 2: return V(2, 0, 1, 1);
-    case 3 * 8 + 3: return V(2, 0, 2, 0);
-    case 4 * 8 + 0: return V(2, 1, 0, 0);
-    case 4 * 8 + 1: return V(2, 1, 1, 0);
-    case 4 * 8 + 2: return V(2, 1, 1, 1);
-    case 4 * 8 + 3: return V(2, 1, 2, 0);
-    case 4 * 8 + 4: return V(2, 1, 2, 1);
-    case 5 * 8 + 0: return V(2, 2, 0, 0);
-    case 5 * 8 + 1: return V(2, 2, 1, 0);
-    case 5 * 8 + 2: return V(2, 2, 1, 1);
-    case 5 * 8 + 3: return V(2, 2, 2, 0);
-    case 5 * 8 + 4: return V(2, 2, 2, 1);
-    case 5 * 8 + 5: return V(2, 2, 2, 2);
-    default: return Variants{nullptr, nullptr, nullptr};
-  }
-#undef V
-}
-
-static int density_block_doubles(int cb, int ck) {
-  static const int Lc[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
-  const int NA = ncum(Lc[cb][0]), NB = ncum(Lc[cb][1]), NC = ncum(Lc[ck][0]), ND = ncum(Lc[ck][1]);
-  return NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
-}
-
-static size_t big_smem_bytes(int cb, int ck, const OpTableHost* h) {
-  return sizeof(double) * ((size_t)h->nslots + density_block_doubles(cb, ck));
-}
-
 // Upload an op table once per context; returns the device view.
 int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   unsigned short *ops = nullptr, *out = nullptr;
@@ -701,301 +98,6 @@ int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   d->nout = h->nout;
   d->nslots = h->nslots;
   return PFE_OK;
-}
-
-__global__ void k_select_class(const unsigned char* __restrict__ cls, int want, int* __restrict__ list,
-                               int* __restrict__ count, long long n) {
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (t < n && cls[t] == want) list[atomicAdd(count, 1)] = (int)t;
-}
-
-static const int kClassL[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
-
-double class_flops(int cb, int ck);  // generated table, pfe_flops.cpp
-
-int molecular_setup(pfe_context* ctx, const pfe_args* a) {
-  cudaStream_t s = ctx->stream;
-  const int nsh = ctx->npshell;
-  const long long npairs = (long long)nsh * (nsh + 1) / 2;
-  ctx->npairs = npairs;
-  PairArrays raw{}, sorted{};
-  int rc;
-  if ((rc = alloc_pairs(ctx, &raw, npairs)) != PFE_OK) return rc;
-  if ((rc = alloc_pairs(ctx, &ctx->pairs, npairs)) != PFE_OK) return rc;
-  sorted = ctx->pairs;
-  int* d_count = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&d_count, sizeof(int) * 8));
-  PFE_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int) * 8, s));
-  {
-    const int bs = 128;
-    const long long nb = (npairs + bs - 1) / bs;
-    k_build_pairs<<<(unsigned)nb, bs, 0, s>>>(ctx->shells, ctx->d_sss, ctx->d_boys, ctx->d_maxc, raw, d_count, npairs);
-    PFE_CUDA(cudaGetLastError());
-  }
-  // bounds of the (21) and (22) pair classes on the interpreter
-  {
-    int* list = nullptr;
-    int* cnt = nullptr;
-    PFE_CUDA(ctx->alloc((void**)&list, sizeof(int) * npairs));
-    PFE_CUDA(ctx->alloc((void**)&cnt, sizeof(int)));
-    for (int cls = 4; cls <= 5; ++cls) {
-      PFE_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int), s));
-      k_select_class<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(raw.cls, cls, list, cnt, npairs);
-      int hn = 0;
-      PFE_CUDA(cudaMemcpyAsync(&hn, cnt, sizeof(int), cudaMemcpyDeviceToHost, s));
-      PFE_CUDA(cudaStreamSynchronize(s));
-      if (hn == 0) continue;
-      const OpTableHost* h = host_optable(cls, cls);
-      OpTableDev d{};
-      if ((rc = upload_optable(ctx, h, &d)) != PFE_OK) return rc;
-      const size_t smem = sizeof(double) * (size_t)h->nslots;
-      if (cls == 4) {
-        PFE_CUDA(cudaFuncSetAttribute(k_schwarz_big<2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_schwarz_big<2, 1><<<std::min(hn, 4 * ctx->num_sms), 256, smem, s>>>(raw, ctx->shells.prim, ctx->d_maxc, list, hn, d);
-      } else {
-        PFE_CUDA(cudaFuncSetAttribute(k_schwarz_big<2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_schwarz_big<2, 2><<<std::min(hn, 4 * ctx->num_sms), 256, smem, s>>>(raw, ctx->shells.prim, ctx->d_maxc, list, hn, d);
-      }
-      PFE_CUDA(cudaGetLastError());
-      PFE_CUDA(cudaStreamSynchronize(s));
-    }
-    ctx->free_now(list);
-    ctx->free_now(cnt);
-  }
-  // sort: stable by key (bound descending), then stable by class
-  int *perm_a = nullptr, *perm_b = nullptr;
-  unsigned long long* key_b = nullptr;
-  unsigned char* cls_b = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&perm_a, sizeof(int) * npairs));
-  PFE_CUDA(ctx->alloc((void**)&perm_b, sizeof(int) * npairs));
-  PFE_CUDA(ctx->alloc((void**)&key_b, sizeof(unsigned long long) * npairs));
-  PFE_CUDA(ctx->alloc((void**)&cls_b, npairs));
-  k_iota<<<(unsigned)((npairs + 255) / 256), 256, 0, s>>>(perm_a, npairs);
-  size_t tmp_bytes = 0, tmp2 = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, raw.key, key_b, perm_a, perm_b, (int)npairs, 0, 64, s);
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp2, raw.cls, cls_b, perm_a, perm_b, (int)npairs, 0, 8, s);
-  tmp_bytes = std::max(tmp_bytes, tmp2);
-  void* d_tmp = nullptr;
-  PFE_CUDA(ctx->alloc(&d_tmp, tmp_bytes + 16));
-  PFE_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, raw.key, key_b, perm_a, perm_b, (int)npairs, 0, 64, s));
-  // reorder the class bytes by the first permutation, then sort by class (stable)
-  {
-    unsigned char* cls_perm = nullptr;
-    PFE_CUDA(ctx->alloc((void**)&cls_perm, npairs));
-    // gather classes with perm_b
-    PairArrays tmpv = raw;
-    (void)tmpv;
-    thrust_gather_u8(raw.cls, perm_b, cls_perm, npairs, s);
-    PFE_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, cls_perm, cls_b, perm_b, perm_a, (int)npairs, 0, 8, s));
-    ctx->free_later(cls_perm);
-  }
-  k_gather_pairs<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(raw, sorted, perm_a, npairs);
-  PFE_CUDA(cudaGetLastError());
-  int hcount[8] = {0};
-  PFE_CUDA(cudaMemcpyAsync(hcount, d_count, sizeof(int) * 8, cudaMemcpyDeviceToHost, s));
-  PFE_CUDA(cudaStreamSynchronize(s));
-  int off = 0;
-  for (int c = 0; c < 6; ++c) {
-    ctx->class_off[c] = off;
-    ctx->class_n[c] = hcount[c];
-    off += hcount[c];
-  }
-  // chunk lists for every class pair cb >= ck
-  ctx->nlaunch = 0;
-  ctx->census_quartets = 0.0;
-  ctx->census_flops = 0.0;
-  ctx->census_ref = 0.0;
-  int* nvalid = nullptr;
-  int* nchunk = nullptr;
-  int* offs = nullptr;
-  const int maxn = *std::max_element(ctx->class_n, ctx->class_n + 6);
-  PFE_CUDA(ctx->alloc((void**)&nvalid, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&nchunk, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&offs, sizeof(int) * (maxn + 1)));
-  long long* d_sum = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&d_sum, sizeof(long long) * 2));
-  for (int cb = 0; cb < 6; ++cb)
-    for (int ck = 0; ck <= cb; ++ck) {
-      const int nb = ctx->class_n[cb], nk = ctx->class_n[ck];
-      if (nb == 0 || nk == 0) continue;
-      const int b0 = ctx->class_off[cb], k0 = ctx->class_off[ck];
-      k_count_chunks<<<(nb + 127) / 128, 128, 0, s>>>(ctx->pairs.schwarz, b0, nb, k0, nk, cb == ck, ctx->inttol,
-                                                      nvalid, nchunk);
-      PFE_CUDA(cudaGetLastError());
-      size_t sb = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, sb, nchunk, offs, nb + 1, s);
-      void* st = nullptr;
-      PFE_CUDA(ctx->alloc(&st, sb + 16));
-      PFE_CUDA(cudaMemsetAsync(nchunk + nb, 0, sizeof(int), s));
-      PFE_CUDA(cub::DeviceScan::ExclusiveSum(st, sb, nchunk, offs, nb + 1, s));
-      size_t rb = 0;
-      cub::DeviceReduce::Sum(nullptr, rb, nvalid, d_sum, nb, s);
-      void* rt = nullptr;
-      PFE_CUDA(ctx->alloc(&rt, rb + 16));
-      PFE_CUDA(cub::DeviceReduce::Sum(rt, rb, nvalid, d_sum, nb, s));
-      int total = 0;
-      long long nq = 0;
-      PFE_CUDA(cudaMemcpyAsync(&total, offs + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
-      PFE_CUDA(cudaMemcpyAsync(&nq, d_sum, sizeof(long long), cudaMemcpyDeviceToHost, s));
-      PFE_CUDA(cudaStreamSynchronize(s));
-      ctx->free_now(st);
-      ctx->free_now(rt);
-      if (total == 0) continue;
-      ClassLaunch cl{};
-      cl.cb = cb;
-      cl.ck = ck;
-      cl.has_straight = launcher(cb, ck) != nullptr;
-      cl.has_table = false;
-      cl.variant = 0;
-      if (const OpTableHost* h = host_optable(cb, ck)) {
-        OpTableDev d{};
-        if ((rc = upload_optable(ctx, h, &d)) != PFE_OK) return rc;
-        cl.has_table = true;
-        cl.ops = d.ops; cl.levels = d.levels; cl.out = d.out;
-        cl.nlevels = d.nlevels; cl.nout = d.nout; cl.nslots = d.nslots;
-        cl.smem_big = big_smem_bytes(cb, ck, h);
-        cl.per_warp = h->nslots + density_block_doubles(cb, ck);
-        const size_t limit = 200 * 1024;
-        cl.wpb = (int)std::max<size_t>(1, std::min<size_t>(8, limit / (sizeof(double) * cl.per_warp)));
-        cl.smem_warp = sizeof(double) * (size_t)cl.per_warp * cl.wpb;
-        PFE_CUDA(variants(cb, ck).allow(cl.smem_big, cl.smem_warp));
-        // default before tuning: straight-line for small classes, else one quartet per warp
-        const int ni = h->nout;
-        cl.variant = (cl.has_straight && ni <= 100) ? 0 : (sizeof(double) * cl.per_warp <= 100 * 1024 ? 1 : 2);
-      }
-      for (int v = 0; v < 3; ++v) cl.tuned_ms[v] = 0.f;
-      cl.nchunks_host = total;
-      cl.quartets = (double)nq;
-      PFE_CUDA(ctx->alloc((void**)&cl.chunks, sizeof(int4) * total));
-      PFE_CUDA(ctx->alloc((void**)&cl.d_nchunks, sizeof(int)));
-      PFE_CUDA(cudaMemcpyAsync(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice, s));
-      k_fill_chunks<<<(nb + 127) / 128, 128, 0, s>>>(nvalid, offs, b0, k0, nb, cl.chunks);
-      PFE_CUDA(cudaGetLastError());
-      PFE_CUDA(cudaStreamSynchronize(s));
-      ctx->launches[ctx->nlaunch++] = cl;
-      ctx->census_quartets += (double)nq;
-      ctx->census_flops += (double)nq * class_flops(cb, ck);
-    }
-  ctx->free_now(nvalid);
-  ctx->free_now(nchunk);
-  ctx->free_now(offs);
-  ctx->free_now(d_sum);
-  ctx->free_now(d_tmp);
-  ctx->free_now(perm_a);
-  ctx->free_now(perm_b);
-  ctx->free_now(key_b);
-  ctx->free_now(cls_b);
-  ctx->free_now(d_count);
-  free_pairs(ctx, &raw);
-  ctx->free_pending();
-  return PFE_OK;
-}
-
-static void launch_class(pfe_context* ctx, const ClassLaunch& cl, const QuartetLaunch& ql, int variant, cudaStream_t s) {
-  const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
-  if (variant == 0 || !cl.has_table) {
-    int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
-    launcher(cl.cb, cl.ck)(ql, std::max(grid, 1), s);
-    return;
-  }
-  OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
-  if (variant == 1) {
-    int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
-    variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);
-  } else {
-    int grid = std::min(work, ctx->num_sms * 2);
-    variants(cl.cb, cl.ck).big(ql, t, std::max(grid, 1), cl.smem_big, s);
-  }
-}
-
-// Time every available variant of every class launch on the real chunk lists
-// and keep the fastest (run once per set-up, before the first timed build).
-int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
-  const size_t pp = (size_t)ctx->npgs * ctx->npgs;
-  QuartetLaunch ql{};
-  ql.pairs = ctx->pairs;
-  ql.prim = ctx->shells.prim;
-  ql.boys = ctx->d_boys;
-  ql.density = d_pp;
-  ql.jp = ctx->d_jp;
-  ql.kp = ctx->d_kp;
-  ql.npgs = ctx->npgs;
-  ql.myid = ctx->myid;
-  ql.numprocs = ctx->numprocs;
-  cudaEvent_t e0, e1;
-  PFE_CUDA(cudaEventCreate(&e0));
-  PFE_CUDA(cudaEventCreate(&e1));
-  for (int i = 0; i < ctx->nlaunch; ++i) {
-    ClassLaunch& cl = ctx->launches[i];
-    ql.chunks = cl.chunks;
-    ql.nchunks = cl.d_nchunks;
-    float best = 1e30f;
-    int bestv = cl.variant;
-    for (int v = 0; v < 3; ++v) {
-      if ((v == 0 && !cl.has_straight) || (v > 0 && !cl.has_table)) continue;
-      if (v == 1 && sizeof(double) * (size_t)cl.per_warp > 200 * 1024) continue;
-      launch_class(ctx, cl, ql, v, s);  // warm-up
-      float t = 1e30f;
-      for (int r = 0; r < 2; ++r) {
-        PFE_CUDA(cudaEventRecord(e0, s));
-        launch_class(ctx, cl, ql, v, s);
-        PFE_CUDA(cudaEventRecord(e1, s));
-        PFE_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        t = std::min(t, ms);
-      }
-      PFE_CUDA(cudaGetLastError());
-      cl.tuned_ms[v] = t;
-      if (t < best) { best = t; bestv = v; }
-    }
-    cl.variant = bestv;
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, sizeof(double) * pp, s));
-  PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, sizeof(double) * pp, s));
-  PFE_CUDA(cudaStreamSynchronize(s));
-  ctx->tuned = true;
-  return PFE_OK;
-}
-
-int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s) {
-  const size_t pp = (size_t)ctx->npgs * ctx->npgs;
-  PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, sizeof(double) * pp, s));
-  PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, sizeof(double) * pp, s));
-  QuartetLaunch ql{};
-  ql.pairs = ctx->pairs;
-  ql.prim = ctx->shells.prim;
-  ql.boys = ctx->d_boys;
-  ql.density = d_pp;
-  ql.jp = ctx->d_jp;
-  ql.kp = ctx->d_kp;
-  ql.npgs = ctx->npgs;
-  ql.myid = ctx->myid;
-  ql.numprocs = ctx->numprocs;
-  if (ctx->profile) {
-    for (int i = 0; i <= ctx->nlaunch && i < 64; ++i)
-      if (!ctx->ev[i]) PFE_CUDA(cudaEventCreate(&ctx->ev[i]));
-    ctx->nprof = ctx->nlaunch;
-    PFE_CUDA(cudaEventRecord(ctx->ev[0], s));
-  }
-  for (int i = 0; i < ctx->nlaunch; ++i) {
-    const ClassLaunch& cl = ctx->launches[i];
-    ql.chunks = cl.chunks;
-    ql.nchunks = cl.d_nchunks;
-    launch_class(ctx, cl, ql, cl.variant, s);
-    PFE_CUDA(cudaGetLastError());
-    if (ctx->profile) {
-      PFE_CUDA(cudaEventRecord(ctx->ev[i + 1], s));
-      ctx->ev_cls[i] = 1000 * kClassL[cl.cb][0] + 100 * kClassL[cl.cb][1] + 10 * kClassL[cl.ck][0] + kClassL[cl.ck][1];
-      ctx->ev_quartets[i] = cl.quartets;
-      ctx->ev_flops[i] = cl.quartets * class_flops(cl.cb, cl.ck);
-      ctx->ev_variant[i] = cl.variant;
-      for (int v = 0; v < 3; ++v) ctx->ev_tuned[i][v] = cl.tuned_ms[v];
-    }
-  }
-  return contract_outputs(ctx, ctx->d_jp, ctx->d_kp, d_cc, d_xc, /*symmetrize=*/true, 1, s);
 }
 
 int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, double* d_cc, double* d_xc,
@@ -1016,8 +118,7 @@ int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, doubl
                                    (long long)nc * np, ctx->d_cc, nc, 0, &zero, target, nc, (long long)nc * nc, ncell);
     if (st != CUBLAS_STATUS_SUCCESS) { set_error("cublasDgemmStridedBatched (W.CC^T) failed"); return PFE_ECUDA; }
     if (symmetrize) {
-      const long long n = (long long)nc * nc * ncell;
-      k_symmetrize<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ctx->d_w2, dst[o], nc, ncell);
+      launch_symmetrize(ctx->d_w2, dst[o], nc, ncell, s);
       PFE_CUDA(cudaGetLastError());
     }
   }
