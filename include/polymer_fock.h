@@ -157,6 +157,17 @@ int32_t pfe_overlap_kinetic(const pfe_onee_args *a, double *s_p, double *t_p);
 /* NUCLEAR_ATTRACTION(0) (src/ponee.f90:418-603): N_P(npgs,npgs,cells1), host out. */
 int32_t pfe_nuclear_attraction(const pfe_onee_args *a, double *n_p);
 
+/* No counterpart in the reference.  pfe_overlap_kinetic without any device
+ * allocation: for callers that may not allocate device memory while running
+ * (a fixed memory budget, an allocator that owns the device).  Its device data
+ * live in one 16 MiB array compiled into the library, so the inputs and
+ * 2*npgs*npgs*cells1 results must fit there (a 976-primitive molecule does);
+ * larger inputs return PFE_EINVAL with the size needed.  The first call on a
+ * device does the set-up (module load and symbol lookup on that device) and
+ * should come before any stream capture.  Calls share the one buffer per
+ * device, so they are serialised by a lock; host buffers as pfe_overlap_kinetic. */
+int32_t pfe_overlap_kinetic_noalloc(const pfe_onee_args *a, double *s_p, double *t_p);
+
 /* Library version string. */
 const char *pfe_version(void);
 

@@ -116,6 +116,8 @@ def lib(path: str = LIB_PATH):
     L.pfe_overlap_kinetic.restype = ctypes.c_int32
     L.pfe_nuclear_attraction.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp]
     L.pfe_nuclear_attraction.restype = ctypes.c_int32
+    L.pfe_overlap_kinetic_noalloc.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp, _dp]
+    L.pfe_overlap_kinetic_noalloc.restype = ctypes.c_int32
     L.pfe_context_profile.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.pfe_context_profile.restype = ctypes.c_int32
     L.pfe_context_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeKernelStat), ctypes.c_int32]
@@ -148,4 +150,4 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_overlap_kinetic',
            'pfe_nuclear_attraction', 'pfe_context_profile', 'pfe_context_kernel_stats',
            'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
-           'pfe_version']
+           'pfe_version', 'pfe_overlap_kinetic_noalloc']

@@ -9,6 +9,9 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "pfe_common.cuh"
@@ -335,9 +338,111 @@ done:
   return rc;
 }
 
+// ---------------------------------------------------------------- fixed-scratch variant
+//
+// pfe_overlap_kinetic_noalloc runs k_overlap_kinetic with all of its device
+// data (the shell map, centres, exponents and the S_P/T_P results) staged in
+// one statically sized device array of this file instead of cudaMalloc'd
+// buffers, for callers that may not allocate device memory once they are
+// running (a pre-reserved memory budget, a custom allocator that owns the
+// device, a process that must not grow its footprint).  Limit: everything must
+// fit in kNoAllocScratchBytes (16 MiB), i.e. 2*npgs^2*cells + the inputs; a
+// C20H42 6-31G** molecule (976 primitives) fits, larger inputs are refused.
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;          // held for the whole call: calls share the one buffer
+static void* g_noalloc_ptr[64] = {nullptr};
+
+static size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Device address of the scratch on the current device.  The first call on a
+// device does the set-up (loads the module there, looks up the symbol).
+static int noalloc_scratch(void** out) {
+  int dev = 0;
+  PFE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_error("device index out of range"); return PFE_EINVAL; }
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_error(std::string("cudaGetSymbolAddress of the fixed scratch failed: ") + cudaGetErrorString(e));
+      return PFE_ECUDA;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return PFE_OK;
+}
+
+static int onee_noalloc(const pfe_onee_args* a, double* s_p, double* t_p) {
+  if (!a || !s_p || !t_p || a->npgs <= 0 || a->npshell <= 0) { set_error("invalid one-electron arguments"); return PFE_EINVAL; }
+  for (int k = 0; k < 3; ++k)
+    if (a->cel1[k] < 0 || a->cel2[k] < 0) { set_error("negative cutoff"); return PFE_EINVAL; }
+  const long long n1 = (long long)(2 * a->cel1[0] + 1) * (2 * a->cel1[1] + 1) * (2 * a->cel1[2] + 1);
+  const size_t out_n = (size_t)a->npgs * a->npgs * n1;
+  const size_t psz = (size_t)a->npshell * NPOW * NPOW * NPOW;
+  // scratch layout: S_P | T_P | x | y | z | zt | P_SHELL | P_SHELL_ANG
+  const size_t b_out = round256(sizeof(double) * out_n), b_pg = round256(sizeof(double) * a->npgs);
+  const size_t b_ps = round256(sizeof(int) * psz), b_ang = round256(sizeof(int) * a->npshell);
+  const size_t need = 2 * b_out + 4 * b_pg + b_ps + b_ang;
+  if (need > kNoAllocScratchBytes) {
+    char msg[256];
+    std::snprintf(msg, sizeof msg,
+                  "pfe_overlap_kinetic_noalloc: needs %zu bytes of device scratch, the fixed buffer holds %zu "
+                  "(npgs %d, %lld cells); use pfe_overlap_kinetic",
+                  need, kNoAllocScratchBytes, a->npgs, n1);
+    set_error(msg);
+    return PFE_EINVAL;
+  }
+  for (int s = 0; s < a->npshell; ++s)
+    if (a->p_shell_ang[s] < 0 || a->p_shell_ang[s] > LMAX_SUPPORTED) {
+      set_error("P_SHELL_ANG outside the one-electron kernels (s, p, d)");
+      return a->p_shell_ang[s] < 0 ? PFE_EINVAL : PFE_EUNSUPPORTED;
+    }
+  for (size_t i = 0; i < psz; ++i)
+    if (a->p_shell[i] > a->npgs) { set_error("P_SHELL entry beyond NPGS"); return PFE_EINVAL; }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  void* base = nullptr;
+  int rc = noalloc_scratch(&base);
+  if (rc != PFE_OK) return rc;
+  unsigned char* p = static_cast<unsigned char*>(base);
+  double* ds = reinterpret_cast<double*>(p);
+  double* dt = reinterpret_cast<double*>(p + b_out);
+  double* dx = reinterpret_cast<double*>(p + 2 * b_out);
+  double* dy = reinterpret_cast<double*>(p + 2 * b_out + b_pg);
+  double* dz = reinterpret_cast<double*>(p + 2 * b_out + 2 * b_pg);
+  double* dzt = reinterpret_cast<double*>(p + 2 * b_out + 3 * b_pg);
+  int* dps = reinterpret_cast<int*>(p + 2 * b_out + 4 * b_pg);
+  int* dang = reinterpret_cast<int*>(p + 2 * b_out + 4 * b_pg + b_ps);
+  PFE_CUDA(cudaMemcpy(dx, a->pgsx, sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+  PFE_CUDA(cudaMemcpy(dy, a->pgsy, sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+  PFE_CUDA(cudaMemcpy(dz, a->pgsz, sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+  PFE_CUDA(cudaMemcpy(dzt, a->zt, sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
+  PFE_CUDA(cudaMemcpy(dps, a->p_shell, sizeof(int) * psz, cudaMemcpyHostToDevice));
+  PFE_CUDA(cudaMemcpy(dang, a->p_shell_ang, sizeof(int) * a->npshell, cudaMemcpyHostToDevice));
+  // S_P/T_P entries of primitives that no shell component reaches stay zero,
+  // as with the allocating entry point: clear both results first
+  PFE_CUDA(cudaMemset(ds, 0, sizeof(double) * out_n));
+  PFE_CUDA(cudaMemset(dt, 0, sizeof(double) * out_n));
+  OneeDev d{};
+  d.npgs = a->npgs; d.npshell = a->npshell; d.natom = a->natom;
+  d.p_shell = dps; d.ang = dang; d.x = dx; d.y = dy; d.z = dz; d.zt = dzt;
+  for (int k = 0; k < 3; ++k) { d.cel1[k] = a->cel1[k]; d.cel2[k] = a->cel2[k]; d.period[k] = a->period[k]; }
+  d.helix = a->helix;
+  const long long total = (long long)a->npshell * a->npshell * n1;
+  k_overlap_kinetic<<<(unsigned)((total + 127) / 128), 128>>>(d, ds, dt);
+  PFE_CUDA(cudaGetLastError());
+  PFE_CUDA(cudaMemcpy(s_p, ds, sizeof(double) * out_n, cudaMemcpyDeviceToHost));
+  PFE_CUDA(cudaMemcpy(t_p, dt, sizeof(double) * out_n, cudaMemcpyDeviceToHost));
+  return PFE_OK;
+}
+
 }  // namespace pfe
 
 extern "C" {
 int32_t pfe_overlap_kinetic(const pfe_onee_args* a, double* s_p, double* t_p) { return pfe::onee_run(a, s_p, t_p, nullptr); }
 int32_t pfe_nuclear_attraction(const pfe_onee_args* a, double* n_p) { return pfe::onee_run(a, nullptr, nullptr, n_p); }
+int32_t pfe_overlap_kinetic_noalloc(const pfe_onee_args* a, double* s_p, double* t_p) { return pfe::onee_noalloc(a, s_p, t_p); }
 }
