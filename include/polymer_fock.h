@@ -91,10 +91,25 @@ int32_t pfe_context_setup(pfe_context *ctx, const pfe_args *a);
 /*
  * One Fock build with device pointers: d_p_p (and d_p_p_helix when helix != 0)
  * laid out as in pfe_args; d_c_c, d_x_c receive C_C/X_C.  `stream` is a
- * cudaStream_t (NULL = legacy default).  Asynchronous: returns after enqueueing.
+ * cudaStream_t (NULL = legacy default).  Lattices: asynchronous.  Molecules
+ * whose CC gives every primitive at most one contracted function digest in
+ * contracted space and read P_C off P_P; the call then synchronises the stream
+ * to confirm P_P = CC^T P_C CC (the reference's P_P always is) and returns
+ * PFE_EINVAL otherwise (inside a stream capture the confirmation is skipped).
  */
 int32_t pfe_context_fock(pfe_context *ctx, const double *d_p_p, const double *d_p_p_helix,
                          double *d_c_c, double *d_x_c, void *stream);
+
+/* Molecules: the same build from the contracted density d_p_c (ncgs x ncgs,
+ * P_C of src/pdensitymatrix.f90, before DECONTRACT_DENSITYMATRIX), fully
+ * asynchronous.  Replaces DECONTRACT_DENSITYMATRIX + FOURINDEX_ERI. */
+int32_t pfe_context_fock_pc(pfe_context *ctx, const double *d_p_c, double *d_c_c, double *d_x_c, void *stream);
+
+/* Digest into primitive targets (then contract with CC on cuBLAS) even when
+ * contracted targets are possible; takes effect at the next pfe_context_setup.
+ * For callers whose P_P is not a decontracted density.  No counterpart in the
+ * reference. */
+int32_t pfe_context_primitive_targets(pfe_context *ctx, int32_t enable);
 
 /* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */
 typedef struct pfe_census {

@@ -110,6 +110,11 @@ def lib(path: str = LIB_PATH):
     L.pfe_context_fock.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.pfe_context_fock.restype = ctypes.c_int32
+    L.pfe_context_fock_pc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                      ctypes.c_void_p]
+    L.pfe_context_fock_pc.restype = ctypes.c_int32
+    L.pfe_context_primitive_targets.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    L.pfe_context_primitive_targets.restype = ctypes.c_int32
     L.pfe_context_census.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeCensus)]
     L.pfe_context_census.restype = ctypes.c_int32
     L.pfe_overlap_kinetic.argtypes = [ctypes.POINTER(PfeOneeArgs), _dp, _dp]
@@ -150,4 +155,5 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_context_setup', 'pfe_context_fock', 'pfe_context_census', 'pfe_overlap_kinetic',
            'pfe_nuclear_attraction', 'pfe_context_profile', 'pfe_context_kernel_stats',
            'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
-           'pfe_version', 'pfe_overlap_kinetic_noalloc']
+           'pfe_version', 'pfe_overlap_kinetic_noalloc', 'pfe_context_fock_pc',
+           'pfe_context_primitive_targets']

@@ -190,6 +190,13 @@ static void reset_context(pfe_context* ctx) {
   ctx->d_tidx = nullptr;
   ctx->d_tcoef = nullptr;
   ctx->d_blk = nullptr;
+  ctx->d_rep = nullptr;
+  ctx->d_repc = nullptr;
+  ctx->d_pt = nullptr;
+  ctx->d_flag = nullptr;
+  ctx->d_gr_start = ctx->d_gr_n = ctx->d_bk_list = nullptr;
+  ctx->d_gr_max = nullptr;
+  ctx->ngroups = 0;
   ctx->d_pp = ctx->d_pph = ctx->d_out_c = ctx->d_out_x = nullptr;
   ctx->pp_bytes = ctx->pph_bytes = ctx->out_bytes = 0;
   ctx->nlaunch = 0;
@@ -289,7 +296,7 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
       }
       if (nz > 1) single = false;
     }
-    ctx->contracted = single && ctx->molecular;
+    ctx->contracted = single && ctx->molecular && !ctx->force_primitive;
     if (!ctx->contracted) {
       for (int p = 0; p < a->npgs; ++p) {
         const bool ghost = tidx[p] < 0;
@@ -322,6 +329,20 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
     PFE_CUDA(cudaMemcpy(ctx->d_tidx, tidx.data(), sizeof(int) * a->npgs, cudaMemcpyHostToDevice));
     PFE_CUDA(cudaMemcpy(ctx->d_tcoef, tcoef.data(), sizeof(double) * a->npgs, cudaMemcpyHostToDevice));
     PFE_CUDA(cudaMemcpy(ctx->d_blk, blk.data(), sizeof(int) * a->npshell, cudaMemcpyHostToDevice));
+    // representative primitive of every target (largest |coefficient|): P_C(mu,nu) is read
+    // off P_P at the representatives of mu and nu
+    std::vector<int> rep(ctx->nt, -1);
+    std::vector<double> repc(ctx->nt, 0.0);
+    for (int p = 0; p < a->npgs; ++p) {
+      const int r = tidx[p];
+      if (r >= 0 && std::fabs(tcoef[p]) > std::fabs(repc[r])) { rep[r] = p; repc[r] = tcoef[p]; }
+    }
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_rep, sizeof(int) * ctx->nt));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_repc, sizeof(double) * ctx->nt));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_pt, sizeof(double) * (size_t)ctx->nt * ctx->nt));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_flag, sizeof(unsigned int)));
+    PFE_CUDA(cudaMemcpy(ctx->d_rep, rep.data(), sizeof(int) * ctx->nt, cudaMemcpyHostToDevice));
+    PFE_CUDA(cudaMemcpy(ctx->d_repc, repc.data(), sizeof(double) * ctx->nt, cudaMemcpyHostToDevice));
   }
   // accumulators and GEMM scratch
   const size_t pp = (size_t)a->npgs * a->npgs * ctx->ncell1;
@@ -415,8 +436,40 @@ int32_t pfe_context_fock(pfe_context* ctx, const double* d_p_p, const double* d_
   if (ctx->helix != 0.0 && !d_p_p_helix) { set_error("helix != 0 needs P_P_HELIX"); return PFE_EINVAL; }
   PFE_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t s = (cudaStream_t)stream;
-  return ctx->molecular ? molecular_fock(ctx, d_p_p, d_c_c, d_x_c, s)
-                        : lattice_fock(ctx, d_p_p, d_p_p_helix, d_c_c, d_x_c, s);
+  if (!ctx->molecular) return lattice_fock(ctx, d_p_p, d_p_p_helix, d_c_c, d_x_c, s);
+  int rc = molecular_fock(ctx, d_p_p, d_c_c, d_x_c, s);
+  if (rc != PFE_OK || !ctx->contracted) return rc;
+  // contracted targets read P_C off P_P: confirm P_P = CC^T P_C CC (not possible
+  // while the stream is being captured; pfe_context_fock_pc takes P_C itself)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  PFE_CUDA(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return PFE_OK;
+  bool ok = true;
+  if ((rc = molecular_density_ok(ctx, s, &ok)) != PFE_OK) return rc;
+  if (!ok) {
+    set_error("P_P is not the decontraction CC^T P_C CC of a contracted density; set the context up with "
+              "primitive targets (pfe_context_primitive_targets, then pfe_context_setup)");
+    return PFE_EINVAL;
+  }
+  return PFE_OK;
+}
+
+int32_t pfe_context_fock_pc(pfe_context* ctx, const double* d_p_c, double* d_c_c, double* d_x_c, void* stream) {
+  if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
+  if (!d_p_c || !d_c_c || !d_x_c) { set_error("null device pointer"); return PFE_EINVAL; }
+  if (!ctx->molecular) { set_error("pfe_context_fock_pc: molecules only (lattices take P_P and P_P_HELIX)"); return PFE_EUNSUPPORTED; }
+  PFE_CUDA(cudaSetDevice(ctx->device));
+  return molecular_fock_pc(ctx, d_p_c, d_c_c, d_x_c, (cudaStream_t)stream);
+}
+
+int32_t pfe_context_primitive_targets(pfe_context* ctx, int32_t enable) {
+  if (!ctx) { set_error("null context"); return PFE_EINVAL; }
+  if (ctx->force_primitive != (enable != 0)) {
+    ctx->force_primitive = enable != 0;
+    ctx->ready = false;  // the next set-up rebuilds the schedule
+    ctx->key = 0;
+  }
+  return PFE_OK;
 }
 
 int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
@@ -482,6 +535,7 @@ int32_t pfe_measure_fp64_peak(int32_t device, double* tflops) {
 
 static std::mutex g_default_mu;
 static pfe_context* g_default[64] = {nullptr};
+static pfe_context* g_default_prim[64] = {nullptr};  // primitive targets, for P_P that is not decontracted
 
 int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
   std::lock_guard<std::mutex> lock(g_default_mu);
@@ -539,6 +593,23 @@ int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
   rc = ctx->molecular ? molecular_fock(ctx, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, s)
                       : lattice_fock(ctx, ctx->d_pp, d_pph, ctx->d_out_c, ctx->d_out_x, s);
   if (rc != PFE_OK) return rc;
+  bool ok = true;
+  if ((rc = molecular_density_ok(ctx, s, &ok)) != PFE_OK) return rc;
+  if (!ok) {
+    // P_P is not CC^T P_C CC: build with primitive targets, as the reference does
+    if (!g_default_prim[dev]) {
+      if ((rc = pfe_context_create(dev, &g_default_prim[dev])) != PFE_OK) return rc;
+      g_default_prim[dev]->force_primitive = true;
+    }
+    pfe_context* pc = g_default_prim[dev];
+    if (!(pc->ready && pc->key == key)) {
+      if ((rc = setup_impl(pc, a, hs, key)) != PFE_OK) { pc->ready = false; return rc; }
+    }
+    PFE_CUDA(cudaStreamSynchronize(s));
+    if (!pc->tuned && (rc = autotune(pc, ctx->d_pp, pc->stream)) != PFE_OK) return rc;
+    if ((rc = molecular_fock(pc, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, pc->stream)) != PFE_OK) return rc;
+    PFE_CUDA(cudaStreamSynchronize(pc->stream));
+  }
   PFE_CUDA(cudaMemcpyAsync(c_c, ctx->d_out_c, out_bytes, cudaMemcpyDeviceToHost, s));
   PFE_CUDA(cudaMemcpyAsync(x_c, ctx->d_out_x, out_bytes, cudaMemcpyDeviceToHost, s));
   PFE_CUDA(cudaStreamSynchronize(s));

@@ -53,6 +53,7 @@ struct ClassLaunch {
   int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
   size_t smem_big, smem_warp;
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
+  double* xg;                // block variant: per-block X scratch in global memory, or null
 };
 
 }  // namespace pfe
@@ -92,6 +93,17 @@ struct pfe_context {
   double* d_tcoef = nullptr; // primitive -> coefficient (CC entry, or 1)
   int* d_blk = nullptr;      // shell -> contracted block id
   int nblk = 0;
+  bool force_primitive = false;  // set before set-up: primitive targets even when CC allows contracted ones
+  int* d_rep = nullptr;      // target -> representative primitive (largest |coefficient|)
+  double* d_repc = nullptr;  // its coefficient
+  double* d_pt = nullptr;    // density in target space (nt x nt): P_C read off P_P, or P_P
+  unsigned int* d_flag = nullptr;  // set when P_P is not the decontraction of a contracted density
+  // groups: runs of pairs of one contracted block pair (molecules)
+  int ngroups = 0;
+  int* d_gr_start = nullptr;
+  int* d_gr_n = nullptr;
+  double* d_gr_max = nullptr;
+  int* d_bk_list = nullptr;  // group ids ordered by (class, size bucket, group)
   double* d_w1 = nullptr;
   double* d_w2 = nullptr;
   pfe::PairArrays pairs{};
@@ -162,6 +174,8 @@ int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d
 int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, double* d_cc, double* d_xc,
                      bool symmetrize, int ncell, cudaStream_t s);
 int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s);
+int molecular_density_ok(pfe_context* ctx, cudaStream_t s, bool* ok);
+int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
 struct OpTableDev;
 const struct OpTableHost* host_optable(int cb, int ck);
 int upload_optable(pfe_context* ctx, const struct OpTableHost* h, OpTableDev* d);

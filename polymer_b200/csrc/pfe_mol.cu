@@ -1,25 +1,37 @@
 // Molecular path of the Fock build (all cells 0, HELIX 0).
 //
+// Work is organised by contracted shell quartets.  A "group" is the run of
+// primitive-shell pairs of one ordered contracted block pair (the primitive
+// shells of one contracted shell share centre, angular type and target rows);
+// a "group quartet" (G|H) holds every primitive quartet of a bra group and a
+// ket group.
+//
 // Set-up (device):
 //   * every unordered primitive-shell pair, oriented higher L first, then
-//     higher contracted block, then higher shell index, with the reference's
-//     Schwarz bound (component 1 excluded, src/pfourindexdirect.f90:326-363);
-//   * pairs grouped by ordered contracted block pair ("group"): the pairs of a
-//     group feed the same contracted J/K elements;
-//   * sorted by (class, group's largest bound desc, group, bound desc), so the
-//     groups a bra can reach form a prefix of each ket class and the pairs of a
-//     group are adjacent;
-//   * per (bra class, ket class) the screened triangle in 32-ket chunks.
+//     higher block, then higher shell index, with the reference's Schwarz bound
+//     (component 1 excluded, src/pfourindexdirect.f90:326-363);
+//   * pairs sorted by (class, group maximum desc, group, bound desc): groups are
+//     contiguous runs, each sorted by bound, and within a class the groups a
+//     bra can reach form a prefix;
+//   * ket groups of every class listed by size bucket (similar primitive counts
+//     side by side); per (bra class, ket class) chunks of one bra group and up
+//     to 32 ket groups of one bucket, cut by the group maxima (the reference's
+//     screen IJIJ*KLKL < INTTOL, src/pfourindexdirect.f90:529, can only pass
+//     inside that prefix).
 // Build:
-//   * k_quartets (straight-line, one quartet per lane): the reference's screen
-//     IJIJ*KLKL >= INTTOL per lane (src/pfourindexdirect.f90:529); digestion with
-//     8-fold symmetry into contracted targets; lanes of one group reduce with a
-//     segmented warp reduction before one FP64 atomic per segment;
-//   * k_quartets_warp / k_quartets_big (op-table interpreter, one quartet per
-//     warp / block) for the larger classes, accumulating a group's quartets in
-//     registers before its atomics;
+//   * the density in target space: contracted P_C read off P_P at one primitive
+//     per contracted function (checked against every element of P_P), or P_P
+//     itself when CC is a general contraction;
+//   * per class one kernel: every primitive quartet of a group quartet passing
+//     the reference's screen is evaluated (tabulated Boys function, generated
+//     HGP recursion) and contracted, with its coefficients and its 8-fold
+//     symmetry weight, into X(abcd) of the group quartet; X is then digested
+//     once against the target-space density into J'/K' (FP64 atomics; the
+//     bra's J' warp-reduced first).  Straight-line code with one group quartet
+//     per lane, or the op-table interpreter with one (warp) or all (block)
+//     threads per primitive quartet and X in shared memory;
 //   * C_C = J' + J'^T and X_C = K' + K'^T (contracted targets), or the cuBLAS
-//     contraction CC (J'+J'^T) CC^T when CC is a general contraction.
+//     contraction CC (J'+J'^T) CC^T for primitive targets.
 
 #include <cublas_v2.h>
 #include <cub/cub.cuh>
@@ -34,19 +46,25 @@
 
 namespace pfe {
 
+constexpr int NBUCKET = 6;   // ket-group size buckets: 1, 2-3, 4-7, 8-15, 16-31, 32+
+
 struct MolLaunch {
   PairArrays pairs;
-  const int* prim;       // shell components -> primitive
-  const int* tidx;       // primitive -> target row (-1: none)
-  const double* tcoef;   // primitive -> coefficient
+  const int* prim;        // shell components -> primitive
+  const int* tidx;        // primitive -> target row (-1: none)
+  const double* tcoef;    // primitive -> coefficient
   const double* boys;
-  const double* density; // P_P (npgs x npgs, column-major)
-  double* jt;            // J' targets (nt x nt)
-  double* kt;            // K' targets
-  const int4* chunks;    // (bra pair, first ket, end ket, 0)
+  const double* dt;       // density in target space (nt x nt, column-major)
+  double* jt;             // J' targets (nt x nt)
+  double* kt;             // K' targets
+  const int* gr_start;    // group -> first pair
+  const int* gr_n;        // group -> number of pairs
+  const double* gr_max;   // group -> largest bound
+  const int* bk_list;     // ket groups by (class, bucket, group)
+  const int4* chunks;     // (bra group, first list entry, end list entry, 0)
   const int* nchunks;
   double inttol;
-  int npgs, nt;
+  int nt;
   int myid, numprocs;
 };
 
@@ -147,50 +165,146 @@ __global__ void k_mol_gather(PairArrays src, PairArrays dst, const int* __restri
   dst.gmax[t] = src.gmax[s];
 }
 
-// Ket range of bra p: the groups whose largest bound passes the screen with p
-// (a prefix, groups being ordered by that bound), cut at q <= p for one class;
-// also counts the quartets that pass individually.
-__global__ void k_mol_count(const double* __restrict__ sch, const double* __restrict__ gmax, int b0, int nb, int k0,
-                            int nk, bool same, double inttol, int* __restrict__ nrange, int* __restrict__ nchunk,
-                            int* __restrict__ nquart) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nb) return;
-  const double sp = sch[b0 + p];
-  int lo = 0, hi = nk;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (sp * gmax[k0 + mid] < inttol) hi = mid; else lo = mid + 1;
-  }
-  int e = lo;
-  if (same && e > p + 1) e = p + 1;
-  int nq = 0;
-  for (int q = 0; q < e; ++q) nq += (sp * sch[k0 + q] < inttol) ? 0 : 1;
-  nrange[p] = e;
-  nchunk[p] = (e + 31) >> 5;
-  nquart[p] = nq;
+// ------------------------------------------------------------------ groups and chunks
+
+__global__ void k_group_heads(const int* __restrict__ gid, int* __restrict__ head, long long n) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < n) head[t] = (t == 0 || gid[t] != gid[t - 1]) ? 1 : 0;
 }
 
-__global__ void k_mol_fill(const int* __restrict__ nrange, const int* __restrict__ off, int b0, int k0, int nb,
-                           int4* __restrict__ chunks) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nb) return;
-  const int e = nrange[p];
-  int o = off[p];
-  for (int q = 0; q < e; q += 32, ++o) chunks[o] = make_int4(b0 + p, k0 + q, k0 + min(q + 32, e), 0);
+__global__ void k_group_fill(const int* __restrict__ head, const int* __restrict__ gix, const double* __restrict__ sch,
+                             const unsigned char* __restrict__ cls, int* __restrict__ gr_start,
+                             double* __restrict__ gr_max, unsigned char* __restrict__ gr_cls, long long n) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n || !head[t]) return;
+  const int g = gix[t];
+  gr_start[g] = (int)t;
+  gr_max[g] = sch[t];   // a group is sorted by bound, descending
+  gr_cls[g] = cls[t];
+}
+
+__device__ __forceinline__ int size_bucket(int n) { return min(NBUCKET - 1, 31 - __clz(max(n, 1))); }
+
+__global__ void k_group_size(const int* __restrict__ gr_start, const unsigned char* __restrict__ gr_cls, int ngroups,
+                             long long npairs, int* __restrict__ gr_n, unsigned char* __restrict__ bkey) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int n = (int)((g + 1 < ngroups ? (long long)gr_start[g + 1] : npairs) - gr_start[g]);
+  gr_n[g] = n;
+  bkey[g] = (unsigned char)(gr_cls[g] * 8 + size_bucket(n));
+}
+
+struct Segs {
+  int s0[NBUCKET], s1[NBUCKET];
+};
+
+// End (exclusive list position) of the ket groups of bucket segment [s0, s1)
+// that bra group G can reach: group maxima are non-increasing along a segment;
+// for one class only groups up to G itself (the triangle).
+__device__ __forceinline__ int reach_end(const double* __restrict__ gr_max, const int* __restrict__ bk_list, int s0,
+                                         int s1, double gmx, int G, bool same, double inttol) {
+  int lo = s0, hi = s1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (gmx * gr_max[bk_list[mid]] < inttol) hi = mid; else lo = mid + 1;
+  }
+  int e = lo;
+  if (same) {
+    int l2 = s0, h2 = e;
+    while (l2 < h2) {
+      const int mid = (l2 + h2) >> 1;
+      if (bk_list[mid] <= G) l2 = mid + 1; else h2 = mid;
+    }
+    e = l2;
+  }
+  return e;
+}
+
+__global__ void k_chunk_count(const double* __restrict__ gr_max, const int* __restrict__ bk_list, int g0, int ng,
+                              Segs sg, bool same, double inttol, int* __restrict__ nchunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ng) return;
+  const int G = g0 + i;
+  const double gmx = gr_max[G];
+  int n = 0;
+  for (int b = 0; b < NBUCKET; ++b) {
+    if (sg.s0[b] >= sg.s1[b]) continue;
+    const int e = reach_end(gr_max, bk_list, sg.s0[b], sg.s1[b], gmx, G, same, inttol);
+    n += (e - sg.s0[b] + 31) >> 5;
+  }
+  nchunk[i] = n;
+}
+
+__global__ void k_chunk_fill(const double* __restrict__ gr_max, const int* __restrict__ bk_list, int g0, int ng,
+                             Segs sg, bool same, double inttol, const int* __restrict__ off, int4* __restrict__ chunks) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ng) return;
+  const int G = g0 + i;
+  const double gmx = gr_max[G];
+  int o = off[i];
+  for (int b = 0; b < NBUCKET; ++b) {
+    if (sg.s0[b] >= sg.s1[b]) continue;
+    const int e = reach_end(gr_max, bk_list, sg.s0[b], sg.s1[b], gmx, G, same, inttol);
+    for (int k = sg.s0[b]; k < e; k += 32) chunks[o++] = make_int4(G, k, min(k + 32, e), 0);
+  }
+}
+
+// Primitive quartets of every chunk that pass the screen (the census): lane per
+// ket group, binary search over each ket group's bound-sorted pairs.
+__global__ void k_chunk_census(const int4* __restrict__ chunks, int nchunks, const int* __restrict__ bk_list,
+                               const int* __restrict__ gr_start, const int* __restrict__ gr_n,
+                               const double* __restrict__ sch, double inttol, unsigned long long* __restrict__ total) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= nchunks) return;
+  const int4 ch = chunks[c];
+  unsigned long long n = 0;
+  const int li = ch.y + lane;
+  if (li < ch.z) {
+    const int G = ch.x, H = bk_list[li];
+    const int g0 = gr_start[G], gn = gr_n[G], h0 = gr_start[H], hn = gr_n[H];
+    for (int p = g0; p < g0 + gn; ++p) {
+      const double sp = sch[p];
+      const int qe = (G == H) ? p + 1 : h0 + hn;
+      int lo = h0, hi = qe;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (sp * sch[mid] < inttol) hi = mid; else lo = mid + 1;
+      }
+      n += (unsigned long long)(lo - h0);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if (lane == 0 && n) atomicAdd(total, n);
+}
+
+// ------------------------------------------------------------------ density in target space
+
+// P_T(mu, nu) = P_P(r_mu, r_nu) / (c_mu c_nu) at the representative primitives.
+__global__ void k_target_density(const double* __restrict__ pp, int npgs, const int* __restrict__ rep,
+                                 const double* __restrict__ repc, int nt, double* __restrict__ pt) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nt * nt) return;
+  const int mu = (int)(t % nt), nu = (int)(t / nt);
+  const int a = rep[mu], b = rep[nu];
+  pt[t] = (a >= 0 && b >= 0) ? pp[a + (size_t)npgs * b] / (repc[mu] * repc[nu]) : 0.0;
+}
+
+// Every P_P(a,b) must equal c_a c_b P_T(t_a, t_b) (zero for primitives without a
+// coefficient) to rounding; otherwise the flag is raised.
+__global__ void k_check_density(const double* __restrict__ pp, int npgs, const int* __restrict__ tidx,
+                                const double* __restrict__ tcoef, const double* __restrict__ pt, int nt,
+                                unsigned int* __restrict__ flag) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)npgs * npgs) return;
+  const int a = (int)(t % npgs), b = (int)(t / npgs);
+  const int ta = tidx[a], tb = tidx[b];
+  const double want = (ta >= 0 && tb >= 0) ? tcoef[a] * tcoef[b] * pt[ta + (size_t)nt * tb] : 0.0;
+  const double got = pp[t];
+  if (!(fabs(got - want) <= 1e-12 * fmax(fabs(got), fabs(want)))) atomicOr(flag, 1u);
 }
 
 // ------------------------------------------------------------------ digestion helpers
-
-// Sum over the lanes of this lane's segment [lane, seg_end] (segments are
-// contiguous lane ranges); the segment's first lane ends with the full sum.
-__device__ __forceinline__ double seg_sum(double v, int lane, int seg_end) {
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const double w = __shfl_down_sync(0xffffffffu, v, o);
-    if (lane + o <= seg_end) v += w;
-  }
-  return v;
-}
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -202,166 +316,190 @@ __device__ __forceinline__ void add_target(double* __restrict__ M, int nt, int r
   if (r >= 0 && c >= 0 && v != 0.0) atomicAdd(M + r + (size_t)nt * c, v);
 }
 
-template <int NA, int NB, int NC, int ND>
-struct Digest {
-  double Pab[NA * NB], Pcd[NC * ND], Pac[NA * NC], Pad[NA * ND], Pbc[NB * NC], Pbd[NB * ND];
-  double jab[NA * NB], jcd[NC * ND], kad[NA * ND], kbd[NB * ND], kac[NA * NC], kbc[NB * NC];
-};
+__device__ __forceinline__ double dt_at(const double* __restrict__ D, int nt, int i, int j) {
+  return (i >= 0 && j >= 0) ? __ldg(D + i + (size_t)nt * j) : 0.0;
+}
 
 // ------------------------------------------------------------------ straight-line classes
 
-template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(128) k_quartets(MolLaunch ql) {
+// One group quartet per lane: the warp shares the bra group, each lane owns one
+// ket group of the chunk.  X(abcd) of the lane's group quartet stays in
+// registers; the bra's primitive pairs are walked in step by the whole warp.
+// Classes with more integrals than registers hold X in NPASS launches, pass
+// PASS keeping the bra components ab in [AB0, AB1) (the recursion is repeated
+// per pass; the outputs a pass does not keep are dead code in it).
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS>
+__global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
   constexpr int NI = NA * NB * NC * ND;
+  constexpr int NAB = NA * NB;
+  constexpr int NCD = NC * ND;
   constexpr int LT = LA + LB + LC + LD;
+  constexpr int ABP = (NAB + NPASS - 1) / NPASS;
+  constexpr int AB0 = PASS * ABP;
+  constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
+  constexpr int XN = (AB1 - AB0) * NCD;
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const int nchunks = *ql.nchunks;
   const int stride = gridDim.x * wpb * ql.numprocs;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs, nt = ql.nt;
-  const double* __restrict__ D = ql.density;
+  const int nt = ql.nt;
+  const double tol = ql.inttol;
   for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
     const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    const int q = ch.y + lane;
-    const bool act = q < ch.z;
-    const int qq = act ? q : ch.y;
-    const double sp = pr.schwarz[p];
-    const bool valid = act && !(sp * pr.schwarz[qq] < ql.inttol);
-    const double zb = pr.zeta[p], ze = pr.zeta[qq];
-    const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-    const double Qx = pr.P[0][qq], Qy = pr.P[1][qq], Qz = pr.P[2][qq];
-    const double zz = zb + ze;
-    const double rho = zb * ze / zz;
-    const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
-    const double T = rho * (dx * dx + dy * dy + dz * dz);
-    const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-    double F[LT + 1];
-    boys_tab<LT>(T, pref, ql.boys, F);
-    double out[NI];
-    if constexpr (LT == 0) {
-      out[0] = F[0];
-    } else {
-      EriGeom<double> g;
-      const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
-      g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
-      g.QC[0] = pr.PA[0][qq]; g.QC[1] = pr.PA[1][qq]; g.QC[2] = pr.PA[2][qq];
-      g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
-      g.CD[0] = pr.AB[0][qq]; g.CD[1] = pr.AB[1][qq]; g.CD[2] = pr.AB[2][qq];
-      g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
-      g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
-      g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
-      eri_dispatch<LA, LB, LC, LD>(F, g, out);
+    const int G = ch.x;
+    const int li = ch.y + lane;
+    const bool act = li < ch.z;
+    const int H = ql.bk_list[act ? li : ch.y];
+    const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
+    const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
+    const double hmax = act ? ql.gr_max[H] : 0.0;
+    double hmax_w = hmax;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) hmax_w = fmax(hmax_w, __shfl_xor_sync(0xffffffffu, hmax_w, o));
+    double X[XN];
+#pragma unroll
+    for (int i = 0; i < XN; ++i) X[i] = 0.0;
+    for (int p = g0; p < g0 + gn; ++p) {
+      const double sp = pr.schwarz[p];
+      if (sp * hmax_w < tol) break;   // every later bra pair fails for every lane
+      const int I = pr.si[p], J = pr.sj[p];
+      double cab[NAB];
+#pragma unroll
+      for (int ab = AB0; ab < AB1; ++ab)
+        cab[ab] = ql.tcoef[ql.prim[I * MAXCOMP + ab / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + ab % NB]];
+      const double zb = pr.zeta[p];
+      const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
+      const double Sp = pr.S[p];
+      const double wIJ = (I != J) ? 2.0 : 1.0;
+      const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
+      for (int q = h0; q < qe; ++q) {
+        if (sp * pr.schwarz[q] < tol) break;   // the reference's screen; pairs sorted by bound
+        const double ze = pr.zeta[q];
+        const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
+        const double zz = zb + ze;
+        const double rho = zb * ze / zz;
+        const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
+        const double T = rho * (dx * dx + dy * dy + dz * dz);
+        const double pref = c2pi * Sp * pr.S[q] * sqrt(rho);
+        double F[LT + 1];
+        boys_tab<LT>(T, pref, ql.boys, F);
+        double out[NI];
+        if constexpr (LT == 0) {
+          out[0] = F[0];
+        } else {
+          EriGeom<double> g;
+          const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
+          g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
+          g.QC[0] = pr.PA[0][q]; g.QC[1] = pr.PA[1][q]; g.QC[2] = pr.PA[2][q];
+          g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
+          g.CD[0] = pr.AB[0][q]; g.CD[1] = pr.AB[1][q]; g.CD[2] = pr.AB[2][q];
+          g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
+          g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
+          g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
+          eri_dispatch<LA, LB, LC, LD>(F, g, out);
+        }
+        const int K = pr.si[q], L = pr.sj[q];
+        const double w = wIJ * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
+        double ccd[NCD];
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          const double c1 = w * ql.tcoef[ql.prim[K * MAXCOMP + cc]];
+#pragma unroll
+          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.tcoef[ql.prim[L * MAXCOMP + d]];
+        }
+#pragma unroll
+        for (int ab = AB0; ab < AB1; ++ab)
+#pragma unroll
+          for (int cd = 0; cd < NCD; ++cd)
+            X[(ab - AB0) * NCD + cd] = fma(cab[ab] * ccd[cd], out[ab * NCD + cd], X[(ab - AB0) * NCD + cd]);
+      }
     }
-    const int I = pr.si[p], J = pr.sj[p], K = pr.si[qq], L = pr.sj[qq];
-    const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-    const double wj = valid ? 0.25 * deg : 0.0, wk = valid ? 0.125 * deg : 0.0;
-    int pa[NA], pb[NB], pc[NC], pd[ND];
-#pragma unroll
-    for (int x = 0; x < NA; ++x) pa[x] = ql.prim[I * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < NB; ++x) pb[x] = ql.prim[J * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < NC; ++x) pc[x] = ql.prim[K * MAXCOMP + x];
-#pragma unroll
-    for (int x = 0; x < ND; ++x) pd[x] = ql.prim[L * MAXCOMP + x];
-    Digest<NA, NB, NC, ND> dg;
-#pragma unroll
-    for (int a = 0; a < NA; ++a) {
-#pragma unroll
-      for (int b = 0; b < NB; ++b) { dg.Pab[a * NB + b] = dens_at(D, npgs, pa[a], pb[b]); dg.jab[a * NB + b] = 0.0; }
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc) { dg.Pac[a * NC + cc] = dens_at(D, npgs, pa[a], pc[cc]); dg.kac[a * NC + cc] = 0.0; }
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pad[a * ND + d] = dens_at(D, npgs, pa[a], pd[d]); dg.kad[a * ND + d] = 0.0; }
-    }
-#pragma unroll
-    for (int b = 0; b < NB; ++b) {
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc) { dg.Pbc[b * NC + cc] = dens_at(D, npgs, pb[b], pc[cc]); dg.kbc[b * NC + cc] = 0.0; }
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pbd[b * ND + d] = dens_at(D, npgs, pb[b], pd[d]); dg.kbd[b * ND + d] = 0.0; }
-    }
-#pragma unroll
-    for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-      for (int d = 0; d < ND; ++d) { dg.Pcd[cc * ND + d] = dens_at(D, npgs, pc[cc], pd[d]); dg.jcd[cc * ND + d] = 0.0; }
-#pragma unroll
-    for (int a = 0; a < NA; ++a)
-#pragma unroll
-      for (int b = 0; b < NB; ++b)
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-          for (int d = 0; d < ND; ++d) {
-            const double v = out[((a * NB + b) * NC + cc) * ND + d];
-            dg.jab[a * NB + b] += dg.Pcd[cc * ND + d] * v;
-            dg.jcd[cc * ND + d] += dg.Pab[a * NB + b] * v;
-            dg.kad[a * ND + d] += dg.Pbc[b * NC + cc] * v;
-            dg.kbd[b * ND + d] += dg.Pac[a * NC + cc] * v;
-            dg.kac[a * NC + cc] += dg.Pbd[b * ND + d] * v;
-            dg.kbc[b * NC + cc] += dg.Pad[a * ND + d] * v;
-          }
-    // targets and coefficients of every component
+    // digestion of this pass's part of X against the target-space density
+    const double* __restrict__ D = ql.dt;
+    const int I0 = pr.si[g0], J0 = pr.sj[g0], K0 = pr.si[h0], L0 = pr.sj[h0];
     int ta[NA], tb[NB], tc[NC], td[ND];
-    double ca[NA], cb[NB], cc_[NC], cd[ND];
 #pragma unroll
-    for (int x = 0; x < NA; ++x) { ta[x] = ql.tidx[pa[x]]; ca[x] = ql.tcoef[pa[x]]; }
+    for (int x = 0; x < NA; ++x) ta[x] = ql.tidx[ql.prim[I0 * MAXCOMP + x]];
 #pragma unroll
-    for (int x = 0; x < NB; ++x) { tb[x] = ql.tidx[pb[x]]; cb[x] = ql.tcoef[pb[x]]; }
+    for (int x = 0; x < NB; ++x) tb[x] = ql.tidx[ql.prim[J0 * MAXCOMP + x]];
 #pragma unroll
-    for (int x = 0; x < NC; ++x) { tc[x] = ql.tidx[pc[x]]; cc_[x] = ql.tcoef[pc[x]]; }
+    for (int x = 0; x < NC; ++x) tc[x] = ql.tidx[ql.prim[K0 * MAXCOMP + x]];
 #pragma unroll
-    for (int x = 0; x < ND; ++x) { td[x] = ql.tidx[pd[x]]; cd[x] = ql.tcoef[pd[x]]; }
-    // segments: consecutive lanes of one contracted block pair share every target
-    const int g = act ? pr.gid[qq] : -1 - lane;
-    const unsigned seg = __match_any_sync(0xffffffffu, g);
-    const int seg_end = 31 - __clz(seg);
-    const bool head = lane == (__ffs(seg) - 1);
-    // J'(ab): the whole warp shares the bra (and its coefficients)
+    for (int x = 0; x < ND; ++x) td[x] = ql.tidx[ql.prim[L0 * MAXCOMP + x]];
+    // X(abcd) of this pass (zero outside it: constant-folded in the unrolled loops)
+    auto XV = [&](int a, int b, int cc, int d) -> double {
+      const int ab = a * NB + b;
+      return (ab >= AB0 && ab < AB1) ? X[(ab - AB0) * NCD + cc * ND + d] : 0.0;
+    };
+    // J'(ab) += 1/4 sum_cd P(cd) X: the bra is the warp's, reduce over lanes first
 #pragma unroll
-    for (int a = 0; a < NA; ++a)
+    for (int ab = AB0; ab < AB1; ++ab) {
+      double v = 0.0;
+#pragma unroll
+      for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tc[cc], td[d]), X[(ab - AB0) * NCD + cc * ND + d], v);
+      v = warp_sum(v);
+      if (lane == 0) add_target(ql.jt, nt, ta[ab / NB], tb[ab % NB], 0.25 * v);
+    }
+    if (act) {
+      // J'(cd) += 1/4 sum_ab P(ab) X
+      double Pab[NAB];
+#pragma unroll
+      for (int ab = AB0; ab < AB1; ++ab) Pab[ab] = dt_at(D, nt, ta[ab / NB], tb[ab % NB]);
+#pragma unroll
+      for (int cd = 0; cd < NCD; ++cd) {
+        double v = 0.0;
+#pragma unroll
+        for (int ab = AB0; ab < AB1; ++ab) v = fma(Pab[ab], X[(ab - AB0) * NCD + cd], v);
+        add_target(ql.jt, nt, tc[cd / ND], td[cd % ND], 0.25 * v);
+      }
+      // K'(ad) += 1/8 P(bc) X ; K'(ac) += 1/8 P(bd) X
+#pragma unroll
+      for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, tb[b], tc[cc]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, ta[a], td[d], 0.125 * v);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tb[b], td[d]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, ta[a], tc[cc], 0.125 * v);
+        }
+      }
+      // K'(bd) += 1/8 P(ac) X ; K'(bc) += 1/8 P(ad) X
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
-        const double v = warp_sum(dg.jab[a * NB + b] * wj);
-        if (lane == 0) add_target(ql.jt, nt, ta[a], tb[b], v * ca[a] * cb[b]);
-      }
-    // the rest: every lane weighs by its own ket coefficients, then the
-    // segment sums and its first lane adds
 #pragma unroll
-    for (int cc = 0; cc < NC; ++cc)
+        for (int d = 0; d < ND; ++d) {
+          double v = 0.0;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        const double v = seg_sum(dg.jcd[cc * ND + d] * wj * cc_[cc] * cd[d], lane, seg_end);
-        if (head) add_target(ql.jt, nt, tc[cc], td[d], v);
-      }
+          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
 #pragma unroll
-    for (int a = 0; a < NA; ++a) {
+            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, ta[a], tc[cc]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, tb[b], td[d], 0.125 * v);
+        }
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        const double v = seg_sum(dg.kad[a * ND + d] * wk * cd[d], lane, seg_end);
-        if (head) add_target(ql.kt, nt, ta[a], td[d], v * ca[a]);
-      }
+        for (int cc = 0; cc < NC; ++cc) {
+          double v = 0.0;
 #pragma unroll
-      for (int cc = 0; cc < NC; ++cc) {
-        const double v = seg_sum(dg.kac[a * NC + cc] * wk * cc_[cc], lane, seg_end);
-        if (head) add_target(ql.kt, nt, ta[a], tc[cc], v * ca[a]);
-      }
-    }
+          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
 #pragma unroll
-    for (int b = 0; b < NB; ++b) {
-#pragma unroll
-      for (int d = 0; d < ND; ++d) {
-        const double v = seg_sum(dg.kbd[b * ND + d] * wk * cd[d], lane, seg_end);
-        if (head) add_target(ql.kt, nt, tb[b], td[d], v * cb[b]);
-      }
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc) {
-        const double v = seg_sum(dg.kbc[b * NC + cc] * wk * cc_[cc], lane, seg_end);
-        if (head) add_target(ql.kt, nt, tb[b], tc[cc], v * cb[b]);
+            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, ta[a], td[d]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, tb[b], tc[cc], 0.125 * v);
+        }
       }
     }
   }
@@ -369,14 +507,16 @@ __global__ void __launch_bounds__(128) k_quartets(MolLaunch ql) {
 
 // ------------------------------------------------------------------ interpreted classes
 
-// Digestion targets of one quartet, t in [0, NT): J'(ab), J'(cd), K'(ad),
-// K'(bd), K'(ac), K'(bc).  slots(): the matrix (0 = J', 1 = K') and the two
-// component slots (a: 0.., b: NA.., c: NA+NB.., d: NA+NB+NC..) of target t;
-// value(): its density-weighted sum over the quartet's integrals.
+// Digestion of a contracted X(abcd) into the targets of one group quartet,
+// target t in [0, NT): J'(ab), J'(cd), K'(ad), K'(bd), K'(ac), K'(bc).
 template <int NA, int NB, int NC, int ND>
-struct Targets {
+struct Digest {
   static constexpr int NT = NA * NB + NC * ND + (NA + NB) * (NC + ND);
   static constexpr int SB = NA, SC = NA + NB, SD = NA + NB + NC;
+  static constexpr int NP = NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
+  // density blocks in shared memory: Pab | Pcd | Pac | Pad | Pbc | Pbd
+  static constexpr int OAB = 0, OCD = NA * NB, OAC = OCD + NC * ND, OAD = OAC + NA * NC, OBC = OAD + NA * ND,
+                       OBD = OBC + NB * NC;
   __device__ static void slots(int t, int* kind, int* s1, int* s2) {
     int r = t;
     if (r < NA * NB) { *kind = 0; *s1 = r / NB; *s2 = SB + r % NB; return; }
@@ -391,327 +531,276 @@ struct Targets {
     r -= NA * NC;
     *kind = 1; *s1 = SB + r / NC; *s2 = SC + r % NC;
   }
-  __device__ static double value(int t, const double* __restrict__ v, const unsigned short* __restrict__ out,
-                                 const double* Pab, const double* Pcd, const double* Pac, const double* Pad,
-                                 const double* Pbc, const double* Pbd) {
+  __device__ static double value(int t, const double* __restrict__ X, const double* __restrict__ P) {
     double acc = 0.0;
     int r = t;
     if (r < NA * NB) {
       const int a = r / NB, b = r % NB;
-      for (int cc = 0; cc < NC; ++cc)
-        for (int d = 0; d < ND; ++d) acc += Pcd[cc * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-      return acc;
+      for (int cd = 0; cd < NC * ND; ++cd) acc = fma(P[OCD + cd], X[(a * NB + b) * NC * ND + cd], acc);
+      return 0.25 * acc;
     }
     r -= NA * NB;
     if (r < NC * ND) {
-      const int cc = r / ND, d = r % ND;
-      for (int a = 0; a < NA; ++a)
-        for (int b = 0; b < NB; ++b) acc += Pab[a * NB + b] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-      return acc;
+      for (int ab = 0; ab < NA * NB; ++ab) acc = fma(P[OAB + ab], X[ab * NC * ND + r], acc);
+      return 0.25 * acc;
     }
     r -= NC * ND;
     if (r < NA * ND) {
       const int a = r / ND, d = r % ND;
       for (int b = 0; b < NB; ++b)
-        for (int cc = 0; cc < NC; ++cc) acc += Pbc[b * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-      return acc;
+        for (int cc = 0; cc < NC; ++cc) acc = fma(P[OBC + b * NC + cc], X[((a * NB + b) * NC + cc) * ND + d], acc);
+      return 0.125 * acc;
     }
     r -= NA * ND;
     if (r < NB * ND) {
       const int b = r / ND, d = r % ND;
       for (int a = 0; a < NA; ++a)
-        for (int cc = 0; cc < NC; ++cc) acc += Pac[a * NC + cc] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-      return acc;
+        for (int cc = 0; cc < NC; ++cc) acc = fma(P[OAC + a * NC + cc], X[((a * NB + b) * NC + cc) * ND + d], acc);
+      return 0.125 * acc;
     }
     r -= NB * ND;
     if (r < NA * NC) {
       const int a = r / NC, cc = r % NC;
       for (int b = 0; b < NB; ++b)
-        for (int d = 0; d < ND; ++d) acc += Pbd[b * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-      return acc;
+        for (int d = 0; d < ND; ++d) acc = fma(P[OBD + b * ND + d], X[((a * NB + b) * NC + cc) * ND + d], acc);
+      return 0.125 * acc;
     }
     r -= NA * NC;
     const int b = r / NC, cc = r % NC;
     for (int a = 0; a < NA; ++a)
-      for (int d = 0; d < ND; ++d) acc += Pad[a * ND + d] * v[out[((a * NB + b) * NC + cc) * ND + d]];
-    return acc;
+      for (int d = 0; d < ND; ++d) acc = fma(P[OAD + a * ND + d], X[((a * NB + b) * NC + cc) * ND + d], acc);
+    return 0.125 * acc;
   }
 };
 
-// One quartet per warp (several warps per block) on the level-scheduled op
-// table.  When a class has at most 256 targets, each lane keeps its targets'
-// coefficient-weighted sums in registers while consecutive kets belong to one
-// contracted block pair (same contracted targets) and adds them once per run;
-// the bra's J'(ab) is added once per chunk.
+// Shared-memory layout of one interpreter team (a warp or a block), in doubles:
+// v[nslots] | P blocks[NP] | cab[NA*NB] | ccd[NC*ND] | X[NI] (X only when it is
+// not in global scratch: the (22|22) working set exceeds shared memory)
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(256) k_quartets_warp(MolLaunch ql, OpTableDev tab, int per_warp) {
+struct TeamLayout {
+  static constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
+  static constexpr int NI = NA * NB * NC * ND;
+  static __host__ __device__ int doubles(int nslots, bool x_in_smem) {
+    return nslots + Digest<NA, NB, NC, ND>::NP + NA * NB + NC * ND + (x_in_smem ? NI : 0);
+  }
+};
+
+// Team-cooperative evaluation of the group quartets of one chunk: all threads
+// of the team (a warp, or the block) share one primitive quartet at a time and
+// run the op table level by level; X accumulates in shared (or global) memory.
+template <int LA, int LB, int LC, int LD, bool BLOCK>
+__device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& tab, const int4 ch, double* sm,
+                                        double* xg, OpGeom& geo, int* prm, double* sw, int tid, int team) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
+  constexpr int NI = NA * NB * NC * ND;
+  constexpr int NCD = NC * ND;
   constexpr int LT = LA + LB + LC + LD;
-  using TG = Targets<NA, NB, NC, ND>;
-  constexpr int NT = TG::NT;
-  constexpr int NPRM = NA + NB + NC + ND;
-  constexpr int NR = (NT + 31) / 32;
-  constexpr bool HOLD = NR <= 8;
-  extern __shared__ double smem[];
-  __shared__ OpGeom s_geo[8];
-  __shared__ int s_prm[8][NPRM];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
-  double* v = smem + (size_t)wid * per_warp;
-  double* Pab = v + tab.nslots;
-  double* Pcd = Pab + NA * NB;
-  double* Pac = Pcd + NC * ND;
-  double* Pad = Pac + NA * NC;
-  double* Pbc = Pad + NA * ND;
-  double* Pbd = Pbc + NB * NC;
-  OpGeom& geo = s_geo[wid];
-  int* prm = s_prm[wid];
+  using DG = Digest<NA, NB, NC, ND>;
+  auto sync = [&]() { if constexpr (BLOCK) __syncthreads(); else __syncwarp(); };
+  double* v = sm;
+  double* P = v + tab.nslots;
+  double* cab = P + DG::NP;
+  double* ccd = cab + NA * NB;
+  double* X = xg ? xg : ccd + NCD;
   const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs, nt = ql.nt;
-  const double* __restrict__ D = ql.density;
-  const int nchunks = *ql.nchunks;
+  const int nt = ql.nt;
+  const double tol = ql.inttol;
+  const double* __restrict__ D = ql.dt;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const int base = LT + 2;
-  const int stride = gridDim.x * wpb * ql.numprocs;
-  double hold[HOLD ? NR : 1];
-  // adds the held sums of this lane's targets; ket slots of prm still hold a
-  // member of the run being flushed (all members share their targets)
-  auto flush = [&](bool with_bra) {
-#pragma unroll
-    for (int r = 0; r < (HOLD ? NR : 0); ++r) {
-      const int t = lane + 32 * r;
-      if (t < NT && (with_bra || t >= NA * NB)) {
-        int kind, s1, s2;
-        TG::slots(t, &kind, &s1, &s2);
-        add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[prm[s1]], ql.tidx[prm[s2]], hold[r]);
-        hold[r] = 0.0;
-      }
+  const int G = ch.x;
+  const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
+  {
+    const int I0 = pr.si[g0], J0 = pr.sj[g0];
+    for (int x = tid; x < NA; x += team) prm[x] = ql.prim[I0 * MAXCOMP + x];
+    for (int x = tid; x < NB; x += team) prm[DG::SB + x] = ql.prim[J0 * MAXCOMP + x];
+  }
+  sync();
+  for (int t = tid; t < NA * NB; t += team)
+    P[DG::OAB + t] = dt_at(D, nt, ql.tidx[prm[t / NB]], ql.tidx[prm[DG::SB + t % NB]]);
+  for (int k = ch.y; k < ch.z; ++k) {
+    const int H = ql.bk_list[k];
+    const int h0 = ql.gr_start[H], hn = ql.gr_n[H];
+    const double hmax = ql.gr_max[H];
+    {
+      const int K0 = pr.si[h0], L0 = pr.sj[h0];
+      for (int x = tid; x < NC; x += team) prm[DG::SC + x] = ql.prim[K0 * MAXCOMP + x];
+      for (int x = tid; x < ND; x += team) prm[DG::SD + x] = ql.prim[L0 * MAXCOMP + x];
     }
-  };
-  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
-    const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    const int I = pr.si[p], J = pr.sj[p];
-    for (int x = lane; x < NA; x += 32) prm[x] = ql.prim[I * MAXCOMP + x];
-    for (int x = lane; x < NB; x += 32) prm[TG::SB + x] = ql.prim[J * MAXCOMP + x];
-    __syncwarp();
-    for (int t = lane; t < NA * NB; t += 32) Pab[t] = dens_at(D, npgs, prm[t / NB], prm[TG::SB + t % NB]);
-    const double zb = pr.zeta[p], sp = pr.schwarz[p];
-    const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-#pragma unroll
-    for (int r = 0; r < (HOLD ? NR : 1); ++r) hold[r] = 0.0;
-    int run = -1;  // contracted block pair of the held sums
-    for (int qq = ch.y; qq < ch.z; ++qq) {
-      if (sp * pr.schwarz[qq] < ql.inttol) continue;   // the reference's screen (warp-uniform)
-      const int K = pr.si[qq], L = pr.sj[qq];
-      if (HOLD) {
-        const int g = pr.gid[qq];
-        if (g != run) {
-          if (run >= 0) flush(false);
-          run = g;
-          __syncwarp();
-        }
-      }
-      const double ze = pr.zeta[qq];
-      const double Qx = pr.P[0][qq], Qy = pr.P[1][qq], Qz = pr.P[2][qq];
-      const double zz = zb + ze, rho = zb * ze / zz;
-      const double T = rho * ((Px - Qx) * (Px - Qx) + (Py - Qy) * (Py - Qy) + (Pz - Qz) * (Pz - Qz));
-      const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-      if (lane == 0) {
-        double F[LT + 1];
-        boys_tab<LT>(T, pref, ql.boys, F);
-        v[0] = 0.0;
-#pragma unroll
-        for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
-      } else if (lane == 1) {
-        const double W[3] = {(zb * Px + ze * Qx) / zz, (zb * Py + ze * Qy) / zz, (zb * Pz + ze * Qz) / zz};
-        const double Pv[3] = {Px, Py, Pz}, Qv[3] = {Qx, Qy, Qz};
-        double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
-        for (int k = 0; k < 3; ++k) {
-          PA[k] = pr.PA[k][p]; QC[k] = pr.PA[k][qq]; AB[k] = pr.AB[k][p]; CD[k] = pr.AB[k][qq];
-          WP[k] = W[k] - Pv[k]; WQ[k] = W[k] - Qv[k];
-        }
-        set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
-      }
-      for (int x = lane; x < NC; x += 32) prm[TG::SC + x] = ql.prim[K * MAXCOMP + x];
-      for (int x = lane; x < ND; x += 32) prm[TG::SD + x] = ql.prim[L * MAXCOMP + x];
-      __syncwarp();
+    for (int i = tid; i < NI; i += team) X[i] = 0.0;
+    sync();
+    {
       const int* pa = prm;
-      const int* pb = prm + TG::SB;
-      const int* pc = prm + TG::SC;
-      const int* pd = prm + TG::SD;
-      for (int t = lane; t < NC * ND; t += 32) Pcd[t] = dens_at(D, npgs, pc[t / ND], pd[t % ND]);
-      for (int t = lane; t < NA * NC; t += 32) Pac[t] = dens_at(D, npgs, pa[t / NC], pc[t % NC]);
-      for (int t = lane; t < NA * ND; t += 32) Pad[t] = dens_at(D, npgs, pa[t / ND], pd[t % ND]);
-      for (int t = lane; t < NB * NC; t += 32) Pbc[t] = dens_at(D, npgs, pb[t / NC], pc[t % NC]);
-      for (int t = lane; t < NB * ND; t += 32) Pbd[t] = dens_at(D, npgs, pb[t / ND], pd[t % ND]);
-      for (int l = 0; l < tab.nlevels; ++l) {
-        const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-        for (int o = o0 + lane; o < o1; o += 32) {
-          const unsigned short* op = tab.ops + 6 * o;
-          const int h = op[0];
-          const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-          double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-          if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-          if (cB) val += (double)cB * geo.Z * v[op[5]];
-          v[base + o] = val;
-        }
-        __syncwarp();
-      }
-      const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-      const double wj = 0.25 * deg, wk = 0.125 * deg;
-#pragma unroll
-      for (int r = 0; r < NR; ++r) {
-        const int t = lane + 32 * r;
-        if (t < NT) {
-          int kind, s1, s2;
-          TG::slots(t, &kind, &s1, &s2);
-          const int p1 = prm[s1], p2 = prm[s2];
-          const double w = (kind == 0 ? wj : wk) * ql.tcoef[p1] * ql.tcoef[p2] *
-                           TG::value(t, v, tab.out, Pab, Pcd, Pac, Pad, Pbc, Pbd);
-          if constexpr (HOLD) hold[r] += w;
-          else add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[p1], ql.tidx[p2], w);
-        }
-      }
-      __syncwarp();
+      const int* pb = prm + DG::SB;
+      const int* pc = prm + DG::SC;
+      const int* pd = prm + DG::SD;
+      for (int t = tid; t < NC * ND; t += team) P[DG::OCD + t] = dt_at(D, nt, ql.tidx[pc[t / ND]], ql.tidx[pd[t % ND]]);
+      for (int t = tid; t < NA * NC; t += team) P[DG::OAC + t] = dt_at(D, nt, ql.tidx[pa[t / NC]], ql.tidx[pc[t % NC]]);
+      for (int t = tid; t < NA * ND; t += team) P[DG::OAD + t] = dt_at(D, nt, ql.tidx[pa[t / ND]], ql.tidx[pd[t % ND]]);
+      for (int t = tid; t < NB * NC; t += team) P[DG::OBC + t] = dt_at(D, nt, ql.tidx[pb[t / NC]], ql.tidx[pc[t % NC]]);
+      for (int t = tid; t < NB * ND; t += team) P[DG::OBD + t] = dt_at(D, nt, ql.tidx[pb[t / ND]], ql.tidx[pd[t % ND]]);
     }
-    if (HOLD && run >= 0) flush(true);
-    __syncwarp();
+    for (int p = g0; p < g0 + gn; ++p) {
+      const double sp = pr.schwarz[p];
+      if (sp * hmax < tol) break;
+      const int I = pr.si[p], J = pr.sj[p];
+      for (int t = tid; t < NA * NB; t += team)
+        cab[t] = ql.tcoef[ql.prim[I * MAXCOMP + t / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + t % NB]];
+      const double zb = pr.zeta[p];
+      const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
+      const int qe = (G == H) ? p + 1 : h0 + hn;
+      for (int q = h0; q < qe; ++q) {
+        if (sp * pr.schwarz[q] < tol) break;   // the reference's screen (team-uniform)
+        const int K = pr.si[q], L = pr.sj[q];
+        const double ze = pr.zeta[q];
+        const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
+        const double zz = zb + ze, rho = zb * ze / zz;
+        if (tid == 0) {
+          const double T = rho * ((Px - Qx) * (Px - Qx) + (Py - Qy) * (Py - Qy) + (Pz - Qz) * (Pz - Qz));
+          const double pref = c2pi * pr.S[p] * pr.S[q] * sqrt(rho);
+          double F[LT + 1];
+          boys_tab<LT>(T, pref, ql.boys, F);
+          v[0] = 0.0;
+#pragma unroll
+          for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
+          sw[0] = ((I != J) ? 2.0 : 1.0) * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
+        } else if (tid == 1) {
+          const double W[3] = {(zb * Px + ze * Qx) / zz, (zb * Py + ze * Qy) / zz, (zb * Pz + ze * Qz) / zz};
+          const double Pv[3] = {Px, Py, Pz}, Qv[3] = {Qx, Qy, Qz};
+          double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
+          for (int k2 = 0; k2 < 3; ++k2) {
+            PA[k2] = pr.PA[k2][p]; QC[k2] = pr.PA[k2][q]; AB[k2] = pr.AB[k2][p]; CD[k2] = pr.AB[k2][q];
+            WP[k2] = W[k2] - Pv[k2]; WQ[k2] = W[k2] - Qv[k2];
+          }
+          set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
+        }
+        for (int t = tid; t < NCD; t += team)
+          ccd[t] = ql.tcoef[ql.prim[K * MAXCOMP + t / ND]] * ql.tcoef[ql.prim[L * MAXCOMP + t % ND]];
+        sync();
+        for (int l = 0; l < tab.nlevels; ++l) {
+          const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
+          for (int o = o0 + tid; o < o1; o += team) {
+            const unsigned short* op = tab.ops + 6 * o;
+            const int h = op[0];
+            const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
+            double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
+            if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
+            if (cB) val += (double)cB * geo.Z * v[op[5]];
+            v[base + o] = val;
+          }
+          sync();
+        }
+        const double w = sw[0];
+        for (int i = tid; i < NI; i += team) X[i] = fma(w * cab[i / NCD] * ccd[i % NCD], v[tab.out[i]], X[i]);
+        sync();
+      }
+    }
+    // digestion of the group quartet
+    for (int t = tid; t < DG::NT; t += team) {
+      int kind, s1, s2;
+      DG::slots(t, &kind, &s1, &s2);
+      add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[prm[s1]], ql.tidx[prm[s2]], DG::value(t, X, P));
+    }
+    sync();
   }
 }
 
-// One quartet at a time per block (the largest classes).
 template <int LA, int LB, int LC, int LD>
-__global__ void __launch_bounds__(256) k_quartets_big(MolLaunch ql, OpTableDev tab) {
-  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
-  constexpr int LT = LA + LB + LC + LD;
-  constexpr int NT = Targets<NA, NB, NC, ND>::NT;
+__global__ void __launch_bounds__(256) k_gq_warp(MolLaunch ql, OpTableDev tab, int per_warp) {
+  constexpr int NPRM = ncum(LA) + ncum(LB) + ncum(LC) + ncum(LD);
   extern __shared__ double smem[];
-  double* v = smem;
-  double* Pab = smem + tab.nslots;
-  double* Pcd = Pab + NA * NB;
-  double* Pac = Pcd + NC * ND;
-  double* Pad = Pac + NA * NC;
-  double* Pbc = Pad + NA * ND;
-  double* Pbd = Pbc + NB * NC;
-  __shared__ OpGeom geo;
-  __shared__ int prm[NA + NB + NC + ND];
-  __shared__ double s_w[2];
-  const PairArrays pr = ql.pairs;
-  const int npgs = ql.npgs, nt = ql.nt;
-  const double* __restrict__ D = ql.density;
+  __shared__ OpGeom s_geo[8];
+  __shared__ int s_prm[8][NPRM];
+  __shared__ double s_w[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int nchunks = *ql.nchunks;
-  const double c2pi = 2.0 / sqrt(REF_PI);
-  const int base = LT + 2;
-  for (int c = blockIdx.x * ql.numprocs + ql.myid; c < nchunks; c += gridDim.x * ql.numprocs) {
-    const int4 ch = ql.chunks[c];
-    const int p = ch.x;
-    const double sp = pr.schwarz[p];
-    for (int qq = ch.y; qq < ch.z; ++qq) {
-      if (sp * pr.schwarz[qq] < ql.inttol) continue;
-      if (threadIdx.x == 0) {
-        const double zb = pr.zeta[p], ze = pr.zeta[qq];
-        const double Pv[3] = {pr.P[0][p], pr.P[1][p], pr.P[2][p]};
-        const double Qv[3] = {pr.P[0][qq], pr.P[1][qq], pr.P[2][qq]};
-        const double zz = zb + ze, rho = zb * ze / zz;
-        const double T = rho * ((Pv[0] - Qv[0]) * (Pv[0] - Qv[0]) + (Pv[1] - Qv[1]) * (Pv[1] - Qv[1]) +
-                                (Pv[2] - Qv[2]) * (Pv[2] - Qv[2]));
-        const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
-        double F[LT + 1];
-        boys_tab<LT>(T, pref, ql.boys, F);
-        v[0] = 0.0;
-        for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
-        double PA[3], QC[3], AB[3], CD[3], WP[3], WQ[3];
-        for (int k = 0; k < 3; ++k) {
-          const double W = (zb * Pv[k] + ze * Qv[k]) / zz;
-          PA[k] = pr.PA[k][p]; QC[k] = pr.PA[k][qq]; AB[k] = pr.AB[k][p]; CD[k] = pr.AB[k][qq];
-          WP[k] = W - Pv[k]; WQ[k] = W - Qv[k];
-        }
-        set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
-        const int I = pr.si[p], J = pr.sj[p], K = pr.si[qq], L = pr.sj[qq];
-        const double deg = (I != J ? 2.0 : 1.0) * (K != L ? 2.0 : 1.0) * (p != qq ? 2.0 : 1.0);
-        s_w[0] = 0.25 * deg;
-        s_w[1] = 0.125 * deg;
-        for (int x = 0; x < NA; ++x) prm[x] = ql.prim[I * MAXCOMP + x];
-        for (int x = 0; x < NB; ++x) prm[NA + x] = ql.prim[J * MAXCOMP + x];
-        for (int x = 0; x < NC; ++x) prm[NA + NB + x] = ql.prim[K * MAXCOMP + x];
-        for (int x = 0; x < ND; ++x) prm[NA + NB + NC + x] = ql.prim[L * MAXCOMP + x];
-      }
-      __syncthreads();
-      const int* pa = prm;
-      const int* pb = prm + NA;
-      const int* pc = prm + NA + NB;
-      const int* pd = prm + NA + NB + NC;
-      for (int t = threadIdx.x; t < NA * NB; t += blockDim.x) Pab[t] = dens_at(D, npgs, pa[t / NB], pb[t % NB]);
-      for (int t = threadIdx.x; t < NC * ND; t += blockDim.x) Pcd[t] = dens_at(D, npgs, pc[t / ND], pd[t % ND]);
-      for (int t = threadIdx.x; t < NA * NC; t += blockDim.x) Pac[t] = dens_at(D, npgs, pa[t / NC], pc[t % NC]);
-      for (int t = threadIdx.x; t < NA * ND; t += blockDim.x) Pad[t] = dens_at(D, npgs, pa[t / ND], pd[t % ND]);
-      for (int t = threadIdx.x; t < NB * NC; t += blockDim.x) Pbc[t] = dens_at(D, npgs, pb[t / NC], pc[t % NC]);
-      for (int t = threadIdx.x; t < NB * ND; t += blockDim.x) Pbd[t] = dens_at(D, npgs, pb[t / ND], pd[t % ND]);
-      run_optable(tab, v, geo, base);
-      for (int t = threadIdx.x; t < NT; t += blockDim.x) {
-        int kind, r1, r2;
-        Targets<NA, NB, NC, ND>::slots(t, &kind, &r1, &r2);
-        const double val = Targets<NA, NB, NC, ND>::value(t, v, tab.out, Pab, Pcd, Pac, Pad, Pbc, Pbd);
-        const int p1 = prm[r1], p2 = prm[r2];
-        add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[p1], ql.tidx[p2],
-                   (kind == 0 ? s_w[0] : s_w[1]) * val * ql.tcoef[p1] * ql.tcoef[p2]);
-      }
-      __syncthreads();
-    }
-  }
+  const int stride = gridDim.x * wpb * ql.numprocs;
+  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride)
+    gq_team<LA, LB, LC, LD, false>(ql, tab, ql.chunks[c], smem + (size_t)wid * per_warp, nullptr, s_geo[wid],
+                                   s_prm[wid], s_w + wid, lane, 32);
+}
+
+// xg: per-block X scratch in global memory (gridDim.x * NI doubles), or null
+// for X in shared memory.
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(256) k_gq_block(MolLaunch ql, OpTableDev tab, double* xg) {
+  constexpr int NPRM = ncum(LA) + ncum(LB) + ncum(LC) + ncum(LD);
+  extern __shared__ double smem[];
+  __shared__ OpGeom s_geo;
+  __shared__ int s_prm[NPRM];
+  __shared__ double s_w[1];
+  const int nchunks = *ql.nchunks;
+  for (int c = blockIdx.x * ql.numprocs + ql.myid; c < nchunks; c += gridDim.x * ql.numprocs)
+    gq_team<LA, LB, LC, LD, true>(ql, tab, ql.chunks[c], smem,
+                                  xg ? xg + (size_t)blockIdx.x * (ncum(LA) * ncum(LB) * ncum(LC) * ncum(LD)) : nullptr,
+                                  s_geo, s_prm, s_w, threadIdx.x, blockDim.x);
 }
 
 // ------------------------------------------------------------------ launch tables
 
 using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
 
-template <int LA, int LB, int LC, int LD>
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS>
+struct Passes {
+  static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
+    k_gq<LA, LB, LC, LD, NPASS, PASS><<<grid, 128, 0, s>>>(ql);
+    if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1>::run(ql, grid, s);
+  }
+};
+
+template <int LA, int LB, int LC, int LD, int NPASS>
 static void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
-  k_quartets<LA, LB, LC, LD><<<grid, 128, 0, s>>>(ql);
+  Passes<LA, LB, LC, LD, NPASS, 0>::run(ql, grid, s);
 }
 
+// straight-line classes and their passes (X of at most 40 integrals per pass)
 static LaunchFn straight_launcher(int cb, int ck) {
-#define Q(A, B, C, D) &launch_q<A, B, C, D>
+#define Q(A, B, C, D, P) &launch_q<A, B, C, D, P>
   static const LaunchFn table[6][6] = {
-      {Q(0, 0, 0, 0), nullptr, nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 0, 0, 0), Q(1, 0, 1, 0), nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 1, 0, 0), Q(1, 1, 1, 0), Q(1, 1, 1, 1), nullptr, nullptr, nullptr},
-      {Q(2, 0, 0, 0), Q(2, 0, 1, 0), Q(2, 0, 1, 1), Q(2, 0, 2, 0), nullptr, nullptr},
-      {Q(2, 1, 0, 0), Q(2, 1, 1, 0), nullptr, nullptr, nullptr, nullptr},
-      {Q(2, 2, 0, 0), nullptr, nullptr, nullptr, nullptr, nullptr}};
+      {Q(0, 0, 0, 0, 1), nullptr, nullptr, nullptr, nullptr, nullptr},
+      {Q(1, 0, 0, 0, 1), Q(1, 0, 1, 0, 1), nullptr, nullptr, nullptr, nullptr},
+      {Q(1, 1, 0, 0, 1), Q(1, 1, 1, 0, 2), Q(1, 1, 1, 1, 8), nullptr, nullptr, nullptr},
+      {Q(2, 0, 0, 0, 1), Q(2, 0, 1, 0, 1), Q(2, 0, 1, 1, 5), Q(2, 0, 2, 0, 3), nullptr, nullptr},
+      {Q(2, 1, 0, 0, 1), Q(2, 1, 1, 0, 4), nullptr, nullptr, nullptr, nullptr},
+      {Q(2, 2, 0, 0, 3), nullptr, nullptr, nullptr, nullptr, nullptr}};
 #undef Q
   return table[cb][ck];
 }
 
-using BigFn = void (*)(const MolLaunch&, const OpTableDev&, int grid, size_t smem, cudaStream_t);
+using BigFn = void (*)(const MolLaunch&, const OpTableDev&, double* xg, int grid, size_t smem, cudaStream_t);
 using WarpFn = void (*)(const MolLaunch&, const OpTableDev&, int grid, int wpb, int per_warp, size_t smem, cudaStream_t);
 
 template <int LA, int LB, int LC, int LD>
-static void launch_big(const MolLaunch& ql, const OpTableDev& t, int grid, size_t smem, cudaStream_t s) {
-  k_quartets_big<LA, LB, LC, LD><<<grid, 256, smem, s>>>(ql, t);
+static void launch_big(const MolLaunch& ql, const OpTableDev& t, double* xg, int grid, size_t smem, cudaStream_t s) {
+  k_gq_block<LA, LB, LC, LD><<<grid, 256, smem, s>>>(ql, t, xg);
 }
 
 template <int LA, int LB, int LC, int LD>
 static void launch_warp(const MolLaunch& ql, const OpTableDev& t, int grid, int wpb, int per_warp, size_t smem,
                         cudaStream_t s) {
-  k_quartets_warp<LA, LB, LC, LD><<<grid, 32 * wpb, smem, s>>>(ql, t, per_warp);
+  k_gq_warp<LA, LB, LC, LD><<<grid, 32 * wpb, smem, s>>>(ql, t, per_warp);
 }
 
 template <int LA, int LB, int LC, int LD>
 static cudaError_t allow_smem_both(size_t big, size_t warp) {
-  cudaError_t e = cudaFuncSetAttribute(k_quartets_big<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
+  cudaError_t e = cudaFuncSetAttribute(k_gq_block<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_quartets_warp<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp);
+  return cudaFuncSetAttribute(k_gq_warp<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp);
 }
+
+template <int LA, int LB, int LC, int LD>
+static int team_doubles(int nslots, bool x_in_smem) { return TeamLayout<LA, LB, LC, LD>::doubles(nslots, x_in_smem); }
 
 struct Variants {
   BigFn big;
   WarpFn warp;
   cudaError_t (*allow)(size_t, size_t);
+  int (*doubles)(int, bool);
 };
 
 static Variants variants(int cb, int ck) {
-#define V(A, B, C, D) Variants{&launch_big<A, B, C, D>, &launch_warp<A, B, C, D>, &allow_smem_both<A, B, C, D>}
+#define V(A, B, C, D) \
+  Variants{&launch_big<A, B, C, D>, &launch_warp<A, B, C, D>, &allow_smem_both<A, B, C, D>, &team_doubles<A, B, C, D>}
   switch (cb * 8 + ck) {
     case 0: return V(0, 0, 0, 0);
     case 8: return V(1, 0, 0, 0);
@@ -734,23 +823,41 @@ static Variants variants(int cb, int ck) {
     case 43: return V(2, 2, 2, 0);
     case 44: return V(2, 2, 2, 1);
     case 45: return V(2, 2, 2, 2);
-    default: return Variants{nullptr, nullptr, nullptr};
+    default: return Variants{nullptr, nullptr, nullptr, nullptr};
   }
 #undef V
 }
 
-static int density_block_doubles(int cb, int ck) {
-  const int NA = ncum(kCL[cb][0]), NB = ncum(kCL[cb][1]), NC = ncum(kCL[ck][0]), ND = ncum(kCL[ck][1]);
-  return NA * NB + NC * ND + NA * NC + NA * ND + NB * NC + NB * ND;
+// ------------------------------------------------------------------ set-up
+
+template <typename KeyT>
+static int radix_sort_pairs(pfe_context* ctx, const KeyT* kin, KeyT* kout, const int* vin, int* vout, int n, int bits,
+                            cudaStream_t s) {
+  size_t tb = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, n, 0, bits, s);
+  void* tmp = nullptr;
+  PFE_CUDA(ctx->alloc(&tmp, tb + 16));
+  PFE_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, n, 0, bits, s));
+  ctx->free_later(tmp);
+  return PFE_OK;
 }
 
-// ------------------------------------------------------------------ set-up
+static int exclusive_sum(pfe_context* ctx, const int* in, int* out, int n, cudaStream_t s) {
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, s);
+  void* tmp = nullptr;
+  PFE_CUDA(ctx->alloc(&tmp, tb + 16));
+  PFE_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, n, s));
+  ctx->free_later(tmp);
+  return PFE_OK;
+}
 
 int molecular_setup(pfe_context* ctx, const pfe_args* a) {
   (void)a;
   cudaStream_t s = ctx->stream;
   const int nsh = ctx->npshell;
   const long long npairs = (long long)nsh * (nsh + 1) / 2;
+  if (npairs >= (1LL << 31)) { set_error("too many shell pairs for 32-bit pair indices"); return PFE_EINVAL; }
   ctx->npairs = npairs;
   PairArrays raw{};
   int rc;
@@ -792,12 +899,12 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
     ctx->free_now(list);
     ctx->free_now(cnt);
   }
-  // group maxima and the four sort keys
-  const long long ngroups = (long long)ctx->nblk * ctx->nblk;
+  // sort by (class, group maximum desc, group, bound desc): four stable radix passes
+  const long long ngid = (long long)ctx->nblk * ctx->nblk;
   unsigned long long *gbits = nullptr, *k_sch = nullptr, *k_gmax = nullptr, *k64 = nullptr;
   int *perm_a = nullptr, *perm_b = nullptr, *k32 = nullptr, *k32b = nullptr;
   unsigned char *k8 = nullptr, *k8b = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&gbits, sizeof(unsigned long long) * ngroups));
+  PFE_CUDA(ctx->alloc((void**)&gbits, sizeof(unsigned long long) * ngid));
   PFE_CUDA(ctx->alloc((void**)&k_sch, sizeof(unsigned long long) * npairs));
   PFE_CUDA(ctx->alloc((void**)&k_gmax, sizeof(unsigned long long) * npairs));
   PFE_CUDA(ctx->alloc((void**)&k64, sizeof(unsigned long long) * npairs));
@@ -807,144 +914,187 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
   PFE_CUDA(ctx->alloc((void**)&k32b, sizeof(int) * npairs));
   PFE_CUDA(ctx->alloc((void**)&k8, npairs));
   PFE_CUDA(ctx->alloc((void**)&k8b, npairs));
-  PFE_CUDA(cudaMemsetAsync(gbits, 0, sizeof(unsigned long long) * ngroups, s));
+  PFE_CUDA(cudaMemsetAsync(gbits, 0, sizeof(unsigned long long) * ngid, s));
   k_mol_groupmax<<<nb256, 256, 0, s>>>(raw.schwarz, raw.gid, gbits, npairs);
   k_mol_keys<<<nb256, 256, 0, s>>>(raw.schwarz, raw.gid, gbits, k_sch, k_gmax, raw.gmax, npairs);
   k_mol_iota<<<nb256, 256, 0, s>>>(perm_a, npairs);
   PFE_CUDA(cudaGetLastError());
   {
     const int n = (int)npairs;
-    size_t t1 = 0, t2 = 0, t3 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t1, k_sch, k64, perm_a, perm_b, n, 0, 64, s);
-    cub::DeviceRadixSort::SortPairs(nullptr, t2, k32, k32b, perm_b, perm_a, n, 0, 32, s);
-    cub::DeviceRadixSort::SortPairs(nullptr, t3, k8, k8b, perm_a, perm_b, n, 0, 8, s);
-    const size_t tb = std::max(t1, std::max(t2, t3)) + 16;
-    void* tmp = nullptr;
-    PFE_CUDA(ctx->alloc(&tmp, tb));
-    size_t tt = tb;
-    // 1: bound descending
-    PFE_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tt, k_sch, k64, perm_a, perm_b, n, 0, 64, s));
-    // 2: group (stable)
+    if ((rc = radix_sort_pairs(ctx, k_sch, k64, perm_a, perm_b, n, 64, s)) != PFE_OK) return rc;
     k_gather_t<int><<<nb256, 256, 0, s>>>(raw.gid, perm_b, k32, npairs);
-    tt = tb;
-    PFE_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tt, k32, k32b, perm_b, perm_a, n, 0, 32, s));
-    // 3: group maximum descending (stable)
+    if ((rc = radix_sort_pairs(ctx, k32, k32b, perm_b, perm_a, n, 32, s)) != PFE_OK) return rc;
     k_gather_t<unsigned long long><<<nb256, 256, 0, s>>>(k_gmax, perm_a, k_sch, npairs);
-    tt = tb;
-    PFE_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tt, k_sch, k64, perm_a, perm_b, n, 0, 64, s));
-    // 4: class (stable)
+    if ((rc = radix_sort_pairs(ctx, k_sch, k64, perm_a, perm_b, n, 64, s)) != PFE_OK) return rc;
     k_gather_t<unsigned char><<<nb256, 256, 0, s>>>(raw.cls, perm_b, k8, npairs);
-    tt = tb;
-    PFE_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tt, k8, k8b, perm_b, perm_a, n, 0, 8, s));
+    if ((rc = radix_sort_pairs(ctx, k8, k8b, perm_b, perm_a, n, 8, s)) != PFE_OK) return rc;
     k_mol_gather<<<(unsigned)((npairs + 127) / 128), 128, 0, s>>>(raw, ctx->pairs, perm_a, npairs);
     PFE_CUDA(cudaGetLastError());
     PFE_CUDA(cudaStreamSynchronize(s));
-    ctx->free_now(tmp);
   }
-  for (void* p : {(void*)gbits, (void*)k_sch, (void*)k_gmax, (void*)k64, (void*)perm_a, (void*)perm_b, (void*)k32,
-                  (void*)k32b, (void*)k8, (void*)k8b})
-    ctx->free_now(p);
   int hcount[8] = {0};
   PFE_CUDA(cudaMemcpy(hcount, d_count, sizeof(int) * 8, cudaMemcpyDeviceToHost));
-  ctx->free_now(d_count);
-  free_pairs(ctx, &raw);
   int off = 0;
   for (int c = 0; c < 6; ++c) {
     ctx->class_off[c] = off;
     ctx->class_n[c] = hcount[c];
     off += hcount[c];
   }
+  // groups: runs of one gid in the sorted pairs
+  int *head = nullptr, *gix = nullptr;
+  PFE_CUDA(ctx->alloc((void**)&head, sizeof(int) * npairs));
+  PFE_CUDA(ctx->alloc((void**)&gix, sizeof(int) * npairs));
+  k_group_heads<<<nb256, 256, 0, s>>>(ctx->pairs.gid, head, npairs);
+  if ((rc = exclusive_sum(ctx, head, gix, (int)npairs, s)) != PFE_OK) return rc;
+  int last_gix = 0, last_head = 0;
+  PFE_CUDA(cudaMemcpyAsync(&last_gix, gix + npairs - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaMemcpyAsync(&last_head, head + npairs - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaStreamSynchronize(s));
+  const int ng = last_gix + last_head;
+  ctx->ngroups = ng;
+  unsigned char *gr_cls = nullptr, *bkey = nullptr, *bkey_sorted = nullptr;
+  int* giota = nullptr;
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_gr_start, sizeof(int) * ng));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_gr_n, sizeof(int) * ng));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_gr_max, sizeof(double) * ng));
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_bk_list, sizeof(int) * ng));
+  PFE_CUDA(ctx->alloc((void**)&gr_cls, ng));
+  PFE_CUDA(ctx->alloc((void**)&bkey, ng));
+  PFE_CUDA(ctx->alloc((void**)&bkey_sorted, ng));
+  PFE_CUDA(ctx->alloc((void**)&giota, sizeof(int) * ng));
+  k_group_fill<<<nb256, 256, 0, s>>>(head, gix, ctx->pairs.schwarz, ctx->pairs.cls, ctx->d_gr_start, ctx->d_gr_max,
+                                     gr_cls, npairs);
+  k_group_size<<<(ng + 255) / 256, 256, 0, s>>>(ctx->d_gr_start, gr_cls, ng, npairs, ctx->d_gr_n, bkey);
+  k_mol_iota<<<(ng + 255) / 256, 256, 0, s>>>(giota, ng);
+  PFE_CUDA(cudaGetLastError());
+  if ((rc = radix_sort_pairs(ctx, bkey, bkey_sorted, giota, ctx->d_bk_list, ng, 8, s)) != PFE_OK) return rc;
+  std::vector<unsigned char> h_cls(ng), h_bkey(ng);
+  PFE_CUDA(cudaMemcpyAsync(h_cls.data(), gr_cls, ng, cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaMemcpyAsync(h_bkey.data(), bkey_sorted, ng, cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaStreamSynchronize(s));
+  int cg0[6], cgn[6];
+  for (int c = 0; c < 6; ++c) { cg0[c] = 0; cgn[c] = 0; }
+  for (int g = ng - 1; g >= 0; --g) { cg0[h_cls[g]] = g; ++cgn[h_cls[g]]; }
+  Segs seg[6];
+  for (int c = 0; c < 6; ++c)
+    for (int b = 0; b < NBUCKET; ++b) seg[c].s0[b] = seg[c].s1[b] = 0;
+  for (int i = 0; i < ng; ++i) {
+    const int c = h_bkey[i] >> 3, b = h_bkey[i] & 7;
+    if (seg[c].s1[b] == 0) seg[c].s0[b] = i;
+    seg[c].s1[b] = i + 1;
+  }
   // chunk lists for every class pair cb >= ck
   ctx->nlaunch = 0;
   ctx->census_quartets = ctx->census_flops = ctx->census_ref = 0.0;
-  const int maxn = *std::max_element(ctx->class_n, ctx->class_n + 6);
-  int *nrange = nullptr, *nchunk = nullptr, *offs = nullptr, *nquart = nullptr;
-  long long* d_sum = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&nrange, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&nchunk, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&offs, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&nquart, sizeof(int) * (maxn + 1)));
-  PFE_CUDA(ctx->alloc((void**)&d_sum, sizeof(long long)));
+  int maxg = 1;
+  for (int c = 0; c < 6; ++c) maxg = std::max(maxg, cgn[c]);
+  int *nchunk = nullptr, *offs = nullptr;
+  unsigned long long* d_total = nullptr;
+  PFE_CUDA(ctx->alloc((void**)&nchunk, sizeof(int) * (maxg + 1)));
+  PFE_CUDA(ctx->alloc((void**)&offs, sizeof(int) * (maxg + 1)));
+  PFE_CUDA(ctx->alloc((void**)&d_total, sizeof(unsigned long long)));
   for (int cb = 0; cb < 6; ++cb)
     for (int ck = 0; ck <= cb; ++ck) {
-      const int nb = ctx->class_n[cb], nk = ctx->class_n[ck];
-      if (nb == 0 || nk == 0) continue;
-      const int b0 = ctx->class_off[cb], k0 = ctx->class_off[ck];
-      k_mol_count<<<(nb + 127) / 128, 128, 0, s>>>(ctx->pairs.schwarz, ctx->pairs.gmax, b0, nb, k0, nk, cb == ck,
-                                                   ctx->inttol, nrange, nchunk, nquart);
-      PFE_CUDA(cudaGetLastError());
-      PFE_CUDA(cudaMemsetAsync(nchunk + nb, 0, sizeof(int), s));
-      size_t sb = 0;
-      cub::DeviceScan::ExclusiveSum(nullptr, sb, nchunk, offs, nb + 1, s);
-      void* st = nullptr;
-      PFE_CUDA(ctx->alloc(&st, sb + 16));
-      PFE_CUDA(cub::DeviceScan::ExclusiveSum(st, sb, nchunk, offs, nb + 1, s));
-      size_t rb = 0;
-      cub::DeviceReduce::Sum(nullptr, rb, nquart, d_sum, nb, s);
-      void* rt = nullptr;
-      PFE_CUDA(ctx->alloc(&rt, rb + 16));
-      PFE_CUDA(cub::DeviceReduce::Sum(rt, rb, nquart, d_sum, nb, s));
+      const int nbg = cgn[cb];
+      bool any = false;
+      for (int b = 0; b < NBUCKET; ++b) any = any || seg[ck].s1[b] > seg[ck].s0[b];
+      if (nbg == 0 || !any) continue;
+      k_chunk_count<<<(nbg + 127) / 128, 128, 0, s>>>(ctx->d_gr_max, ctx->d_bk_list, cg0[cb], nbg, seg[ck], cb == ck,
+                                                      ctx->inttol, nchunk);
+      PFE_CUDA(cudaMemsetAsync(nchunk + nbg, 0, sizeof(int), s));
+      if ((rc = exclusive_sum(ctx, nchunk, offs, nbg + 1, s)) != PFE_OK) return rc;
       int total = 0;
-      long long nq = 0;
-      PFE_CUDA(cudaMemcpyAsync(&total, offs + nb, sizeof(int), cudaMemcpyDeviceToHost, s));
-      PFE_CUDA(cudaMemcpyAsync(&nq, d_sum, sizeof(long long), cudaMemcpyDeviceToHost, s));
+      PFE_CUDA(cudaMemcpyAsync(&total, offs + nbg, sizeof(int), cudaMemcpyDeviceToHost, s));
       PFE_CUDA(cudaStreamSynchronize(s));
-      ctx->free_now(st);
-      ctx->free_now(rt);
       if (total == 0) continue;
       ClassLaunch cl{};
       cl.cb = cb;
       cl.ck = ck;
       cl.nchunks_host = total;
-      cl.quartets = (double)nq;
       PFE_CUDA(ctx->alloc((void**)&cl.chunks, sizeof(int4) * total));
       PFE_CUDA(ctx->alloc((void**)&cl.d_nchunks, sizeof(int)));
       PFE_CUDA(cudaMemcpyAsync(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice, s));
-      k_mol_fill<<<(nb + 127) / 128, 128, 0, s>>>(nrange, offs, b0, k0, nb, cl.chunks);
+      k_chunk_fill<<<(nbg + 127) / 128, 128, 0, s>>>(ctx->d_gr_max, ctx->d_bk_list, cg0[cb], nbg, seg[ck], cb == ck,
+                                                     ctx->inttol, offs, cl.chunks);
+      PFE_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
+      k_chunk_census<<<(total + 3) / 4, 128, 0, s>>>(cl.chunks, total, ctx->d_bk_list, ctx->d_gr_start, ctx->d_gr_n,
+                                                     ctx->pairs.schwarz, ctx->inttol, d_total);
       PFE_CUDA(cudaGetLastError());
+      unsigned long long nq = 0;
+      PFE_CUDA(cudaMemcpyAsync(&nq, d_total, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       PFE_CUDA(cudaStreamSynchronize(s));
+      cl.quartets = (double)nq;
       cl.has_straight = straight_launcher(cb, ck) != nullptr;
       cl.has_table = false;
       cl.variant = 0;
+      cl.xg = nullptr;
       if (const OpTableHost* h = host_optable(cb, ck)) {
         OpTableDev d{};
         if ((rc = upload_optable(ctx, h, &d)) != PFE_OK) return rc;
+        const Variants vv = variants(cb, ck);
         cl.has_table = true;
         cl.ops = d.ops; cl.levels = d.levels; cl.out = d.out;
         cl.nlevels = d.nlevels; cl.nout = d.nout; cl.nslots = d.nslots;
-        cl.smem_big = sizeof(double) * ((size_t)h->nslots + density_block_doubles(cb, ck));
-        cl.per_warp = h->nslots + density_block_doubles(cb, ck);
-        cl.wpb = (int)std::max<size_t>(1, std::min<size_t>(8, (200 * 1024) / (sizeof(double) * cl.per_warp)));
+        cl.per_warp = vv.doubles(h->nslots, true);
+        cl.smem_big = sizeof(double) * (size_t)cl.per_warp;
+        {  // warps per block that fit the most warps per SM in shared memory (228 KB, ~3 KB static per block)
+          const size_t pw = sizeof(double) * (size_t)cl.per_warp;
+          int best = 1, best_w = 0;
+          for (int w = 1; w <= 8; ++w) {
+            if (w * pw > 200 * 1024) break;
+            const int resident = w * (int)((228 * 1024) / (w * pw + 3 * 1024));
+            if (resident >= best_w) { best_w = resident; best = w; }
+          }
+          cl.wpb = best;
+        }
         cl.smem_warp = sizeof(double) * (size_t)cl.per_warp * cl.wpb;
-        PFE_CUDA(variants(cb, ck).allow(cl.smem_big, cl.smem_warp));
-        cl.variant = (cl.has_straight && h->nout <= 100) ? 0 : (sizeof(double) * cl.per_warp <= 100 * 1024 ? 1 : 2);
+        if (cl.smem_big > 220 * 1024) {   // X to global scratch, one slice per block of the block variant
+          cl.smem_big = sizeof(double) * (size_t)vv.doubles(h->nslots, false);
+          if (cl.smem_big > 220 * 1024) {
+            set_error("op-table working set of a quartet class exceeds shared memory");
+            return PFE_EUNSUPPORTED;
+          }
+          PFE_CUDA(ctx->alloc((void**)&cl.xg, sizeof(double) * (size_t)h->nout * 2 * ctx->num_sms));
+        }
+        PFE_CUDA(vv.allow(cl.smem_big, std::min<size_t>(cl.smem_warp, 220 * 1024)));
+        cl.variant = cl.has_straight ? 0 : (cl.smem_warp <= 200 * 1024 && cl.per_warp * sizeof(double) <= 100 * 1024 ? 1 : 2);
+      }
+      if (!cl.has_straight && !cl.has_table) {
+        set_error("no kernel for a quartet class");
+        return PFE_EUNSUPPORTED;
       }
       for (int v = 0; v < 3; ++v) cl.tuned_ms[v] = 0.f;
       ctx->launches[ctx->nlaunch++] = cl;
       ctx->census_quartets += (double)nq;
       ctx->census_flops += (double)nq * class_flops(cb, ck);
     }
-  for (void* p : {(void*)nrange, (void*)nchunk, (void*)offs, (void*)nquart, (void*)d_sum}) ctx->free_now(p);
-  // the reference's loop visits both orders of every pair and of bra/ket: 8x the unique quartets
-  ctx->census_ref = 0.0;
+  ctx->free_now(d_count);
+  free_pairs(ctx, &raw);
+  for (void* p : {(void*)gbits, (void*)k_sch, (void*)k_gmax, (void*)k64, (void*)perm_a, (void*)perm_b, (void*)k32,
+                  (void*)k32b, (void*)k8, (void*)k8b, (void*)head, (void*)gix, (void*)gr_cls, (void*)bkey,
+                  (void*)bkey_sorted, (void*)giota, (void*)nchunk, (void*)offs, (void*)d_total})
+    ctx->free_now(p);
   ctx->free_pending();
   return PFE_OK;
 }
 
 // ------------------------------------------------------------------ build
 
-static MolLaunch make_launch(pfe_context* ctx, const double* d_pp) {
+static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   MolLaunch ql{};
   ql.pairs = ctx->pairs;
   ql.prim = ctx->shells.prim;
   ql.tidx = ctx->d_tidx;
   ql.tcoef = ctx->d_tcoef;
   ql.boys = ctx->d_boys;
-  ql.density = d_pp;
+  ql.dt = d_dt;
   ql.jt = ctx->d_jp;
   ql.kt = ctx->d_kp;
+  ql.gr_start = ctx->d_gr_start;
+  ql.gr_n = ctx->d_gr_n;
+  ql.gr_max = ctx->d_gr_max;
+  ql.bk_list = ctx->d_bk_list;
   ql.inttol = ctx->inttol;
-  ql.npgs = ctx->npgs;
   ql.nt = ctx->nt;
   ql.myid = ctx->myid;
   ql.numprocs = ctx->numprocs;
@@ -955,7 +1105,7 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
   ql.chunks = cl.chunks;
   ql.nchunks = cl.d_nchunks;
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
-  if (variant == 0 || !cl.has_table) {
+  if ((variant == 0 && cl.has_straight) || !cl.has_table) {
     const int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
     straight_launcher(cl.cb, cl.ck)(ql, std::max(grid, 1), s);
     return;
@@ -965,15 +1115,35 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
     const int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
     variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);
   } else {
-    const int grid = std::min(work, ctx->num_sms * 2);
-    variants(cl.cb, cl.ck).big(ql, t, std::max(grid, 1), cl.smem_big, s);
+    const int grid = std::min(work, ctx->num_sms * 2);   // cl.xg holds 2 * num_sms slices
+    variants(cl.cb, cl.ck).big(ql, t, cl.xg, std::max(grid, 1), cl.smem_big, s);
   }
 }
 
 static size_t target_bytes(const pfe_context* ctx) { return sizeof(double) * (size_t)ctx->nt * ctx->nt; }
 
+// Density in target space: P_P itself (primitive targets) or P_C read off P_P
+// and checked (contracted targets); returns the pointer the kernels read.
+static const double* target_density(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
+  if (!ctx->contracted) return d_pp;
+  const long long nt2 = (long long)ctx->nt * ctx->nt, np2 = (long long)ctx->npgs * ctx->npgs;
+  k_target_density<<<(unsigned)((nt2 + 255) / 256), 256, 0, s>>>(d_pp, ctx->npgs, ctx->d_rep, ctx->d_repc, ctx->nt,
+                                                                   ctx->d_pt);
+  cudaMemsetAsync(ctx->d_flag, 0, sizeof(unsigned int), s);
+  k_check_density<<<(unsigned)((np2 + 255) / 256), 256, 0, s>>>(d_pp, ctx->npgs, ctx->d_tidx, ctx->d_tcoef,
+                                                                  ctx->d_pt, ctx->nt, ctx->d_flag);
+  return ctx->d_pt;
+}
+
+static bool variant_ok(const ClassLaunch& cl, int v) {
+  if (v == 0) return cl.has_straight;
+  if (v == 1) return cl.has_table && cl.smem_warp <= 200 * 1024;
+  return cl.has_table;
+}
+
 int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
-  const MolLaunch ql = make_launch(ctx, d_pp);
+  const MolLaunch ql = make_launch(ctx, target_density(ctx, d_pp, s));
+  PFE_CUDA(cudaGetLastError());
   cudaEvent_t e0, e1;
   PFE_CUDA(cudaEventCreate(&e0));
   PFE_CUDA(cudaEventCreate(&e1));
@@ -982,8 +1152,7 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
     float best = 1e30f;
     int bestv = cl.variant;
     for (int v = 0; v < 3; ++v) {
-      if ((v == 0 && !cl.has_straight) || (v > 0 && !cl.has_table)) continue;
-      if (v == 1 && sizeof(double) * (size_t)cl.per_warp > 200 * 1024) continue;
+      if (!variant_ok(cl, v)) continue;
       launch_class(ctx, cl, ql, v, s);
       float t = 1e30f;
       for (int r = 0; r < 2; ++r) {
@@ -1010,10 +1179,10 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
   return PFE_OK;
 }
 
-int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s) {
+static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double* d_xc, cudaStream_t s) {
   PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, target_bytes(ctx), s));
-  const MolLaunch ql = make_launch(ctx, d_pp);
+  const MolLaunch ql = make_launch(ctx, d_dt);
   if (ctx->profile) {
     for (int i = 0; i <= ctx->nlaunch && i < 64; ++i)
       if (!ctx->ev[i]) PFE_CUDA(cudaEventCreate(&ctx->ev[i]));
@@ -1040,6 +1209,42 @@ int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d
     return PFE_OK;
   }
   return contract_outputs(ctx, ctx->d_jp, ctx->d_kp, d_cc, d_xc, /*symmetrize=*/true, 1, s);
+}
+
+int molecular_fock(pfe_context* ctx, const double* d_pp, double* d_cc, double* d_xc, cudaStream_t s) {
+  const double* d_dt = target_density(ctx, d_pp, s);
+  PFE_CUDA(cudaGetLastError());
+  return run_build(ctx, d_dt, d_cc, d_xc, s);
+}
+
+// Build from the contracted density P_C (ncgs x ncgs): read directly as the
+// target-space density, or decontracted on the device (P_P = CC^T P_C CC,
+// src/pdensitymatrix.f90:343-381) for primitive targets.
+int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s) {
+  if (ctx->contracted) return run_build(ctx, d_pc, d_cc, d_xc, s);
+  const int np = ctx->npgs, nc = ctx->ncgs;
+  const double one = 1.0, zero = 0.0;
+  cublasSetStream(ctx->blas, s);
+  // W1 = P_C . CC (nc x np); P_P = CC^T . W1 (np x np) into the target-density buffer
+  cublasStatus_t st = cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, np, nc, &one, d_pc, nc, ctx->d_cc, nc, &zero,
+                                  ctx->d_w1, nc);
+  if (st != CUBLAS_STATUS_SUCCESS) { set_error("cublasDgemm (P_C.CC) failed"); return PFE_ECUDA; }
+  st = cublasDgemm(ctx->blas, CUBLAS_OP_T, CUBLAS_OP_N, np, np, nc, &one, ctx->d_cc, nc, ctx->d_w1, nc, &zero,
+                   ctx->d_pt, np);
+  if (st != CUBLAS_STATUS_SUCCESS) { set_error("cublasDgemm (CC^T.W) failed"); return PFE_ECUDA; }
+  return run_build(ctx, ctx->d_pt, d_cc, d_xc, s);
+}
+
+// Whether the last build's P_P was the decontraction of a contracted density
+// (always true for primitive targets).  Synchronises the stream.
+int molecular_density_ok(pfe_context* ctx, cudaStream_t s, bool* ok) {
+  *ok = true;
+  if (!ctx->contracted || !ctx->molecular) return PFE_OK;
+  unsigned int f = 0;
+  PFE_CUDA(cudaMemcpyAsync(&f, ctx->d_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+  PFE_CUDA(cudaStreamSynchronize(s));
+  *ok = (f == 0);
+  return PFE_OK;
 }
 
 }  // namespace pfe
