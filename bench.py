@@ -240,6 +240,7 @@ def main():
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-scf', action='store_true', help='skip the time-to-converged SCF leg')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':
@@ -319,7 +320,7 @@ def main():
     if dom:
         ach = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
         traffic = ncu_traffic_per_launch()
-        kname = ['k_quartets', 'k_quartets_warp', 'k_quartets_big'][dom['variant']]
+        kname = ['k_gq', 'k_gq_warp', 'k_gq_block'][dom['variant']]
         roof = {'bound': 'fp64', 'kernel': '%s<%s>' % (kname, dom['cls']), 'achieved': ach, 'peak': peak,
                 'unit': 'TFLOP/s', 'frac': ach / peak if peak else None,
                 'peak_source': 'measured in this run: DFMA loop over all SMs (pfe_measure_fp64_peak); '
@@ -355,6 +356,34 @@ def main():
                'ms_per_step': 1e3 * sum(walls) / args.steps,
                'path': 'pfe_fourindex_eri (host pointers; static inputs cached on the device by content hash)'}
 
+    # ---- time to a converged SCF (1e-8 RMS density): the reference's loop with full FP64
+    # builds against the time-to-solution path (commutator DIIS, incremental density-screened
+    # builds), both judged by E[P] of the final idempotent density with full FP64 J/K
+    scf_line = None
+    if rank == 0 and world == 1 and not args.no_scf:
+        from polymer_b200 import scf
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r_plain = scf.run_scf(sysm, df, device=dev, variational=True)
+        torch.cuda.synchronize()
+        t_plain = time.perf_counter() - t0
+        opts = scf.FastOptions()
+        t0 = time.perf_counter()
+        r_fast = scf.run_scf_fast(sysm, df, opts=opts, device=dev)
+        torch.cuda.synchronize()
+        t_fast = time.perf_counter() - t0
+        scf_line = {'converged_to': 'RMS density change < %g' % sysm.deck.scfconv,
+                    'plain_fp64_s': t_plain, 'plain_iterations': len(r_plain.iterations),
+                    'fast_s': t_fast, 'fast_iterations': len(r_fast.iterations),
+                    'speedup': t_plain / t_fast,
+                    'energy_plain': r_plain.energy_variational, 'energy_fast': r_fast.energy,
+                    'abs_dE': abs(r_fast.energy - r_plain.energy_variational),
+                    'fast_path': 'commutator DIIS; incremental builds from dP_C with density screening %g, '
+                                 'full rebuild every %d; final full FP64 iteration' % (opts.density_tol,
+                                                                                      opts.reset_every),
+                    'plain_path': "reference loop (nuclear-charge guess, density DIIS), full FP64 builds",
+                    'wall_clock': 'host time around each SCF, GPU synchronised'}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sysm, p_p.cpu().numpy())
@@ -370,7 +399,8 @@ def main():
                            if world > 1 else 'single GPU'},
                 'quartets_per_build': cen['quartets'], 'quartets_per_s': cen['quartets'] * value,
                 'gpu_launches': args.steps * int(cen['kernel_launches']),
-                'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'cpu_baseline': cpu}
+                'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'scf': scf_line,
+                'cpu_baseline': cpu}
         print(json.dumps(line))
     df.close()
     if world > 1:

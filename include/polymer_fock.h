@@ -105,6 +105,17 @@ int32_t pfe_context_fock(pfe_context *ctx, const double *d_p_p, const double *d_
  * asynchronous.  Replaces DECONTRACT_DENSITYMATRIX + FOURINDEX_ERI. */
 int32_t pfe_context_fock_pc(pfe_context *ctx, const double *d_p_c, double *d_c_c, double *d_x_c, void *stream);
 
+/* Runtime screening of molecular builds (no counterpart in the reference, whose
+ * only screen is Schwarz(ij)*Schwarz(kl) < INTTOL).  With M = max|P| over the
+ * density blocks a contracted shell quartet digests against: quartets with
+ * Schwarz(ij)*Schwarz(kl)*M < density_tol are skipped (0 = off), and with
+ * PFE_PREC_MIXED those with Schwarz(ij)*Schwarz(kl)*M < mixed_cutoff run the
+ * recursion in FP32 (Boys function, geometry, contraction and J/K in FP64).
+ * Meant for incremental builds from density differences.  Lattices: FP64 and
+ * no density screening only (PFE_EUNSUPPORTED otherwise). */
+int32_t pfe_context_set_screening(pfe_context *ctx, int32_t precision_mode, double mixed_cutoff,
+                                  double density_tol);
+
 /* Digest into primitive targets (then contract with CC on cuBLAS) even when
  * contracted targets are possible; takes effect at the next pfe_context_setup.
  * For callers whose P_P is not a decontracted density.  No counterpart in the

@@ -113,6 +113,8 @@ def lib(path: str = LIB_PATH):
     L.pfe_context_fock_pc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                       ctypes.c_void_p]
     L.pfe_context_fock_pc.restype = ctypes.c_int32
+    L.pfe_context_set_screening.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double]
+    L.pfe_context_set_screening.restype = ctypes.c_int32
     L.pfe_context_primitive_targets.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     L.pfe_context_primitive_targets.restype = ctypes.c_int32
     L.pfe_context_census.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeCensus)]
@@ -156,4 +158,4 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_nuclear_attraction', 'pfe_context_profile', 'pfe_context_kernel_stats',
            'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
            'pfe_version', 'pfe_overlap_kinetic_noalloc', 'pfe_context_fock_pc',
-           'pfe_context_primitive_targets']
+           'pfe_context_primitive_targets', 'pfe_context_set_screening']

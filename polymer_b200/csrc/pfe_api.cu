@@ -192,6 +192,9 @@ static void reset_context(pfe_context* ctx) {
   ctx->d_blk = nullptr;
   ctx->d_rep = nullptr;
   ctx->d_repc = nullptr;
+  ctx->d_tblk = nullptr;
+  ctx->d_bmax = nullptr;
+  ctx->d_n32 = nullptr;
   ctx->d_pt = nullptr;
   ctx->d_flag = nullptr;
   ctx->d_gr_start = ctx->d_gr_n = ctx->d_bk_list = nullptr;
@@ -225,6 +228,13 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
   ctx->numprocs = a->numprocs;
   ctx->precision = a->precision_mode;
   ctx->mixed_cutoff = a->mixed_cutoff;
+  if (a->precision_mode != PFE_PREC_FP64 && a->precision_mode != PFE_PREC_MIXED) {
+    set_error("precision_mode must be PFE_PREC_FP64 or PFE_PREC_MIXED");
+    return PFE_EINVAL;
+  }
+  if (!(a->mixed_cutoff >= 0.0)) { set_error("mixed_cutoff must be >= 0"); return PFE_EINVAL; }
+  ctx->mcut = a->precision_mode == PFE_PREC_MIXED ? a->mixed_cutoff : 0.0;
+  ctx->dtol = 0.0;
   ctx->molecular = (ctx->ncell1 == 1 && a->cel2[0] == 0 && a->cel2[1] == 0 && a->cel2[2] == 0 && a->helix == 0.0);
   cudaStream_t s = ctx->stream;
   const int n = a->npshell;
@@ -337,6 +347,18 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
       const int r = tidx[p];
       if (r >= 0 && std::fabs(tcoef[p]) > std::fabs(repc[r])) { rep[r] = p; repc[r] = tcoef[p]; }
     }
+    // block of every target, for the per-block density maxima
+    std::vector<int> tblk(ctx->nt, -1);
+    for (int sh = 0; sh < a->npshell; ++sh)
+      for (int c = 0; c < ncum(hs.L[sh]); ++c) {
+        const int t = tidx[hs.prim[(size_t)sh * MAXCOMP + c]];
+        if (t >= 0) tblk[t] = blk[sh];
+      }
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_tblk, sizeof(int) * ctx->nt));
+    PFE_CUDA(cudaMemcpy(ctx->d_tblk, tblk.data(), sizeof(int) * ctx->nt, cudaMemcpyHostToDevice));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_bmax, sizeof(double) * (size_t)ctx->nblk * ctx->nblk));
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_n32, sizeof(unsigned long long)));
+    PFE_CUDA(cudaMemset(ctx->d_n32, 0, sizeof(unsigned long long)));
     PFE_CUDA(ctx->alloc((void**)&ctx->d_rep, sizeof(int) * ctx->nt));
     PFE_CUDA(ctx->alloc((void**)&ctx->d_repc, sizeof(double) * ctx->nt));
     PFE_CUDA(ctx->alloc((void**)&ctx->d_pt, sizeof(double) * (size_t)ctx->nt * ctx->nt));
@@ -462,6 +484,22 @@ int32_t pfe_context_fock_pc(pfe_context* ctx, const double* d_p_c, double* d_c_c
   return molecular_fock_pc(ctx, d_p_c, d_c_c, d_x_c, (cudaStream_t)stream);
 }
 
+int32_t pfe_context_set_screening(pfe_context* ctx, int32_t precision_mode, double mixed_cutoff, double density_tol) {
+  if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
+  if (precision_mode != PFE_PREC_FP64 && precision_mode != PFE_PREC_MIXED) {
+    set_error("precision_mode must be PFE_PREC_FP64 or PFE_PREC_MIXED");
+    return PFE_EINVAL;
+  }
+  if (!(mixed_cutoff >= 0.0) || !(density_tol >= 0.0)) { set_error("cutoffs must be >= 0"); return PFE_EINVAL; }
+  if (!ctx->molecular && (precision_mode != PFE_PREC_FP64 || density_tol != 0.0)) {
+    set_error("mixed precision and density screening are implemented for molecules only");
+    return PFE_EUNSUPPORTED;
+  }
+  ctx->mcut = precision_mode == PFE_PREC_MIXED ? mixed_cutoff : 0.0;
+  ctx->dtol = density_tol;
+  return PFE_OK;
+}
+
 int32_t pfe_context_primitive_targets(pfe_context* ctx, int32_t enable) {
   if (!ctx) { set_error("null context"); return PFE_EINVAL; }
   if (ctx->force_primitive != (enable != 0)) {
@@ -477,9 +515,25 @@ int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
   out->quartets = ctx->census_quartets;
   out->quartets_ref = ctx->census_ref;
   out->flops = ctx->census_flops;
-  out->quartets_fp32 = ctx->census_fp32;
+  out->quartets_fp32 = 0.0;
+  if (ctx->molecular && ctx->d_n32) {
+    unsigned long long n32 = 0;
+    PFE_CUDA(cudaMemcpy(&n32, ctx->d_n32, sizeof(n32), cudaMemcpyDeviceToHost));
+    out->quartets_fp32 = (double)n32;
+  }
   out->pairs = ctx->npairs;
-  out->kernel_launches = ctx->nlaunch + (ctx->molecular ? 2 : 3);
+  if (ctx->molecular) {
+    // class kernels (straight-line passes), the target-space density and its check,
+    // the two symmetrisations (primitive targets: the contraction is cuBLAS), the block
+    // maxima under density screening or mixed precision
+    int n = 0;
+    for (int i = 0; i < ctx->nlaunch; ++i)
+      n += (ctx->launches[i].variant == 0 && ctx->launches[i].has_straight) ? ctx->launches[i].npass : 1;
+    n += (ctx->contracted ? 2 : 0) + 2 + ((ctx->dtol > 0.0 || ctx->mcut > 0.0) ? 1 : 0);
+    out->kernel_launches = n;
+  } else {
+    out->kernel_launches = ctx->nlaunch + 3;
+  }
   return PFE_OK;
 }
 

@@ -54,6 +54,7 @@ struct ClassLaunch {
   size_t smem_big, smem_warp;
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
   double* xg;                // block variant: per-block X scratch in global memory, or null
+  int npass;                 // launches of the straight-line variant
 };
 
 }  // namespace pfe
@@ -104,6 +105,13 @@ struct pfe_context {
   int* d_gr_n = nullptr;
   double* d_gr_max = nullptr;
   int* d_bk_list = nullptr;  // group ids ordered by (class, size bucket, group)
+  // density-dependent screening of molecular builds (no counterpart in the reference, which
+  // screens by the Schwarz bounds alone): skip quartets with bound * max|P| < dtol, and run
+  // the recursion in FP32 where bound * max|P| < mcut; max|P| per pair of contracted blocks
+  double dtol = 0.0, mcut = 0.0;
+  int* d_tblk = nullptr;     // target -> block (-1: none)
+  double* d_bmax = nullptr;  // nblk x nblk block maxima of |P_T| of the last build
+  unsigned long long* d_n32 = nullptr;  // quartets of the last build run in FP32
   double* d_w1 = nullptr;
   double* d_w2 = nullptr;
   pfe::PairArrays pairs{};

@@ -43,30 +43,11 @@
 #include "pfe_context.cuh"
 #include "pfe_interp.cuh"
 #include "generated/eri_classes.cuh"
+#include "pfe_mol_kernels.cuh"
 
 namespace pfe {
 
 constexpr int NBUCKET = 6;   // ket-group size buckets: 1, 2-3, 4-7, 8-15, 16-31, 32+
-
-struct MolLaunch {
-  PairArrays pairs;
-  const int* prim;        // shell components -> primitive
-  const int* tidx;        // primitive -> target row (-1: none)
-  const double* tcoef;    // primitive -> coefficient
-  const double* boys;
-  const double* dt;       // density in target space (nt x nt, column-major)
-  double* jt;             // J' targets (nt x nt)
-  double* kt;             // K' targets
-  const int* gr_start;    // group -> first pair
-  const int* gr_n;        // group -> number of pairs
-  const double* gr_max;   // group -> largest bound
-  const int* bk_list;     // ket groups by (class, bucket, group)
-  const int4* chunks;     // (bra group, first list entry, end list entry, 0)
-  const int* nchunks;
-  double inttol;
-  int nt;
-  int myid, numprocs;
-};
 
 static const int kCL[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
 
@@ -304,205 +285,15 @@ __global__ void k_check_density(const double* __restrict__ pp, int npgs, const i
   if (!(fabs(got - want) <= 1e-12 * fmax(fabs(got), fabs(want)))) atomicOr(flag, 1u);
 }
 
-// ------------------------------------------------------------------ digestion helpers
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-__device__ __forceinline__ void add_target(double* __restrict__ M, int nt, int r, int c, double v) {
-  if (r >= 0 && c >= 0 && v != 0.0) atomicAdd(M + r + (size_t)nt * c, v);
-}
-
-__device__ __forceinline__ double dt_at(const double* __restrict__ D, int nt, int i, int j) {
-  return (i >= 0 && j >= 0) ? __ldg(D + i + (size_t)nt * j) : 0.0;
-}
-
-// ------------------------------------------------------------------ straight-line classes
-
-// One group quartet per lane: the warp shares the bra group, each lane owns one
-// ket group of the chunk.  X(abcd) of the lane's group quartet stays in
-// registers; the bra's primitive pairs are walked in step by the whole warp.
-// Classes with more integrals than registers hold X in NPASS launches, pass
-// PASS keeping the bra components ab in [AB0, AB1) (the recursion is repeated
-// per pass; the outputs a pass does not keep are dead code in it).
-template <int LA, int LB, int LC, int LD, int NPASS, int PASS>
-__global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
-  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
-  constexpr int NI = NA * NB * NC * ND;
-  constexpr int NAB = NA * NB;
-  constexpr int NCD = NC * ND;
-  constexpr int LT = LA + LB + LC + LD;
-  constexpr int ABP = (NAB + NPASS - 1) / NPASS;
-  constexpr int AB0 = PASS * ABP;
-  constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
-  constexpr int XN = (AB1 - AB0) * NCD;
-  const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
-  const int nchunks = *ql.nchunks;
-  const int stride = gridDim.x * wpb * ql.numprocs;
-  const double c2pi = 2.0 / sqrt(REF_PI);
-  const PairArrays pr = ql.pairs;
-  const int nt = ql.nt;
-  const double tol = ql.inttol;
-  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
-    const int4 ch = ql.chunks[c];
-    const int G = ch.x;
-    const int li = ch.y + lane;
-    const bool act = li < ch.z;
-    const int H = ql.bk_list[act ? li : ch.y];
-    const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
-    const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
-    const double hmax = act ? ql.gr_max[H] : 0.0;
-    double hmax_w = hmax;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) hmax_w = fmax(hmax_w, __shfl_xor_sync(0xffffffffu, hmax_w, o));
-    double X[XN];
-#pragma unroll
-    for (int i = 0; i < XN; ++i) X[i] = 0.0;
-    for (int p = g0; p < g0 + gn; ++p) {
-      const double sp = pr.schwarz[p];
-      if (sp * hmax_w < tol) break;   // every later bra pair fails for every lane
-      const int I = pr.si[p], J = pr.sj[p];
-      double cab[NAB];
-#pragma unroll
-      for (int ab = AB0; ab < AB1; ++ab)
-        cab[ab] = ql.tcoef[ql.prim[I * MAXCOMP + ab / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + ab % NB]];
-      const double zb = pr.zeta[p];
-      const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-      const double Sp = pr.S[p];
-      const double wIJ = (I != J) ? 2.0 : 1.0;
-      const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
-      for (int q = h0; q < qe; ++q) {
-        if (sp * pr.schwarz[q] < tol) break;   // the reference's screen; pairs sorted by bound
-        const double ze = pr.zeta[q];
-        const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
-        const double zz = zb + ze;
-        const double rho = zb * ze / zz;
-        const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
-        const double T = rho * (dx * dx + dy * dy + dz * dz);
-        const double pref = c2pi * Sp * pr.S[q] * sqrt(rho);
-        double F[LT + 1];
-        boys_tab<LT>(T, pref, ql.boys, F);
-        double out[NI];
-        if constexpr (LT == 0) {
-          out[0] = F[0];
-        } else {
-          EriGeom<double> g;
-          const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
-          g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
-          g.QC[0] = pr.PA[0][q]; g.QC[1] = pr.PA[1][q]; g.QC[2] = pr.PA[2][q];
-          g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
-          g.CD[0] = pr.AB[0][q]; g.CD[1] = pr.AB[1][q]; g.CD[2] = pr.AB[2][q];
-          g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
-          g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
-          g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
-          eri_dispatch<LA, LB, LC, LD>(F, g, out);
-        }
-        const int K = pr.si[q], L = pr.sj[q];
-        const double w = wIJ * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
-        double ccd[NCD];
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc) {
-          const double c1 = w * ql.tcoef[ql.prim[K * MAXCOMP + cc]];
-#pragma unroll
-          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.tcoef[ql.prim[L * MAXCOMP + d]];
-        }
-#pragma unroll
-        for (int ab = AB0; ab < AB1; ++ab)
-#pragma unroll
-          for (int cd = 0; cd < NCD; ++cd)
-            X[(ab - AB0) * NCD + cd] = fma(cab[ab] * ccd[cd], out[ab * NCD + cd], X[(ab - AB0) * NCD + cd]);
-      }
-    }
-    // digestion of this pass's part of X against the target-space density
-    const double* __restrict__ D = ql.dt;
-    const int I0 = pr.si[g0], J0 = pr.sj[g0], K0 = pr.si[h0], L0 = pr.sj[h0];
-    int ta[NA], tb[NB], tc[NC], td[ND];
-#pragma unroll
-    for (int x = 0; x < NA; ++x) ta[x] = ql.tidx[ql.prim[I0 * MAXCOMP + x]];
-#pragma unroll
-    for (int x = 0; x < NB; ++x) tb[x] = ql.tidx[ql.prim[J0 * MAXCOMP + x]];
-#pragma unroll
-    for (int x = 0; x < NC; ++x) tc[x] = ql.tidx[ql.prim[K0 * MAXCOMP + x]];
-#pragma unroll
-    for (int x = 0; x < ND; ++x) td[x] = ql.tidx[ql.prim[L0 * MAXCOMP + x]];
-    // X(abcd) of this pass (zero outside it: constant-folded in the unrolled loops)
-    auto XV = [&](int a, int b, int cc, int d) -> double {
-      const int ab = a * NB + b;
-      return (ab >= AB0 && ab < AB1) ? X[(ab - AB0) * NCD + cc * ND + d] : 0.0;
-    };
-    // J'(ab) += 1/4 sum_cd P(cd) X: the bra is the warp's, reduce over lanes first
-#pragma unroll
-    for (int ab = AB0; ab < AB1; ++ab) {
-      double v = 0.0;
-#pragma unroll
-      for (int cc = 0; cc < NC; ++cc)
-#pragma unroll
-        for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tc[cc], td[d]), X[(ab - AB0) * NCD + cc * ND + d], v);
-      v = warp_sum(v);
-      if (lane == 0) add_target(ql.jt, nt, ta[ab / NB], tb[ab % NB], 0.25 * v);
-    }
-    if (act) {
-      // J'(cd) += 1/4 sum_ab P(ab) X
-      double Pab[NAB];
-#pragma unroll
-      for (int ab = AB0; ab < AB1; ++ab) Pab[ab] = dt_at(D, nt, ta[ab / NB], tb[ab % NB]);
-#pragma unroll
-      for (int cd = 0; cd < NCD; ++cd) {
-        double v = 0.0;
-#pragma unroll
-        for (int ab = AB0; ab < AB1; ++ab) v = fma(Pab[ab], X[(ab - AB0) * NCD + cd], v);
-        add_target(ql.jt, nt, tc[cd / ND], td[cd % ND], 0.25 * v);
-      }
-      // K'(ad) += 1/8 P(bc) X ; K'(ac) += 1/8 P(bd) X
-#pragma unroll
-      for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a) {
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-          double v = 0.0;
-#pragma unroll
-          for (int b = 0; b < NB; ++b)
-#pragma unroll
-            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, tb[b], tc[cc]), XV(a, b, cc, d), v);
-          add_target(ql.kt, nt, ta[a], td[d], 0.125 * v);
-        }
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc) {
-          double v = 0.0;
-#pragma unroll
-          for (int b = 0; b < NB; ++b)
-#pragma unroll
-            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tb[b], td[d]), XV(a, b, cc, d), v);
-          add_target(ql.kt, nt, ta[a], tc[cc], 0.125 * v);
-        }
-      }
-      // K'(bd) += 1/8 P(ac) X ; K'(bc) += 1/8 P(ad) X
-#pragma unroll
-      for (int b = 0; b < NB; ++b) {
-#pragma unroll
-        for (int d = 0; d < ND; ++d) {
-          double v = 0.0;
-#pragma unroll
-          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
-#pragma unroll
-            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, ta[a], tc[cc]), XV(a, b, cc, d), v);
-          add_target(ql.kt, nt, tb[b], td[d], 0.125 * v);
-        }
-#pragma unroll
-        for (int cc = 0; cc < NC; ++cc) {
-          double v = 0.0;
-#pragma unroll
-          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
-#pragma unroll
-            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, ta[a], td[d]), XV(a, b, cc, d), v);
-          add_target(ql.kt, nt, tb[b], tc[cc], 0.125 * v);
-        }
-      }
-    }
-  }
+// Block-pair maxima of |P_T|, as the bit patterns of non-negative doubles.
+__global__ void k_block_dmax(const double* __restrict__ D, int nt, const int* __restrict__ tblk, int nblk,
+                             unsigned long long* __restrict__ bmax) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nt * nt) return;
+  const int b1 = tblk[t % nt], b2 = tblk[t / nt];
+  if (b1 < 0 || b2 < 0) return;
+  const double v = fabs(D[t]);
+  if (v > 0.0) atomicMax(bmax + (size_t)b1 * nblk + b2, (unsigned long long)__double_as_longlong(v));
 }
 
 // ------------------------------------------------------------------ interpreted classes
@@ -604,7 +395,6 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
   double* X = xg ? xg : ccd + NCD;
   const PairArrays pr = ql.pairs;
   const int nt = ql.nt;
-  const double tol = ql.inttol;
   const double* __restrict__ D = ql.dt;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const int base = LT + 2;
@@ -622,6 +412,9 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
     const int H = ql.bk_list[k];
     const int h0 = ql.gr_start[H], hn = ql.gr_n[H];
     const double hmax = ql.gr_max[H];
+    const double thr = quartet_threshold(
+        ql, ql.dtol > 0.0 ? quartet_pmax(ql, pr.si[g0], pr.sj[g0], pr.si[h0], pr.sj[h0]) : 0.0);
+    if (ql.gr_max[G] * hmax < thr) continue;   // no quartet of (G|H) passes (team-uniform)
     {
       const int K0 = pr.si[h0], L0 = pr.sj[h0];
       for (int x = tid; x < NC; x += team) prm[DG::SC + x] = ql.prim[K0 * MAXCOMP + x];
@@ -640,9 +433,11 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       for (int t = tid; t < NB * NC; t += team) P[DG::OBC + t] = dt_at(D, nt, ql.tidx[pb[t / NC]], ql.tidx[pc[t % NC]]);
       for (int t = tid; t < NB * ND; t += team) P[DG::OBD + t] = dt_at(D, nt, ql.tidx[pb[t / ND]], ql.tidx[pd[t % ND]]);
     }
+    sync();   // the blocks are read by the digestion, which may follow with no quartet in between
+    bool any = false;   // team-uniform: every loop decision below is
     for (int p = g0; p < g0 + gn; ++p) {
       const double sp = pr.schwarz[p];
-      if (sp * hmax < tol) break;
+      if (sp * hmax < thr) break;
       const int I = pr.si[p], J = pr.sj[p];
       for (int t = tid; t < NA * NB; t += team)
         cab[t] = ql.tcoef[ql.prim[I * MAXCOMP + t / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + t % NB]];
@@ -650,7 +445,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
       const int qe = (G == H) ? p + 1 : h0 + hn;
       for (int q = h0; q < qe; ++q) {
-        if (sp * pr.schwarz[q] < tol) break;   // the reference's screen (team-uniform)
+        if (sp * pr.schwarz[q] < thr) break;   // the reference's screen (thr = INTTOL; team-uniform)
         const int K = pr.si[q], L = pr.sj[q];
         const double ze = pr.zeta[q];
         const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
@@ -692,11 +487,12 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
         }
         const double w = sw[0];
         for (int i = tid; i < NI; i += team) X[i] = fma(w * cab[i / NCD] * ccd[i % NCD], v[tab.out[i]], X[i]);
+        any = true;
         sync();
       }
     }
     // digestion of the group quartet
-    for (int t = tid; t < DG::NT; t += team) {
+    for (int t = tid; any && t < DG::NT; t += team) {
       int kind, s1, s2;
       DG::slots(t, &kind, &s1, &s2);
       add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[prm[s1]], ql.tidx[prm[s2]], DG::value(t, X, P));
@@ -736,35 +532,11 @@ __global__ void __launch_bounds__(256) k_gq_block(MolLaunch ql, OpTableDev tab, 
                                   s_geo, s_prm, s_w, threadIdx.x, blockDim.x);
 }
 
-// ------------------------------------------------------------------ launch tables
+// FP64 straight-line launchers here; the mixed-precision ones in pfe_mol_mixed.cu
+LaunchFn straight_launcher_mixed(int cb, int ck);
 
-using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
-
-template <int LA, int LB, int LC, int LD, int NPASS, int PASS>
-struct Passes {
-  static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
-    k_gq<LA, LB, LC, LD, NPASS, PASS><<<grid, 128, 0, s>>>(ql);
-    if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1>::run(ql, grid, s);
-  }
-};
-
-template <int LA, int LB, int LC, int LD, int NPASS>
-static void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
-  Passes<LA, LB, LC, LD, NPASS, 0>::run(ql, grid, s);
-}
-
-// straight-line classes and their passes (X of at most 40 integrals per pass)
-static LaunchFn straight_launcher(int cb, int ck) {
-#define Q(A, B, C, D, P) &launch_q<A, B, C, D, P>
-  static const LaunchFn table[6][6] = {
-      {Q(0, 0, 0, 0, 1), nullptr, nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 0, 0, 0, 1), Q(1, 0, 1, 0, 1), nullptr, nullptr, nullptr, nullptr},
-      {Q(1, 1, 0, 0, 1), Q(1, 1, 1, 0, 2), Q(1, 1, 1, 1, 8), nullptr, nullptr, nullptr},
-      {Q(2, 0, 0, 0, 1), Q(2, 0, 1, 0, 1), Q(2, 0, 1, 1, 5), Q(2, 0, 2, 0, 3), nullptr, nullptr},
-      {Q(2, 1, 0, 0, 1), Q(2, 1, 1, 0, 4), nullptr, nullptr, nullptr, nullptr},
-      {Q(2, 2, 0, 0, 3), nullptr, nullptr, nullptr, nullptr, nullptr}};
-#undef Q
-  return table[cb][ck];
+static LaunchFn straight_launcher(int cb, int ck, bool mixed = false) {
+  return mixed ? straight_launcher_mixed(cb, ck) : straight_launcher_t<false>(cb, ck);
 }
 
 using BigFn = void (*)(const MolLaunch&, const OpTableDev&, double* xg, int grid, size_t smem, cudaStream_t);
@@ -1025,6 +797,7 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
       PFE_CUDA(cudaStreamSynchronize(s));
       cl.quartets = (double)nq;
       cl.has_straight = straight_launcher(cb, ck) != nullptr;
+      cl.npass = cl.has_straight ? straight_npass(cb, ck) : 0;
       cl.has_table = false;
       cl.variant = 0;
       cl.xg = nullptr;
@@ -1094,6 +867,12 @@ static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   ql.gr_n = ctx->d_gr_n;
   ql.gr_max = ctx->d_gr_max;
   ql.bk_list = ctx->d_bk_list;
+  ql.blk = ctx->d_blk;
+  ql.bmax = ctx->d_bmax;
+  ql.nblk = ctx->nblk;
+  ql.dtol = ctx->dtol;
+  ql.mcut = ctx->mcut;
+  ql.n32 = ctx->d_n32;
   ql.inttol = ctx->inttol;
   ql.nt = ctx->nt;
   ql.myid = ctx->myid;
@@ -1107,7 +886,7 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
   if ((variant == 0 && cl.has_straight) || !cl.has_table) {
     const int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
-    straight_launcher(cl.cb, cl.ck)(ql, std::max(grid, 1), s);
+    straight_launcher(cl.cb, cl.ck, ctx->mcut > 0.0)(ql, std::max(grid, 1), s);
     return;
   }
   OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
@@ -1182,6 +961,14 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
 static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double* d_xc, cudaStream_t s) {
   PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, target_bytes(ctx), s));
+  PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
+  if (ctx->dtol > 0.0 || ctx->mcut > 0.0) {
+    const long long nt2 = (long long)ctx->nt * ctx->nt;
+    PFE_CUDA(cudaMemsetAsync(ctx->d_bmax, 0, sizeof(double) * (size_t)ctx->nblk * ctx->nblk, s));
+    k_block_dmax<<<(unsigned)((nt2 + 255) / 256), 256, 0, s>>>(d_dt, ctx->nt, ctx->d_tblk, ctx->nblk,
+                                                               (unsigned long long*)ctx->d_bmax);
+    PFE_CUDA(cudaGetLastError());
+  }
   const MolLaunch ql = make_launch(ctx, d_dt);
   if (ctx->profile) {
     for (int i = 0; i <= ctx->nlaunch && i < 64; ++i)

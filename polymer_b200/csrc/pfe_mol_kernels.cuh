@@ -1,0 +1,340 @@
+// Molecular quartet kernels shared by the FP64 and mixed-precision
+// instantiations (pfe_mol.cu, pfe_mol_mixed.cu): the launch block, density
+// bounds, the precision switch of the recursion, the digestion helpers and the
+// straight-line group-quartet kernel with its pass launchers.
+#pragma once
+
+#include "pfe_common.cuh"
+#include "pfe_context.cuh"
+#include "generated/eri_classes.cuh"
+
+namespace pfe {
+
+struct MolLaunch {
+  PairArrays pairs;
+  const int* prim;        // shell components -> primitive
+  const int* tidx;        // primitive -> target row (-1: none)
+  const double* tcoef;    // primitive -> coefficient
+  const double* boys;
+  const double* dt;       // density in target space (nt x nt, column-major)
+  double* jt;             // J' targets (nt x nt)
+  double* kt;             // K' targets
+  const int* gr_start;    // group -> first pair
+  const int* gr_n;        // group -> number of pairs
+  const double* gr_max;   // group -> largest bound
+  const int* bk_list;     // ket groups by (class, bucket, group)
+  const int* blk;         // shell -> contracted block
+  const double* bmax;     // block-pair maxima of |P_T| (density screening / mixed precision)
+  int nblk;
+  double dtol;            // skip quartets with bound * max|P| < dtol (0: the reference's screen only)
+  double mcut;            // FP32 recursion where bound * max|P| < mcut (0: FP64 only)
+  unsigned long long* n32;  // quartets run in FP32
+  const int4* chunks;     // (bra group, first list entry, end list entry, 0)
+  const int* nchunks;
+  double inttol;
+  int nt;
+  int myid, numprocs;
+};
+
+// max|P_T| over the six density blocks a group quartet's digestion reads
+__device__ __forceinline__ double quartet_pmax(const MolLaunch& ql, int I, int J, int K, int L) {
+  const int bI = ql.blk[I], bJ = ql.blk[J], bK = ql.blk[K], bL = ql.blk[L], nb = ql.nblk;
+  const double* bm = ql.bmax;
+  return fmax(fmax(fmax(bm[bI * nb + bJ], bm[bK * nb + bL]), fmax(bm[bI * nb + bK], bm[bI * nb + bL])),
+              fmax(bm[bJ * nb + bK], bm[bJ * nb + bL]));
+}
+
+// Screening threshold on Schwarz(ij)*Schwarz(kl) of a group quartet: the
+// reference's INTTOL, raised to dtol/max|P| under density screening.
+__device__ __forceinline__ double quartet_threshold(const MolLaunch& ql, double pmax) {
+  if (ql.dtol <= 0.0) return ql.inttol;
+  return pmax > 0.0 ? fmax(ql.inttol, ql.dtol / pmax) : INFINITY;
+}
+
+// Primitive-quartet integrals in FP64, or in FP32 from Boys values and geometry
+// computed in FP64 (the recursion is linear in F: it runs on F/pref, and the
+// outputs are scaled by pref in FP64, so FP32 sees values of order one).
+template <typename R, int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void eri_prec(const double* F, double pref, const EriGeom<double>& g, double* out) {
+  constexpr int NI = ncum(LA) * ncum(LB) * ncum(LC) * ncum(LD);
+  constexpr int LT = LA + LB + LC + LD;
+  if constexpr (sizeof(R) == sizeof(double)) {
+    eri_dispatch<LA, LB, LC, LD>(F, g, out);
+  } else {
+    float Ff[LT + 1];
+#pragma unroll
+    for (int m = 0; m <= LT; ++m) Ff[m] = (float)F[m];
+    EriGeom<float> gf;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      gf.PA[k] = (float)g.PA[k]; gf.WP[k] = (float)g.WP[k]; gf.QC[k] = (float)g.QC[k];
+      gf.WQ[k] = (float)g.WQ[k]; gf.AB[k] = (float)g.AB[k]; gf.CD[k] = (float)g.CD[k];
+    }
+    gf.oz = (float)g.oz; gf.oe = (float)g.oe; gf.oze = (float)g.oze; gf.roz = (float)g.roz; gf.roe = (float)g.roe;
+    float of[NI];
+    eri_dispatch<LA, LB, LC, LD>(Ff, gf, of);
+#pragma unroll
+    for (int i = 0; i < NI; ++i) out[i] = pref * (double)of[i];
+  }
+}
+
+// ------------------------------------------------------------------ digestion helpers
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void add_target(double* __restrict__ M, int nt, int r, int c, double v) {
+  if (r >= 0 && c >= 0 && v != 0.0) atomicAdd(M + r + (size_t)nt * c, v);
+}
+
+__device__ __forceinline__ double dt_at(const double* __restrict__ D, int nt, int i, int j) {
+  return (i >= 0 && j >= 0) ? __ldg(D + i + (size_t)nt * j) : 0.0;
+}
+
+// ------------------------------------------------------------------ straight-line classes
+
+// One group quartet per lane: the warp shares the bra group, each lane owns one
+// ket group of the chunk.  X(abcd) of the lane's group quartet stays in
+// registers; the bra's primitive pairs are walked in step by the whole warp.
+// Classes with more integrals than registers hold X in NPASS launches, pass
+// PASS keeping the bra components ab in [AB0, AB1) (the recursion is repeated
+// per pass; the outputs a pass does not keep are dead code in it).
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
+__global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
+  constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
+  constexpr int NI = NA * NB * NC * ND;
+  constexpr int NAB = NA * NB;
+  constexpr int NCD = NC * ND;
+  constexpr int LT = LA + LB + LC + LD;
+  constexpr int ABP = (NAB + NPASS - 1) / NPASS;
+  constexpr int AB0 = PASS * ABP;
+  constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
+  constexpr int XN = (AB1 - AB0) * NCD;
+  const int lane = threadIdx.x & 31;
+  const int wpb = blockDim.x >> 5;
+  const int nchunks = *ql.nchunks;
+  const int stride = gridDim.x * wpb * ql.numprocs;
+  const double c2pi = 2.0 / sqrt(REF_PI);
+  const PairArrays pr = ql.pairs;
+  const int nt = ql.nt;
+  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
+    const int4 ch = ql.chunks[c];
+    const int G = ch.x;
+    const int li = ch.y + lane;
+    const bool act = li < ch.z;
+    const int H = ql.bk_list[act ? li : ch.y];
+    const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
+    const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
+    const double hmax = act ? ql.gr_max[H] : 0.0;
+    const bool dens = ql.dtol > 0.0 || ql.mcut > 0.0;
+    const double pmax = dens ? quartet_pmax(ql, pr.si[g0], pr.sj[g0], pr.si[h0], pr.sj[h0]) : 0.0;
+    const double thr = quartet_threshold(ql, pmax);
+    unsigned n32 = 0;
+    bool any = false;   // this lane evaluated a quartet
+    double X[XN];
+#pragma unroll
+    for (int i = 0; i < XN; ++i) X[i] = 0.0;
+    for (int p = g0; p < g0 + gn; ++p) {
+      const double sp = pr.schwarz[p];
+      if (!__any_sync(0xffffffffu, act && sp * hmax >= thr)) break;   // later bra pairs fail for every lane
+      const int I = pr.si[p], J = pr.sj[p];
+      double cab[NAB];
+#pragma unroll
+      for (int ab = AB0; ab < AB1; ++ab)
+        cab[ab] = ql.tcoef[ql.prim[I * MAXCOMP + ab / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + ab % NB]];
+      const double zb = pr.zeta[p];
+      const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
+      const double Sp = pr.S[p];
+      const double wIJ = (I != J) ? 2.0 : 1.0;
+      const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
+      for (int q = h0; q < qe; ++q) {
+        const double sq = pr.schwarz[q];
+        if (sp * sq < thr) break;   // the reference's screen (thr = INTTOL); pairs sorted by bound
+        const double ze = pr.zeta[q];
+        const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
+        const double zz = zb + ze;
+        const double rho = zb * ze / zz;
+        const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
+        const double T = rho * (dx * dx + dy * dy + dz * dz);
+        const double pref = c2pi * Sp * pr.S[q] * sqrt(rho);
+        // FP32 only when every lane running this step qualifies
+        bool f32 = false;
+        if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < ql.mcut);
+        n32 += f32 ? 1u : 0u;
+        double F[LT + 1];
+        boys_tab<LT>(T, f32 ? 1.0 : pref, ql.boys, F);
+        double out[NI];
+        if constexpr (LT == 0) {
+          out[0] = F[0];
+        } else {
+          EriGeom<double> g;
+          const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
+          g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
+          g.QC[0] = pr.PA[0][q]; g.QC[1] = pr.PA[1][q]; g.QC[2] = pr.PA[2][q];
+          g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
+          g.CD[0] = pr.AB[0][q]; g.CD[1] = pr.AB[1][q]; g.CD[2] = pr.AB[2][q];
+          g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
+          g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
+          g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
+          if constexpr (MIXED) {
+            if (f32) eri_prec<float, LA, LB, LC, LD>(F, pref, g, out);
+            else eri_prec<double, LA, LB, LC, LD>(F, pref, g, out);
+          } else {
+            eri_prec<double, LA, LB, LC, LD>(F, pref, g, out);
+          }
+        }
+        any = true;
+        const int K = pr.si[q], L = pr.sj[q];
+        const double w = wIJ * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
+        double ccd[NCD];
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          const double c1 = w * ql.tcoef[ql.prim[K * MAXCOMP + cc]];
+#pragma unroll
+          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.tcoef[ql.prim[L * MAXCOMP + d]];
+        }
+#pragma unroll
+        for (int ab = AB0; ab < AB1; ++ab)
+#pragma unroll
+          for (int cd = 0; cd < NCD; ++cd)
+            X[(ab - AB0) * NCD + cd] = fma(cab[ab] * ccd[cd], out[ab * NCD + cd], X[(ab - AB0) * NCD + cd]);
+      }
+    }
+    if (MIXED && PASS == 0) {
+      unsigned long long n = n32;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+      if (lane == 0 && n) atomicAdd(ql.n32, n);
+    }
+    // digestion of this pass's part of X against the target-space density
+    if (!__any_sync(0xffffffffu, any)) continue;   // nothing passed the screens in this chunk
+    const double* __restrict__ D = ql.dt;
+    const int I0 = pr.si[g0], J0 = pr.sj[g0], K0 = pr.si[h0], L0 = pr.sj[h0];
+    int ta[NA], tb[NB], tc[NC], td[ND];
+#pragma unroll
+    for (int x = 0; x < NA; ++x) ta[x] = ql.tidx[ql.prim[I0 * MAXCOMP + x]];
+#pragma unroll
+    for (int x = 0; x < NB; ++x) tb[x] = ql.tidx[ql.prim[J0 * MAXCOMP + x]];
+#pragma unroll
+    for (int x = 0; x < NC; ++x) tc[x] = ql.tidx[ql.prim[K0 * MAXCOMP + x]];
+#pragma unroll
+    for (int x = 0; x < ND; ++x) td[x] = ql.tidx[ql.prim[L0 * MAXCOMP + x]];
+    // X(abcd) of this pass (zero outside it: constant-folded in the unrolled loops)
+    auto XV = [&](int a, int b, int cc, int d) -> double {
+      const int ab = a * NB + b;
+      return (ab >= AB0 && ab < AB1) ? X[(ab - AB0) * NCD + cc * ND + d] : 0.0;
+    };
+    // J'(ab) += 1/4 sum_cd P(cd) X: the bra is the warp's, reduce over lanes first
+#pragma unroll
+    for (int ab = AB0; ab < AB1; ++ab) {
+      double v = 0.0;
+#pragma unroll
+      for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tc[cc], td[d]), X[(ab - AB0) * NCD + cc * ND + d], v);
+      v = warp_sum(v);
+      if (lane == 0) add_target(ql.jt, nt, ta[ab / NB], tb[ab % NB], 0.25 * v);
+    }
+    if (act && any) {
+      // J'(cd) += 1/4 sum_ab P(ab) X
+      double Pab[NAB];
+#pragma unroll
+      for (int ab = AB0; ab < AB1; ++ab) Pab[ab] = dt_at(D, nt, ta[ab / NB], tb[ab % NB]);
+#pragma unroll
+      for (int cd = 0; cd < NCD; ++cd) {
+        double v = 0.0;
+#pragma unroll
+        for (int ab = AB0; ab < AB1; ++ab) v = fma(Pab[ab], X[(ab - AB0) * NCD + cd], v);
+        add_target(ql.jt, nt, tc[cd / ND], td[cd % ND], 0.25 * v);
+      }
+      // K'(ad) += 1/8 P(bc) X ; K'(ac) += 1/8 P(bd) X
+#pragma unroll
+      for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, tb[b], tc[cc]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, ta[a], td[d], 0.125 * v);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          double v = 0.0;
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tb[b], td[d]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, ta[a], tc[cc], 0.125 * v);
+        }
+      }
+      // K'(bd) += 1/8 P(ac) X ; K'(bc) += 1/8 P(ad) X
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          double v = 0.0;
+#pragma unroll
+          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
+#pragma unroll
+            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, ta[a], tc[cc]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, tb[b], td[d], 0.125 * v);
+        }
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc) {
+          double v = 0.0;
+#pragma unroll
+          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, ta[a], td[d]), XV(a, b, cc, d), v);
+          add_target(ql.kt, nt, tb[b], tc[cc], 0.125 * v);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ launch tables
+
+using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
+
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
+struct Passes {
+  static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
+    k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED><<<grid, 128, 0, s>>>(ql);
+    if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1, MIXED>::run(ql, grid, s);
+  }
+};
+
+template <int LA, int LB, int LC, int LD, int NPASS, bool MIXED>
+static void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
+  Passes<LA, LB, LC, LD, NPASS, 0, MIXED>::run(ql, grid, s);
+}
+
+// Launches per straight-line class (its passes); must match the table below.
+static inline int straight_npass(int cb, int ck) {
+  static const int np[6][6] = {{1, 0, 0, 0, 0, 0}, {1, 1, 0, 0, 0, 0}, {1, 2, 8, 0, 0, 0},
+                               {1, 1, 5, 3, 0, 0}, {1, 4, 0, 0, 0, 0}, {3, 0, 0, 0, 0, 0}};
+  return np[cb][ck];
+}
+
+// straight-line classes and their passes (X of at most 40 integrals per pass)
+template <bool MIXED>
+static LaunchFn straight_launcher_t(int cb, int ck) {
+#define Q(A, B, C, D, P) &launch_q<A, B, C, D, P, MIXED>
+  static const LaunchFn table[6][6] = {
+      {Q(0, 0, 0, 0, 1), nullptr, nullptr, nullptr, nullptr, nullptr},
+      {Q(1, 0, 0, 0, 1), Q(1, 0, 1, 0, 1), nullptr, nullptr, nullptr, nullptr},
+      {Q(1, 1, 0, 0, 1), Q(1, 1, 1, 0, 2), Q(1, 1, 1, 1, 8), nullptr, nullptr, nullptr},
+      {Q(2, 0, 0, 0, 1), Q(2, 0, 1, 0, 1), Q(2, 0, 1, 1, 5), Q(2, 0, 2, 0, 3), nullptr, nullptr},
+      {Q(2, 1, 0, 0, 1), Q(2, 1, 1, 0, 4), nullptr, nullptr, nullptr, nullptr},
+      {Q(2, 2, 0, 0, 3), nullptr, nullptr, nullptr, nullptr, nullptr}};
+#undef Q
+  return table[cb][ck];
+}
+
+}  // namespace pfe

@@ -73,13 +73,15 @@ def fourindex_eri(sysm: System, p_p: np.ndarray, p_p_helix: Optional[np.ndarray]
 class DeviceFock:
     """A pfe_context bound to one System; callable as the SCF's FockBuilder."""
 
-    def __init__(self, sysm: System, device: int = 0, **kw):
+    def __init__(self, sysm: System, device: int = 0, primitive_targets: bool = False, **kw):
         self.L = lib()
         self.sys = sysm
         self.device = device
         h = ctypes.c_void_p()
         check(self.L, self.L.pfe_context_create(device, ctypes.byref(h)))
         self.ctx = h
+        if primitive_targets:
+            check(self.L, self.L.pfe_context_primitive_targets(self.ctx, 1))
         a, keep = sysm.pfe_args(None, None, **kw)
         check(self.L, self.L.pfe_context_setup(self.ctx, ctypes.byref(a)))
         nc, n = sysm.ncell1, sysm.basis.ncgs
@@ -101,6 +103,20 @@ class DeviceFock:
 
     def force_variant(self, v: int) -> None:
         check(self.L, self.L.pfe_context_force_variant(self.ctx, v))
+
+    def set_screening(self, mixed_cutoff: float = 0.0, density_tol: float = 0.0) -> None:
+        """FP32 recursion below mixed_cutoff and density screening below density_tol (0: off)."""
+        mode = capi.PFE_PREC_MIXED if mixed_cutoff > 0.0 else capi.PFE_PREC_FP64
+        check(self.L, self.L.pfe_context_set_screening(self.ctx, mode, float(mixed_cutoff), float(density_tol)))
+
+    def from_pc(self, p_c: torch.Tensor):
+        """Molecules: contracted device P_C (ncgs x ncgs) -> (C_C, X_C), fully asynchronous."""
+        pc = p_c.reshape(p_c.shape[-2:]).transpose(-1, -2).contiguous()
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(self.L, self.L.pfe_context_fock_pc(self.ctx, ctypes.c_void_p(pc.data_ptr()),
+                                                 ctypes.c_void_p(self.out_c.data_ptr()),
+                                                 ctypes.c_void_p(self.out_x.data_ptr()), ctypes.c_void_p(s)))
+        return self.out_c.transpose(-1, -2).clone(), self.out_x.transpose(-1, -2).clone()
 
     def run_fortran(self, d_pp: torch.Tensor, d_pph: Optional[torch.Tensor], out_c: torch.Tensor,
                     out_x: torch.Tensor, stream=None) -> None:

@@ -55,6 +55,7 @@ class SCFResult:
     fermi: float
     fock_seconds: float = 0.0
     wall_seconds: float = 0.0
+    energy_variational: Optional[float] = None   # E[P] with J/K built from the final P itself
 
 
 class SCFError(RuntimeError):
@@ -89,6 +90,18 @@ class HostState:
                     ph[n] += PI * ii / kk * q[:, ax]
         self.phase = torch.polar(torch.ones_like(ph), ph)  # exp(i*phase), (nk, ncell)
         self.nk_weight = 1.0 / (max(1, 2 * kv[0]) * max(1, 2 * kv[1]) * max(1, 2 * kv[2]))
+        # a molecule (one cell, the Gamma point only) runs FOCK_BUILD in real arithmetic
+        self.gamma_only = len(ks) == 1 and len(self.cells) == 1
+        self._xorth = None   # canonical orthogonaliser of the overlap, fixed for the geometry
+
+
+def _eigh(a: torch.Tensor):
+    """torch.linalg.eigh, retried on the CPU if the device solver reports a failure."""
+    try:
+        return torch.linalg.eigh(a)
+    except RuntimeError:
+        e, v = torch.linalg.eigh(a.cpu())
+        return e.to(a.device), v.to(a.device)
 
 
 def guess_density(sysm: System) -> np.ndarray:
@@ -106,6 +119,36 @@ def guess_density(sysm: System) -> np.ndarray:
         for k in on:
             p[c0, k, k] = float(z) / len(on)
     return p
+
+
+def core_guess(st: HostState) -> torch.Tensor:
+    """Density of the core Hamiltonian T + V (no counterpart in the reference, whose
+    guess is the nuclear-charge diagonal): FOCK_BUILD applied to F = T + V."""
+    p_out, _, _, _ = fock_build(st, st.t_c + st.n_c)
+    return p_out
+
+
+@dataclasses.dataclass
+class FastOptions:
+    """Time-to-solution options of run_scf (no counterpart in the reference).
+
+    incremental: build J/K from the change of the density since the last build
+      (J(P) = J(P_ref) + J(P - P_ref); the build is linear in P), with a full
+      rebuild every ``reset_every`` builds;
+    density_tol: skip quartets with Schwarz*Schwarz*max|dP| below it in the
+      incremental builds;
+    mixed_cutoff: FP32 recursion where Schwarz*Schwarz*max|P| is below it;
+    guess: 'nuclear' (the reference's), 'core', or a callable(System, HostState)
+      returning a cell-major P_C tensor;
+    final_full: once converged, one more iteration with a full FP64 build, whose
+      energy is reported (the fast path is judged by the plain method).
+    """
+    incremental: bool = True
+    density_tol: float = 1e-11
+    mixed_cutoff: float = 0.0
+    reset_every: int = 8
+    guess: object = 'nuclear'
+    final_full: bool = True
 
 
 def decontract(st: HostState, p_c: torch.Tensor) -> torch.Tensor:
@@ -168,8 +211,35 @@ def fermi_occupations(eps: np.ndarray, nelec: int, temphf: float, nk_weight: flo
     return mu, occ
 
 
+def _fock_build_gamma(st: HostState, f_c: torch.Tensor):
+    """FOCK_BUILD of a molecule: the k-sum is the identity, so the Hermitian
+    problem is real symmetric; the canonical orthogonaliser of the overlap (a
+    property of the geometry) is computed once and kept."""
+    sysm, d = st.sys, st.sys.deck
+    ncgs = sysm.basis.ncgs
+    f = f_c[0]
+    asym = float((f - f.T).abs().max())
+    c2s = st.c2s
+    if st._xorth is None:
+        e_s, v_s = _eigh(c2s @ st.s_c[0] @ c2s.T)
+        keep = e_s > d.lindep
+        st._xorth = v_s[:, keep] / torch.sqrt(e_s[keep])
+    x = st._xorth
+    wf = c2s @ (0.5 * (f + f.T)) @ c2s.T
+    e_f, c_f = _eigh(x.T @ wf @ x)
+    eps = torch.full((1, ncgs), 1.0e99, dtype=torch.float64, device=st.device)
+    eps[0, :e_f.shape[0]] = e_f
+    co = c2s.T @ (x @ c_f)
+    mu, occ = fermi_occupations(eps.cpu().numpy(), sysm.deck.nelectrons, d.temphf, st.nk_weight)
+    occ_t = torch.tensor(occ[0, :co.shape[1]], dtype=torch.float64, device=st.device)
+    p_out = ((co * occ_t) @ co.T * st.nk_weight).unsqueeze(0)
+    return p_out, eps, mu, asym
+
+
 def fock_build(st: HostState, f_c: torch.Tensor):
     """New density from the real-space Fock matrices (FOCK_BUILD)."""
+    if st.gamma_only:
+        return _fock_build_gamma(st, f_c)
     sysm, d = st.sys, st.sys.deck
     ncgs = sysm.basis.ncgs
     cplx = torch.complex128
@@ -180,7 +250,7 @@ def fock_build(st: HostState, f_c: torch.Tensor):
     c2s = st.c2s.to(cplx)
     ws_all = c2s @ ws_all @ c2s.T
     wf_all = c2s @ wf_all @ c2s.T
-    e_s, v_s = torch.linalg.eigh(ws_all)
+    e_s, v_s = _eigh(ws_all)
     nk = len(st.kpts)
     eps = torch.full((nk, ncgs), 1.0e99, dtype=torch.float64, device=st.device)
     cos = []
@@ -188,7 +258,7 @@ def fock_build(st: HostState, f_c: torch.Tensor):
         keep = e_s[k] > d.lindep
         x = v_s[k][:, keep] / torch.sqrt(e_s[k][keep]).to(cplx)
         fp = x.conj().T @ wf_all[k] @ x
-        e_f, c_f = torch.linalg.eigh(fp)
+        e_f, c_f = _eigh(fp)
         eps[k, :e_f.shape[0]] = e_f
         co = c2s.T @ (x @ c_f)           # CO(K,J) = sum_L WF(L,J) C2S(L,K)
         cos.append(co)
@@ -207,11 +277,9 @@ def fock_build(st: HostState, f_c: torch.Tensor):
 
 def energy(st: HostState, p_c, c_c, x_c, hfx: float, e_nuc: float, temphf: float, eps, fermi, nelec):
     """ENERGY_CALC (src/pselfconsistentfield.f90:487-648), HF terms only."""
-    comp = {'nuclear_repulsion': e_nuc,
-            'kinetic': float((p_c * st.t_c).sum()),
-            'nuclear_attraction': float((p_c * st.n_c).sum()),
-            'coulomb': float((p_c * 0.5 * c_c).sum()),
-            'exchange': float(-(p_c * 0.25 * x_c).sum() * hfx)}
+    t, v, j, k = torch.stack([(p_c * st.t_c).sum(), (p_c * st.n_c).sum(), (p_c * 0.5 * c_c).sum(),
+                              -(p_c * 0.25 * x_c).sum() * hfx]).tolist()
+    comp = {'nuclear_repulsion': e_nuc, 'kinetic': t, 'nuclear_attraction': v, 'coulomb': j, 'exchange': k}
     e = e_nuc + comp['kinetic'] + comp['nuclear_attraction'] + comp['coulomb'] + comp['exchange']
     if temphf > 0.0:
         comp['internal'] = e
@@ -232,19 +300,52 @@ def energy(st: HostState, p_c, c_c, x_c, hfx: float, e_nuc: float, temphf: float
     return e, comp
 
 
+def variational_energy(st: HostState, fock, p_c: torch.Tensor, eps, mu) -> Tuple[float, float]:
+    """E[P] with J/K of P itself from a full FP64 build; returns (energy, build seconds)."""
+    d = st.sys.deck
+    tf = time.perf_counter()
+    if hasattr(fock, 'from_pc') and st.sys.ncell1 == 1:
+        fock.set_screening()
+        c_v, x_v = fock.from_pc(p_c)
+    else:
+        p_p = decontract(st, p_c)
+        c_v, x_v = fock(p_p, rotate(st, p_p))
+    tb = time.perf_counter() - tf
+    e, _ = energy(st, p_c, c_v, x_v, d.hfexchange, st.sys.e_nuc, d.temphf, eps, mu, d.nelectrons)
+    return e, tb
+
+
 def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.ndarray] = None,
             max_cycles: Optional[int] = None, scfconv: Optional[float] = None,
-            log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True) -> SCFResult:
+            log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True,
+            fast: Optional[FastOptions] = None, variational: bool = False) -> SCFResult:
     """SELF_CONSISTENT_FIELD with the Fock build supplied by ``fock``.
 
     ``fock(P_P, P_P_HELIX)`` maps cell-major primitive densities to cell-major
-    contracted (C_C, X_C): the FOURINDEX_ERI contract.
+    contracted (C_C, X_C): the FOURINDEX_ERI contract.  With ``fast`` (molecules,
+    a DeviceFock builder) the iterations use the options of FastOptions; without
+    it the loop is the reference's.  The reference reports E with the new density
+    and the J/K of the previous one; ``variational`` adds E[P] of the density of
+    the last diagonalisation (idempotent, so E[P] is second order in its error)
+    with its own full FP64 J/K: one more build, the energy two runs are compared by.
     """
     t0 = time.perf_counter()
     d = sysm.deck
     st = HostState(sysm, device)
-    p_c = torch.tensor(guess_density(sysm) if p_c0 is None else p_c0, dtype=torch.float64, device=st.device)
+    if fast is not None and (sysm.ncell1 != 1 or not hasattr(fock, 'from_pc')):
+        raise SCFError('the fast SCF options need a molecule and a device Fock builder')
+    if p_c0 is not None:
+        p_c = torch.tensor(p_c0, dtype=torch.float64, device=st.device)
+    elif fast is not None and fast.guess == 'core':
+        p_c = core_guess(st)
+    elif fast is not None and callable(fast.guess):
+        p_c = fast.guess(sysm, st).to(dtype=torch.float64, device=st.device)
+    else:
+        p_c = torch.tensor(guess_density(sysm), dtype=torch.float64, device=st.device)
     p_p = decontract(st, p_c)
+    ref = None          # (P_C, C_C, X_C) of the last build, for incremental builds
+    nbuild = 0
+    final_pending = False
     nelec = d.nelectrons
     if nelec % 2:
         raise SCFError('ODD NUMBER OF ELECTRONS')
@@ -263,16 +364,31 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
     mu = 0.0
     for iscf in range(1, ncycles + 1):
         ti = time.perf_counter()
-        p_ph = rotate(st, p_p)
         tf = time.perf_counter()
-        c_c, x_c = fock(p_p, p_ph)
+        if fast is None:
+            p_ph = rotate(st, p_p)
+            c_c, x_c = fock(p_p, p_ph)
+        else:
+            full = final_pending or ref is None or not fast.incremental or nbuild % max(1, fast.reset_every) == 0
+            if full:
+                fock.set_screening(mixed_cutoff=0.0 if final_pending else fast.mixed_cutoff)
+                c_c, x_c = fock.from_pc(p_c)
+            else:
+                fock.set_screening(mixed_cutoff=fast.mixed_cutoff, density_tol=fast.density_tol)
+                dc, dx = fock.from_pc(p_c - ref[0])
+                c_c, x_c = ref[1] + dc, ref[2] + dx
+            fock.set_screening()
+            ref = (p_c.clone(), c_c, x_c)
+            nbuild += 1
         fock_s += time.perf_counter() - tf
         f_c = st.t_c + st.n_c + c_c - 0.5 * x_c * d.hfexchange
         p_out, eps, mu, asym = fock_build(st, f_c)
+        p_last = p_out
         dp = p_out - p_c
-        pulay[iscf, iscf] = float((dp * dp).sum())
+        dots = torch.stack([(h * dp).sum() for h in hist_d] + [(dp * dp).sum()]).cpu().numpy()
+        pulay[iscf, iscf] = dots[-1]
         for i in range(1, iscf):
-            pulay[i, iscf] = pulay[iscf, i] = float((hist_d[i - 1] * dp).sum())
+            pulay[i, iscf] = pulay[iscf, i] = dots[i - 1]
         dchg = math.sqrt(pulay[iscf, iscf] / denom)
         hist_in.append(p_c.clone())
         hist_d.append(dp.clone())
@@ -302,10 +418,139 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
             log('%3d %3d  %9.3e %15.12f %17.10f %15.10f %10.4f' % (iscf, idiis, asym, dchg, e,
                                                                    e - e_old if iscf > 1 else 0.0, it.seconds))
         if dchg < conv:
+            if fast is not None and fast.final_full and not final_pending:
+                final_pending = True      # one more iteration on a full FP64 build judges the result
+                e_old = e
+                continue
             converged = True
             break
+        final_pending = False
         e_old = e
     if not converged and raise_on_fail:
         raise SCFError('SCF CONVERGENCE NOT MET')
     e, comp = energy(st, p_c, c_c, x_c, d.hfexchange, sysm.e_nuc, d.temphf, eps, mu, nelec)
-    return SCFResult(converged, e, comp, iters, p_c, eps, mu, fock_s, time.perf_counter() - t0)
+    e_var = None
+    if variational:
+        e_var, t_var = variational_energy(st, fock, p_last, eps, mu)
+        fock_s += t_var
+    return SCFResult(converged, e, comp, iters, p_c, eps, mu, fock_s, time.perf_counter() - t0, e_var)
+
+
+def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, device='cuda',
+                 max_cycles: Optional[int] = None, scfconv: Optional[float] = None, ndiis: int = 8,
+                 log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True) -> SCFResult:
+    """Time-to-solution RHF for molecules (no counterpart in the reference).
+
+    Same Hamiltonian, basis, orthogonalisation (LINDEP) and convergence test
+    (RMS change of P_C below SCFCONV) as SELF_CONSISTENT_FIELD, with:
+    Pulay's commutator DIIS on the Fock matrix (error FPS - SPF in the
+    orthonormal basis, last ``ndiis`` iterations) in place of the reference's
+    density extrapolation; J/K from the DeviceFock ``fock`` with the options of
+    ``opts`` (incremental density-screened builds, FP32 recursion, guess); and,
+    once converged, one more iteration on a full FP64 build whose energy
+    E[P] = tr P (H + J/2 - K/4) of the idempotent density P is reported.
+    Zero-temperature closed shells only (aufbau occupations).
+    """
+    opts = opts or FastOptions()
+    t0 = time.perf_counter()
+    d = sysm.deck
+    if sysm.ncell1 != 1 or not hasattr(fock, 'from_pc'):
+        raise SCFError('the fast SCF needs a molecule and a device Fock builder')
+    if d.temphf > 0.0 or d.nelectrons % 2:
+        raise SCFError('the fast SCF handles zero-temperature closed shells only')
+    st = HostState(sysm, device)
+    if opts.guess == 'core':
+        p_c = core_guess(st)
+    elif callable(opts.guess):
+        p_c = opts.guess(sysm, st).to(dtype=torch.float64, device=st.device)
+    else:
+        p_c = torch.tensor(guess_density(sysm), dtype=torch.float64, device=st.device)
+    nocc = d.nelectrons // 2
+    c2s, s0 = st.c2s, st.s_c[0]
+    e_s, v_s = _eigh(c2s @ s0 @ c2s.T)
+    keep = e_s > d.lindep
+    w = c2s.T @ (v_s[:, keep] / torch.sqrt(e_s[keep]))     # orthonormal -> contracted Cartesian
+    ws = w.T @ s0                                            # P_ortho = ws P ws^T
+    h = st.t_c[0] + st.n_c[0]
+    ncycles = max_cycles or d.scfcycles
+    conv = d.scfconv if scfconv is None else scfconv
+    denom = float(sysm.basis.ncgs ** 2)
+    hist_f: List[torch.Tensor] = []
+    hist_e: List[torch.Tensor] = []
+    iters: List[SCFIteration] = []
+    ref = None
+    nbuild = 0
+    final_pending = False
+    converged = False
+    fock_s = 0.0
+    e = 0.0
+    eps = None
+    for iscf in range(1, ncycles + 1):
+        ti = time.perf_counter()
+        full = final_pending or ref is None or not opts.incremental or nbuild % max(1, opts.reset_every) == 0
+        tf = time.perf_counter()
+        if full:
+            fock.set_screening(mixed_cutoff=0.0 if final_pending else opts.mixed_cutoff)
+            c_c, x_c = fock.from_pc(p_c)
+        else:
+            fock.set_screening(mixed_cutoff=opts.mixed_cutoff, density_tol=opts.density_tol)
+            dc, dx = fock.from_pc(p_c - ref[0])
+            c_c, x_c = ref[1] + dc, ref[2] + dx
+        fock.set_screening()
+        fock_s += time.perf_counter() - tf
+        ref = (p_c.clone(), c_c, x_c)
+        nbuild += 1
+        f = h + c_c[0] - 0.5 * d.hfexchange * x_c[0]
+        f = 0.5 * (f + f.T)
+        fo = w.T @ f @ w
+        po = ws @ p_c[0] @ ws.T
+        err = fo @ po - po @ fo
+        hist_f.append(fo)
+        hist_e.append(err)
+        if len(hist_f) > ndiis:
+            hist_f.pop(0)
+            hist_e.pop(0)
+        m = len(hist_f)
+        e_vals = torch.stack([(p_c[0] * (h + 0.5 * c_c[0] - 0.25 * d.hfexchange * x_c[0])).sum(),
+                              err.abs().max()] + [(hist_e[i] * hist_e[j]).sum() for i in range(m) for j in range(i, m)])
+        vals = e_vals.cpu().numpy()
+        e = float(vals[0]) + sysm.e_nuc
+        fe = float(vals[1])
+        if m >= 2:
+            bm = np.zeros((m + 1, m + 1))
+            k = 2
+            for i in range(m):
+                for j in range(i, m):
+                    bm[i, j] = bm[j, i] = vals[k]
+                    k += 1
+            bm[:m, m] = bm[m, :m] = -1.0
+            rhs = np.zeros(m + 1)
+            rhs[m] = -1.0
+            try:
+                coef = np.linalg.solve(bm, rhs)[:m]
+            except np.linalg.LinAlgError:
+                coef = np.zeros(m)
+                coef[-1] = 1.0
+            fo = sum(float(cf) * fh for cf, fh in zip(coef, hist_f))
+        eo, co = _eigh(fo)
+        cc = w @ co[:, :nocc]
+        p_new = (2.0 * cc @ cc.T).unsqueeze(0)
+        eps = torch.full((1, sysm.basis.ncgs), 1.0e99, dtype=torch.float64, device=st.device)
+        eps[0, :eo.shape[0]] = eo
+        dchg = math.sqrt(float(((p_new - p_c) ** 2).sum()) / denom)
+        it = SCFIteration(iscf, m if m >= 2 else 0, fe, dchg, e, float(eo[nocc - 1]), time.perf_counter() - ti)
+        iters.append(it)
+        if log:
+            log('%3d %3d  %9.3e %15.12f %17.10f %s %10.4f' % (iscf, it.idiis, fe, dchg, e, 'full' if full else 'incr',
+                                                                it.seconds))
+        if final_pending and dchg < conv:
+            converged = True          # e is E[P] of the idempotent p_c with its own full FP64 J/K
+            break
+        final_pending = dchg < conv
+        p_c = p_new
+    if not converged and raise_on_fail:
+        raise SCFError('SCF CONVERGENCE NOT MET')
+    comp = {'total': e}
+    res = SCFResult(converged, e, comp, iters, p_c, eps, float(iters[-1].fermi) if iters else 0.0, fock_s,
+                    time.perf_counter() - t0, e)
+    return res
