@@ -241,6 +241,9 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-scf', action='store_true', help='skip the time-to-converged SCF leg')
+    ap.add_argument('--autotune', action='store_true',
+                    help='time every kernel variant per quartet class and keep the fastest '
+                         '(default: the library\'s measured schedule table)')
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == 'reference':
@@ -272,7 +275,9 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    df.autotune(p_p)   # per-class schedule choice, part of set-up (untimed)
+    if args.autotune:
+        df.autotune(p_p)   # per-class schedule chosen by timing every variant (untimed set-up)
+    cen = df.census()
 
     def step():
         df.run_fortran(pp_f, None, out_c, out_x)
@@ -394,6 +399,7 @@ def main():
                 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
                 'config': {'workload': workload_name(), 'npgs': sysm.basis.npgs, 'ncgs': sysm.basis.ncgs,
                            'npshell': sysm.basis.npshell, 'precision': 'fp64',
+                           'schedule': 'autotuned' if args.autotune else 'default table',
                            'l2': 'flushed before every timed step (256 MiB write)',
                            'parallelism': 'quartet chunks split over %d GPU(s), NCCL all-reduce of J/K' % world
                            if world > 1 else 'single GPU'},

@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, '_build')
 LIB = os.path.join(OUT, 'libpolymer_fock.so')
-SOURCES = ['pfe_api.cu', 'pfe_eri.cu', 'pfe_mol.cu', 'pfe_mol_mixed.cu', 'pfe_lattice.cu', 'pfe_onee.cu']
+SOURCES = ['pfe_api.cu', 'pfe_eri.cu', 'pfe_mol.cu', 'pfe_mol_mixed.cu', 'pfe_mol_big1.cu', 'pfe_mol_big2.cu',
+           'pfe_mol_big3.cu', 'pfe_mol_big4.cu', 'pfe_lattice.cu', 'pfe_onee.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550']

@@ -163,7 +163,7 @@ class Gen:
         return outs
 
 
-OPS_THRESHOLD = 256   # classes with more integrals run on the op-table interpreter
+OPS_THRESHOLD = 1600  # classes with more integrals have no straight-line function (op tables only)
 
 
 def gen_optable(LA, LB, LC, LD):

@@ -192,6 +192,8 @@ static void reset_context(pfe_context* ctx) {
   ctx->d_blk = nullptr;
   ctx->d_rep = nullptr;
   ctx->d_repc = nullptr;
+  ctx->d_scoef = nullptr;
+  ctx->d_stidx = nullptr;
   ctx->d_tblk = nullptr;
   ctx->d_bmax = nullptr;
   ctx->d_n32 = nullptr;
@@ -199,6 +201,7 @@ static void reset_context(pfe_context* ctx) {
   ctx->d_flag = nullptr;
   ctx->d_gr_start = ctx->d_gr_n = ctx->d_bk_list = nullptr;
   ctx->d_gr_max = nullptr;
+  ctx->d_prec = nullptr;
   ctx->ngroups = 0;
   ctx->d_pp = ctx->d_pph = ctx->d_out_c = ctx->d_out_x = nullptr;
   ctx->pp_bytes = ctx->pph_bytes = ctx->out_bytes = 0;
@@ -332,6 +335,20 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
     if ((long long)ctx->nblk * ctx->nblk > (1LL << 30)) {
       set_error("too many shells for the block-pair index (more than 32768 distinct shells)");
       return PFE_EINVAL;
+    }
+    {
+      std::vector<double> scoef((size_t)a->npshell * MAXCOMP, 0.0);
+      std::vector<int> stidx((size_t)a->npshell * MAXCOMP, -1);
+      for (int sh = 0; sh < a->npshell; ++sh)
+        for (int c = 0; c < ncum(hs.L[sh]); ++c) {
+          const int p = hs.prim[(size_t)sh * MAXCOMP + c];
+          scoef[(size_t)sh * MAXCOMP + c] = tcoef[p];
+          stidx[(size_t)sh * MAXCOMP + c] = tidx[p];
+        }
+      PFE_CUDA(ctx->alloc((void**)&ctx->d_scoef, sizeof(double) * scoef.size()));
+      PFE_CUDA(ctx->alloc((void**)&ctx->d_stidx, sizeof(int) * stidx.size()));
+      PFE_CUDA(cudaMemcpy(ctx->d_scoef, scoef.data(), sizeof(double) * scoef.size(), cudaMemcpyHostToDevice));
+      PFE_CUDA(cudaMemcpy(ctx->d_stidx, stidx.data(), sizeof(int) * stidx.size(), cudaMemcpyHostToDevice));
     }
     PFE_CUDA(ctx->alloc((void**)&ctx->d_tidx, sizeof(int) * a->npgs));
     PFE_CUDA(ctx->alloc((void**)&ctx->d_tcoef, sizeof(double) * a->npgs));
@@ -641,9 +658,6 @@ int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
     PFE_CUDA(cudaMemcpyAsync(ctx->d_pph, a->p_p_helix, nh * sizeof(double), cudaMemcpyHostToDevice, s));
     d_pph = ctx->d_pph;
   }
-  if (ctx->molecular && !ctx->tuned) {
-    if ((rc = autotune(ctx, ctx->d_pp, s)) != PFE_OK) return rc;
-  }
   rc = ctx->molecular ? molecular_fock(ctx, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, s)
                       : lattice_fock(ctx, ctx->d_pp, d_pph, ctx->d_out_c, ctx->d_out_x, s);
   if (rc != PFE_OK) return rc;
@@ -660,7 +674,6 @@ int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
       if ((rc = setup_impl(pc, a, hs, key)) != PFE_OK) { pc->ready = false; return rc; }
     }
     PFE_CUDA(cudaStreamSynchronize(s));
-    if (!pc->tuned && (rc = autotune(pc, ctx->d_pp, pc->stream)) != PFE_OK) return rc;
     if ((rc = molecular_fock(pc, ctx->d_pp, ctx->d_out_c, ctx->d_out_x, pc->stream)) != PFE_OK) return rc;
     PFE_CUDA(cudaStreamSynchronize(pc->stream));
   }

@@ -92,6 +92,8 @@ struct pfe_context {
   int nt = 0;                // target dimension (ncgs or npgs)
   int* d_tidx = nullptr;     // primitive -> target row, -1 when it has no coefficient
   double* d_tcoef = nullptr; // primitive -> coefficient (CC entry, or 1)
+  double* d_scoef = nullptr; // shell x component -> coefficient of its primitive (tcoef)
+  int* d_stidx = nullptr;    // shell x component -> target row of its primitive (tidx)
   int* d_blk = nullptr;      // shell -> contracted block id
   int nblk = 0;
   bool force_primitive = false;  // set before set-up: primitive targets even when CC allows contracted ones
@@ -100,6 +102,7 @@ struct pfe_context {
   double* d_pt = nullptr;    // density in target space (nt x nt): P_C read off P_P, or P_P
   unsigned int* d_flag = nullptr;  // set when P_P is not the decontraction of a contracted density
   // groups: runs of pairs of one contracted block pair (molecules)
+  void* d_prec = nullptr;    // the sorted pairs as 128-byte records (PairRec)
   int ngroups = 0;
   int* d_gr_start = nullptr;
   int* d_gr_n = nullptr;

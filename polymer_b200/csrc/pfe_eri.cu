@@ -85,10 +85,15 @@ const OpTableHost* host_optable(int cb, int ck) {
 int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   unsigned short *ops = nullptr, *out = nullptr;
   int* lev = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&ops, sizeof(unsigned short) * 6 * h->nops));
+  PFE_CUDA(ctx->alloc((void**)&ops, sizeof(unsigned short) * 8 * (h->nops + 1)));
   PFE_CUDA(ctx->alloc((void**)&out, sizeof(unsigned short) * h->nout));
   PFE_CUDA(ctx->alloc((void**)&lev, sizeof(int) * (h->nlevels + 1)));
-  PFE_CUDA(cudaMemcpy(ops, h->ops, sizeof(unsigned short) * 6 * h->nops, cudaMemcpyHostToDevice));
+  {  // 16-byte records: the six generated fields and two zero pads
+    std::vector<unsigned short> rec((size_t)8 * (h->nops + 1), 0);
+    for (int o = 0; o < h->nops; ++o)
+      for (int k = 0; k < 6; ++k) rec[(size_t)8 * o + k] = h->ops[(size_t)6 * o + k];
+    PFE_CUDA(cudaMemcpy(ops, rec.data(), sizeof(unsigned short) * rec.size(), cudaMemcpyHostToDevice));
+  }
   PFE_CUDA(cudaMemcpy(out, h->out, sizeof(unsigned short) * h->nout, cudaMemcpyHostToDevice));
   PFE_CUDA(cudaMemcpy(lev, h->levels, sizeof(int) * (h->nlevels + 1), cudaMemcpyHostToDevice));
   d->ops = ops;

@@ -9,7 +9,7 @@
 namespace pfe {
 
 struct OpTableDev {
-  const unsigned short* ops;
+  const unsigned short* ops;   // 8 uint16 per op, 16-byte aligned (see eval_op)
   const int* levels;
   const unsigned short* out;
   int nlevels, nout, nslots;
@@ -21,19 +21,25 @@ struct OpGeom {
   double X[4], Y[4], Z;
 };
 
+// Value of op o of a table: each op is one 16-byte record of eight uint16,
+// (kind<<12 | axis<<10 | cA<<5 | cB, s1, s2, s3, s4, s5, 0, 0), read with one
+// vector load:  G1*v[s1] + G2*v[s2] + cA*X*(v[s3] - Y*v[s4]) + cB*Z*v[s5].
+__device__ __forceinline__ double eval_op(const unsigned short* __restrict__ ops, int o, const double* v,
+                                          const OpGeom& geo) {
+  const uint4 r = __ldg(reinterpret_cast<const uint4*>(ops) + o);
+  const int h = r.x & 0xffff;
+  const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
+  double val = geo.G1[kind][ax] * v[r.x >> 16] + geo.G2[kind][ax] * v[r.y & 0xffff];
+  if (cA) val += (double)cA * geo.X[kind] * (v[r.y >> 16] - geo.Y[kind] * v[r.z & 0xffff]);
+  if (cB) val += (double)cB * geo.Z * v[r.z >> 16];
+  return val;
+}
+
 __device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restrict__ v, const OpGeom& geo,
                                             int base) {
   for (int l = 0; l < t.nlevels; ++l) {
     const int o0 = t.levels[l], o1 = t.levels[l + 1];
-    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-      const unsigned short* op = t.ops + 6 * o;
-      const int h = op[0];
-      const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-      double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-      if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-      if (cB) val += (double)cB * geo.Z * v[op[5]];
-      v[base + o] = val;
-    }
+    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) v[base + o] = eval_op(t.ops, o, v, geo);
     __syncthreads();
   }
 }

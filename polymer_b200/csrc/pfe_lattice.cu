@@ -351,13 +351,7 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
         for (int l = 0; l < tab.nlevels; ++l) {
           const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
           for (int o = o0 + lane; o < o1; o += 32) {
-            const unsigned short* op = tab.ops + 6 * o;
-            const int h = op[0];
-            const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-            double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-            if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-            if (cB) val += (double)cB * geo.Z * v[op[5]];
-            v[base + o] = val;
+            v[base + o] = eval_op(tab.ops, o, v, geo);
           }
           __syncwarp();
         }

@@ -146,6 +146,20 @@ __global__ void k_mol_gather(PairArrays src, PairArrays dst, const int* __restri
   dst.gmax[t] = src.gmax[s];
 }
 
+__global__ void k_pack_pairs(PairArrays pr, PairRec* __restrict__ rec, long long n) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  PairRec r;
+  for (int k = 0; k < 3; ++k) { r.P[k] = pr.P[k][t]; r.PA[k] = pr.PA[k][t]; r.AB[k] = pr.AB[k][t]; }
+  r.zeta = pr.zeta[t];
+  r.S = pr.S[t];
+  r.schwarz = pr.schwarz[t];
+  r.si = pr.si[t];
+  r.sj = pr.sj[t];
+  r.pad[0] = r.pad[1] = r.pad[2] = 0.0;
+  rec[t] = r;
+}
+
 // ------------------------------------------------------------------ groups and chunks
 
 __global__ void k_group_heads(const int* __restrict__ gid, int* __restrict__ head, long long n) {
@@ -402,12 +416,12 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
   const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
   {
     const int I0 = pr.si[g0], J0 = pr.sj[g0];
-    for (int x = tid; x < NA; x += team) prm[x] = ql.prim[I0 * MAXCOMP + x];
-    for (int x = tid; x < NB; x += team) prm[DG::SB + x] = ql.prim[J0 * MAXCOMP + x];
+    for (int x = tid; x < NA; x += team) prm[x] = ql.stidx[I0 * MAXCOMP + x];
+    for (int x = tid; x < NB; x += team) prm[DG::SB + x] = ql.stidx[J0 * MAXCOMP + x];
   }
   sync();
   for (int t = tid; t < NA * NB; t += team)
-    P[DG::OAB + t] = dt_at(D, nt, ql.tidx[prm[t / NB]], ql.tidx[prm[DG::SB + t % NB]]);
+    P[DG::OAB + t] = dt_at(D, nt, prm[t / NB], prm[DG::SB + t % NB]);
   for (int k = ch.y; k < ch.z; ++k) {
     const int H = ql.bk_list[k];
     const int h0 = ql.gr_start[H], hn = ql.gr_n[H];
@@ -417,8 +431,8 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
     if (ql.gr_max[G] * hmax < thr) continue;   // no quartet of (G|H) passes (team-uniform)
     {
       const int K0 = pr.si[h0], L0 = pr.sj[h0];
-      for (int x = tid; x < NC; x += team) prm[DG::SC + x] = ql.prim[K0 * MAXCOMP + x];
-      for (int x = tid; x < ND; x += team) prm[DG::SD + x] = ql.prim[L0 * MAXCOMP + x];
+      for (int x = tid; x < NC; x += team) prm[DG::SC + x] = ql.stidx[K0 * MAXCOMP + x];
+      for (int x = tid; x < ND; x += team) prm[DG::SD + x] = ql.stidx[L0 * MAXCOMP + x];
     }
     for (int i = tid; i < NI; i += team) X[i] = 0.0;
     sync();
@@ -427,11 +441,11 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       const int* pb = prm + DG::SB;
       const int* pc = prm + DG::SC;
       const int* pd = prm + DG::SD;
-      for (int t = tid; t < NC * ND; t += team) P[DG::OCD + t] = dt_at(D, nt, ql.tidx[pc[t / ND]], ql.tidx[pd[t % ND]]);
-      for (int t = tid; t < NA * NC; t += team) P[DG::OAC + t] = dt_at(D, nt, ql.tidx[pa[t / NC]], ql.tidx[pc[t % NC]]);
-      for (int t = tid; t < NA * ND; t += team) P[DG::OAD + t] = dt_at(D, nt, ql.tidx[pa[t / ND]], ql.tidx[pd[t % ND]]);
-      for (int t = tid; t < NB * NC; t += team) P[DG::OBC + t] = dt_at(D, nt, ql.tidx[pb[t / NC]], ql.tidx[pc[t % NC]]);
-      for (int t = tid; t < NB * ND; t += team) P[DG::OBD + t] = dt_at(D, nt, ql.tidx[pb[t / ND]], ql.tidx[pd[t % ND]]);
+      for (int t = tid; t < NC * ND; t += team) P[DG::OCD + t] = dt_at(D, nt, pc[t / ND], pd[t % ND]);
+      for (int t = tid; t < NA * NC; t += team) P[DG::OAC + t] = dt_at(D, nt, pa[t / NC], pc[t % NC]);
+      for (int t = tid; t < NA * ND; t += team) P[DG::OAD + t] = dt_at(D, nt, pa[t / ND], pd[t % ND]);
+      for (int t = tid; t < NB * NC; t += team) P[DG::OBC + t] = dt_at(D, nt, pb[t / NC], pc[t % NC]);
+      for (int t = tid; t < NB * ND; t += team) P[DG::OBD + t] = dt_at(D, nt, pb[t / ND], pd[t % ND]);
     }
     sync();   // the blocks are read by the digestion, which may follow with no quartet in between
     bool any = false;   // team-uniform: every loop decision below is
@@ -440,7 +454,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       if (sp * hmax < thr) break;
       const int I = pr.si[p], J = pr.sj[p];
       for (int t = tid; t < NA * NB; t += team)
-        cab[t] = ql.tcoef[ql.prim[I * MAXCOMP + t / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + t % NB]];
+        cab[t] = ql.scoef[I * MAXCOMP + t / NB] * ql.scoef[J * MAXCOMP + t % NB];
       const double zb = pr.zeta[p];
       const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
       const int qe = (G == H) ? p + 1 : h0 + hn;
@@ -470,18 +484,12 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
           set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
         }
         for (int t = tid; t < NCD; t += team)
-          ccd[t] = ql.tcoef[ql.prim[K * MAXCOMP + t / ND]] * ql.tcoef[ql.prim[L * MAXCOMP + t % ND]];
+          ccd[t] = ql.scoef[K * MAXCOMP + t / ND] * ql.scoef[L * MAXCOMP + t % ND];
         sync();
         for (int l = 0; l < tab.nlevels; ++l) {
           const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
           for (int o = o0 + tid; o < o1; o += team) {
-            const unsigned short* op = tab.ops + 6 * o;
-            const int h = op[0];
-            const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
-            double val = geo.G1[kind][ax] * v[op[1]] + geo.G2[kind][ax] * v[op[2]];
-            if (cA) val += (double)cA * geo.X[kind] * (v[op[3]] - geo.Y[kind] * v[op[4]]);
-            if (cB) val += (double)cB * geo.Z * v[op[5]];
-            v[base + o] = val;
+            v[base + o] = eval_op(tab.ops, o, v, geo);
           }
           sync();
         }
@@ -495,7 +503,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
     for (int t = tid; any && t < DG::NT; t += team) {
       int kind, s1, s2;
       DG::slots(t, &kind, &s1, &s2);
-      add_target(kind == 0 ? ql.jt : ql.kt, nt, ql.tidx[prm[s1]], ql.tidx[prm[s2]], DG::value(t, X, P));
+      add_target(kind == 0 ? ql.jt : ql.kt, nt, prm[s1], prm[s2], DG::value(t, X, P));
     }
     sync();
   }
@@ -535,8 +543,12 @@ __global__ void __launch_bounds__(256) k_gq_block(MolLaunch ql, OpTableDev tab, 
 // FP64 straight-line launchers here; the mixed-precision ones in pfe_mol_mixed.cu
 LaunchFn straight_launcher_mixed(int cb, int ck);
 
+// (classes without a mixed instantiation run their FP64 straight-line kernels)
 static LaunchFn straight_launcher(int cb, int ck, bool mixed = false) {
-  return mixed ? straight_launcher_mixed(cb, ck) : straight_launcher_t<false>(cb, ck);
+  LaunchFn f = mixed ? straight_launcher_mixed(cb, ck) : nullptr;
+  if (!f) f = straight_launcher_t<false>(cb, ck);
+  if (!f) f = straight_launcher_big(cb, ck);
+  return f;
 }
 
 using BigFn = void (*)(const MolLaunch&, const OpTableDev&, double* xg, int grid, size_t smem, cudaStream_t);
@@ -704,6 +716,9 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
     PFE_CUDA(cudaGetLastError());
     PFE_CUDA(cudaStreamSynchronize(s));
   }
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_prec, sizeof(PairRec) * npairs));
+  k_pack_pairs<<<nb256, 256, 0, s>>>(ctx->pairs, (PairRec*)ctx->d_prec, npairs);
+  PFE_CUDA(cudaGetLastError());
   int hcount[8] = {0};
   PFE_CUDA(cudaMemcpy(hcount, d_count, sizeof(int) * 8, cudaMemcpyDeviceToHost));
   int off = 0;
@@ -830,7 +845,9 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
           PFE_CUDA(ctx->alloc((void**)&cl.xg, sizeof(double) * (size_t)h->nout * 2 * ctx->num_sms));
         }
         PFE_CUDA(vv.allow(cl.smem_big, std::min<size_t>(cl.smem_warp, 220 * 1024)));
-        cl.variant = cl.has_straight ? 0 : (cl.smem_warp <= 200 * 1024 && cl.per_warp * sizeof(double) <= 100 * 1024 ? 1 : 2);
+        // default schedule (measured on B200): straight-line code where a class has it, one
+        // primitive quartet per warp up to 640 integrals, per block beyond
+        cl.variant = cl.has_straight ? 0 : ((h->nout <= 640 && cl.smem_warp <= 200 * 1024) ? 1 : 2);
       }
       if (!cl.has_straight && !cl.has_table) {
         set_error("no kernel for a quartet class");
@@ -856,9 +873,10 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
 static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   MolLaunch ql{};
   ql.pairs = ctx->pairs;
+  ql.rec = (const PairRec*)ctx->d_prec;
   ql.prim = ctx->shells.prim;
-  ql.tidx = ctx->d_tidx;
-  ql.tcoef = ctx->d_tcoef;
+  ql.stidx = ctx->d_stidx;
+  ql.scoef = ctx->d_scoef;
   ql.boys = ctx->d_boys;
   ql.dt = d_dt;
   ql.jt = ctx->d_jp;

@@ -10,11 +10,45 @@
 
 namespace pfe {
 
+// One shell pair as the quartet kernels read it, 128 bytes (seven 16-byte
+// loads): P[3], PA[3], AB[3], zeta, S, Schwarz bound, (si, sj), padding.
+struct __align__(16) PairRec {
+  double P[3], PA[3], AB[3];
+  double zeta, S, schwarz;
+  int si, sj;
+  double pad[3];
+};
+static_assert(sizeof(PairRec) == 128, "PairRec layout");
+
+struct PairView {
+  double P[3], PA[3], AB[3], zeta, S;
+  int si, sj;
+};
+
+// the record of pair t after its bound (already loaded) passed the screen
+__device__ __forceinline__ PairView load_pair(const PairRec* __restrict__ rec, int t) {
+  const double2* r = reinterpret_cast<const double2*>(rec + t);
+  const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3), e = __ldg(r + 4),
+                f = __ldg(r + 5), g = __ldg(r + 6);
+  PairView v;
+  v.P[0] = a.x; v.P[1] = a.y; v.P[2] = b.x;
+  v.PA[0] = b.y; v.PA[1] = c.x; v.PA[2] = c.y;
+  v.AB[0] = d.x; v.AB[1] = d.y; v.AB[2] = e.x;
+  v.zeta = e.y; v.S = f.x;
+  v.si = __double2loint(g.x); v.sj = __double2hiint(g.x);
+  return v;
+}
+
+__device__ __forceinline__ double pair_bound(const PairRec* __restrict__ rec, int t) {
+  return __ldg(&rec[t].schwarz);
+}
+
 struct MolLaunch {
   PairArrays pairs;
+  const PairRec* rec;     // the sorted pairs as records
   const int* prim;        // shell components -> primitive
-  const int* tidx;        // primitive -> target row (-1: none)
-  const double* tcoef;    // primitive -> coefficient
+  const int* stidx;       // shell x component -> target row (-1: none)
+  const double* scoef;    // shell x component -> coefficient
   const double* boys;
   const double* dt;       // density in target space (nt x nt, column-major)
   double* jt;             // J' targets (nt x nt)
@@ -102,8 +136,16 @@ __device__ __forceinline__ double dt_at(const double* __restrict__ D, int nt, in
 // Classes with more integrals than registers hold X in NPASS launches, pass
 // PASS keeping the bra components ab in [AB0, AB1) (the recursion is repeated
 // per pass; the outputs a pass does not keep are dead code in it).
+// resident blocks of 128 threads the register allocation aims at: 4 (at most
+// 128 registers) for the classes whose working set fits, else the compiler's choice
+template <int LA, int LB, int LC, int LD>
+struct GqOccupancy {
+  static constexpr int NI = ncum(LA) * ncum(LB) * ncum(LC) * ncum(LD);
+  static constexpr int blocks = (NI <= 16 && LA + LB + LC + LD <= 2) ? 4 : 1;
+};
+
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
-__global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
+__global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch ql) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
   constexpr int NI = NA * NB * NC * ND;
   constexpr int NAB = NA * NB;
@@ -113,24 +155,35 @@ __global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
   constexpr int AB0 = PASS * ABP;
   constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
   constexpr int XN = (AB1 - AB0) * NCD;
+  static_assert(AB0 < NAB, "every pass keeps at least one bra component pair");
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const int nchunks = *ql.nchunks;
   const int stride = gridDim.x * wpb * ql.numprocs;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  const PairArrays pr = ql.pairs;
   const int nt = ql.nt;
   for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
     const int4 ch = ql.chunks[c];
     const int G = ch.x;
+    const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
+    const int2 ijg = __ldg(reinterpret_cast<const int2*>(&ql.rec[g0].si));
+    if constexpr (NPASS > 1) {
+      // a pass whose bra components all lack a coefficient (the lower components of a
+      // pure d or p shell) contributes nothing: skip the chunk (warp-uniform)
+      bool live = false;
+#pragma unroll
+      for (int ab = AB0; ab < AB1; ++ab)
+        live = live || (ql.stidx[ijg.x * MAXCOMP + ab / NB] >= 0 && ql.stidx[ijg.y * MAXCOMP + ab % NB] >= 0);
+      if (!live) continue;
+    }
     const int li = ch.y + lane;
     const bool act = li < ch.z;
     const int H = ql.bk_list[act ? li : ch.y];
-    const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
     const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
     const double hmax = act ? ql.gr_max[H] : 0.0;
     const bool dens = ql.dtol > 0.0 || ql.mcut > 0.0;
-    const double pmax = dens ? quartet_pmax(ql, pr.si[g0], pr.sj[g0], pr.si[h0], pr.sj[h0]) : 0.0;
+    const int2 klh = __ldg(reinterpret_cast<const int2*>(&ql.rec[h0].si));
+    const double pmax = dens ? quartet_pmax(ql, ijg.x, ijg.y, klh.x, klh.y) : 0.0;
     const double thr = quartet_threshold(ql, pmax);
     unsigned n32 = 0;
     bool any = false;   // this lane evaluated a quartet
@@ -138,28 +191,30 @@ __global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
 #pragma unroll
     for (int i = 0; i < XN; ++i) X[i] = 0.0;
     for (int p = g0; p < g0 + gn; ++p) {
-      const double sp = pr.schwarz[p];
+      const double sp = pair_bound(ql.rec, p);
       if (!__any_sync(0xffffffffu, act && sp * hmax >= thr)) break;   // later bra pairs fail for every lane
-      const int I = pr.si[p], J = pr.sj[p];
+      const PairView bp = load_pair(ql.rec, p);
+      const int I = bp.si, J = bp.sj;
       double cab[NAB];
 #pragma unroll
       for (int ab = AB0; ab < AB1; ++ab)
-        cab[ab] = ql.tcoef[ql.prim[I * MAXCOMP + ab / NB]] * ql.tcoef[ql.prim[J * MAXCOMP + ab % NB]];
-      const double zb = pr.zeta[p];
-      const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
-      const double Sp = pr.S[p];
+        cab[ab] = ql.scoef[I * MAXCOMP + ab / NB] * ql.scoef[J * MAXCOMP + ab % NB];
+      const double zb = bp.zeta;
+      const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
+      const double Sp = bp.S;
       const double wIJ = (I != J) ? 2.0 : 1.0;
       const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
       for (int q = h0; q < qe; ++q) {
-        const double sq = pr.schwarz[q];
+        const double sq = pair_bound(ql.rec, q);
         if (sp * sq < thr) break;   // the reference's screen (thr = INTTOL); pairs sorted by bound
-        const double ze = pr.zeta[q];
-        const double Qx = pr.P[0][q], Qy = pr.P[1][q], Qz = pr.P[2][q];
+        const PairView kq = load_pair(ql.rec, q);
+        const double ze = kq.zeta;
+        const double Qx = kq.P[0], Qy = kq.P[1], Qz = kq.P[2];
         const double zz = zb + ze;
         const double rho = zb * ze / zz;
         const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
         const double T = rho * (dx * dx + dy * dy + dz * dz);
-        const double pref = c2pi * Sp * pr.S[q] * sqrt(rho);
+        const double pref = c2pi * Sp * kq.S * sqrt(rho);
         // FP32 only when every lane running this step qualifies
         bool f32 = false;
         if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < ql.mcut);
@@ -172,10 +227,10 @@ __global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
         } else {
           EriGeom<double> g;
           const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
-          g.PA[0] = pr.PA[0][p]; g.PA[1] = pr.PA[1][p]; g.PA[2] = pr.PA[2][p];
-          g.QC[0] = pr.PA[0][q]; g.QC[1] = pr.PA[1][q]; g.QC[2] = pr.PA[2][q];
-          g.AB[0] = pr.AB[0][p]; g.AB[1] = pr.AB[1][p]; g.AB[2] = pr.AB[2][p];
-          g.CD[0] = pr.AB[0][q]; g.CD[1] = pr.AB[1][q]; g.CD[2] = pr.AB[2][q];
+          g.PA[0] = bp.PA[0]; g.PA[1] = bp.PA[1]; g.PA[2] = bp.PA[2];
+          g.QC[0] = kq.PA[0]; g.QC[1] = kq.PA[1]; g.QC[2] = kq.PA[2];
+          g.AB[0] = bp.AB[0]; g.AB[1] = bp.AB[1]; g.AB[2] = bp.AB[2];
+          g.CD[0] = kq.AB[0]; g.CD[1] = kq.AB[1]; g.CD[2] = kq.AB[2];
           g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
           g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
           g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
@@ -187,14 +242,14 @@ __global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
           }
         }
         any = true;
-        const int K = pr.si[q], L = pr.sj[q];
+        const int K = kq.si, L = kq.sj;
         const double w = wIJ * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
         double ccd[NCD];
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) {
-          const double c1 = w * ql.tcoef[ql.prim[K * MAXCOMP + cc]];
+          const double c1 = w * ql.scoef[K * MAXCOMP + cc];
 #pragma unroll
-          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.tcoef[ql.prim[L * MAXCOMP + d]];
+          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.scoef[L * MAXCOMP + d];
         }
 #pragma unroll
         for (int ab = AB0; ab < AB1; ++ab)
@@ -212,16 +267,16 @@ __global__ void __launch_bounds__(128) k_gq(MolLaunch ql) {
     // digestion of this pass's part of X against the target-space density
     if (!__any_sync(0xffffffffu, any)) continue;   // nothing passed the screens in this chunk
     const double* __restrict__ D = ql.dt;
-    const int I0 = pr.si[g0], J0 = pr.sj[g0], K0 = pr.si[h0], L0 = pr.sj[h0];
+    const int I0 = ijg.x, J0 = ijg.y, K0 = klh.x, L0 = klh.y;
     int ta[NA], tb[NB], tc[NC], td[ND];
 #pragma unroll
-    for (int x = 0; x < NA; ++x) ta[x] = ql.tidx[ql.prim[I0 * MAXCOMP + x]];
+    for (int x = 0; x < NA; ++x) ta[x] = ql.stidx[I0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < NB; ++x) tb[x] = ql.tidx[ql.prim[J0 * MAXCOMP + x]];
+    for (int x = 0; x < NB; ++x) tb[x] = ql.stidx[J0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < NC; ++x) tc[x] = ql.tidx[ql.prim[K0 * MAXCOMP + x]];
+    for (int x = 0; x < NC; ++x) tc[x] = ql.stidx[K0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < ND; ++x) td[x] = ql.tidx[ql.prim[L0 * MAXCOMP + x]];
+    for (int x = 0; x < ND; ++x) td[x] = ql.stidx[L0 * MAXCOMP + x];
     // X(abcd) of this pass (zero outside it: constant-folded in the unrolled loops)
     auto XV = [&](int a, int b, int cc, int d) -> double {
       const int ab = a * NB + b;
@@ -311,14 +366,14 @@ struct Passes {
 };
 
 template <int LA, int LB, int LC, int LD, int NPASS, bool MIXED>
-static void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
+void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
   Passes<LA, LB, LC, LD, NPASS, 0, MIXED>::run(ql, grid, s);
 }
 
 // Launches per straight-line class (its passes); must match the table below.
 static inline int straight_npass(int cb, int ck) {
   static const int np[6][6] = {{1, 0, 0, 0, 0, 0}, {1, 1, 0, 0, 0, 0}, {1, 2, 8, 0, 0, 0},
-                               {1, 1, 5, 3, 0, 0}, {1, 4, 0, 0, 0, 0}, {3, 0, 0, 0, 0, 0}};
+                               {1, 1, 5, 3, 0, 0}, {1, 4, 14, 10, 40, 0}, {3, 10, 50, 25, 0, 0}};
   return np[cb][ck];
 }
 
@@ -336,5 +391,9 @@ static LaunchFn straight_launcher_t(int cb, int ck) {
 #undef Q
   return table[cb][ck];
 }
+
+// The large classes' FP64 passes, one translation unit each (pfe_mol_big*.cu)
+// so that they compile in parallel.
+LaunchFn straight_launcher_big(int cb, int ck);
 
 }  // namespace pfe
