@@ -136,6 +136,35 @@ __device__ __forceinline__ double dt_at(const double* __restrict__ D, int nt, in
 // Classes with more integrals than registers hold X in NPASS launches, pass
 // PASS keeping the bra components ab in [AB0, AB1) (the recursion is repeated
 // per pass; the outputs a pass does not keep are dead code in it).
+// Angular momentum of component i of a cumulative shell, in the reference's
+// component order (x power outer, z power inner: s, z, zz, y, yz, yy, x, xz, xy, xx).
+__host__ __device__ constexpr int comp_tot(int L, int i) {
+  return L == 0 ? 0 : (L == 1 ? (i == 0 ? 0 : 1) : (i == 0 ? 0 : (i == 1 || i == 3 || i == 6) ? 1 : 2));
+}
+
+// Bra component pairs ab = a*NB + b ordered by (|a|, |b|): the passes of a
+// class then keep the lower (for pure shells coefficient-free) components
+// together, and such passes skip their chunks.
+template <int LA, int LB>
+struct AbOrder {
+  static constexpr int NA = ncum(LA), NB = ncum(LB), N = NA * NB;
+  int ab[N];    // k-th pair
+  int pos[N];   // position of pair ab
+  __host__ __device__ constexpr AbOrder() : ab(), pos() {
+    for (int i = 0; i < N; ++i) ab[i] = i;
+    for (int i = 1; i < N; ++i)   // stable insertion sort by (|a|, |b|)
+      for (int j = i; j > 0; --j) {
+        const int x = ab[j - 1], y = ab[j];
+        const int kx = comp_tot(LA, x / NB) * 8 + comp_tot(LB, x % NB);
+        const int ky = comp_tot(LA, y / NB) * 8 + comp_tot(LB, y % NB);
+        if (kx <= ky) break;
+        ab[j - 1] = y;
+        ab[j] = x;
+      }
+    for (int i = 0; i < N; ++i) pos[ab[i]] = i;
+  }
+};
+
 // resident blocks of 128 threads the register allocation aims at: 4 (at most
 // 128 registers) for the classes whose working set fits, else the compiler's choice
 template <int LA, int LB, int LC, int LD>
@@ -156,6 +185,10 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
   constexpr int XN = (AB1 - AB0) * NCD;
   static_assert(AB0 < NAB, "every pass keeps at least one bra component pair");
+  constexpr AbOrder<LA, LB> ORD{};
+  // the pass keeps the pairs ab at positions [AB0, AB1) of ORD; X(k, cd) is pair ORD.ab[AB0 + k]
+  auto in_pass = [&](int a, int b) { const int k = ORD.pos[a * NB + b]; return k >= AB0 && k < AB1; };
+  auto xi = [&](int a, int b, int cc, int d) { return (ORD.pos[a * NB + b] - AB0) * NCD + cc * ND + d; };
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
   const int nchunks = *ql.nchunks;
@@ -172,8 +205,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
       // pure d or p shell) contributes nothing: skip the chunk (warp-uniform)
       bool live = false;
 #pragma unroll
-      for (int ab = AB0; ab < AB1; ++ab)
-        live = live || (ql.stidx[ijg.x * MAXCOMP + ab / NB] >= 0 && ql.stidx[ijg.y * MAXCOMP + ab % NB] >= 0);
+      for (int k = AB0; k < AB1; ++k)
+        live = live || (ql.stidx[ijg.x * MAXCOMP + ORD.ab[k] / NB] >= 0 && ql.stidx[ijg.y * MAXCOMP + ORD.ab[k] % NB] >= 0);
       if (!live) continue;
     }
     const int li = ch.y + lane;
@@ -197,8 +230,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
       const int I = bp.si, J = bp.sj;
       double cab[NAB];
 #pragma unroll
-      for (int ab = AB0; ab < AB1; ++ab)
-        cab[ab] = ql.scoef[I * MAXCOMP + ab / NB] * ql.scoef[J * MAXCOMP + ab % NB];
+      for (int k = AB0; k < AB1; ++k)
+        cab[ORD.ab[k]] = ql.scoef[I * MAXCOMP + ORD.ab[k] / NB] * ql.scoef[J * MAXCOMP + ORD.ab[k] % NB];
       const double zb = bp.zeta;
       const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
       const double Sp = bp.S;
@@ -252,10 +285,11 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
           for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.scoef[L * MAXCOMP + d];
         }
 #pragma unroll
-        for (int ab = AB0; ab < AB1; ++ab)
+        for (int k = AB0; k < AB1; ++k)
 #pragma unroll
           for (int cd = 0; cd < NCD; ++cd)
-            X[(ab - AB0) * NCD + cd] = fma(cab[ab] * ccd[cd], out[ab * NCD + cd], X[(ab - AB0) * NCD + cd]);
+            X[(k - AB0) * NCD + cd] =
+                fma(cab[ORD.ab[k]] * ccd[cd], out[ORD.ab[k] * NCD + cd], X[(k - AB0) * NCD + cd]);
       }
     }
     if (MIXED && PASS == 0) {
@@ -277,44 +311,44 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     for (int x = 0; x < NC; ++x) tc[x] = ql.stidx[K0 * MAXCOMP + x];
 #pragma unroll
     for (int x = 0; x < ND; ++x) td[x] = ql.stidx[L0 * MAXCOMP + x];
-    // X(abcd) of this pass (zero outside it: constant-folded in the unrolled loops)
-    auto XV = [&](int a, int b, int cc, int d) -> double {
-      const int ab = a * NB + b;
-      return (ab >= AB0 && ab < AB1) ? X[(ab - AB0) * NCD + cc * ND + d] : 0.0;
-    };
     // J'(ab) += 1/4 sum_cd P(cd) X: the bra is the warp's, reduce over lanes first
 #pragma unroll
-    for (int ab = AB0; ab < AB1; ++ab) {
+    for (int k = AB0; k < AB1; ++k) {
       double v = 0.0;
 #pragma unroll
       for (int cc = 0; cc < NC; ++cc)
 #pragma unroll
-        for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tc[cc], td[d]), X[(ab - AB0) * NCD + cc * ND + d], v);
+        for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tc[cc], td[d]), X[(k - AB0) * NCD + cc * ND + d], v);
       v = warp_sum(v);
-      if (lane == 0) add_target(ql.jt, nt, ta[ab / NB], tb[ab % NB], 0.25 * v);
+      if (lane == 0) add_target(ql.jt, nt, ta[ORD.ab[k] / NB], tb[ORD.ab[k] % NB], 0.25 * v);
     }
     if (act && any) {
       // J'(cd) += 1/4 sum_ab P(ab) X
       double Pab[NAB];
 #pragma unroll
-      for (int ab = AB0; ab < AB1; ++ab) Pab[ab] = dt_at(D, nt, ta[ab / NB], tb[ab % NB]);
+      for (int k = AB0; k < AB1; ++k) Pab[ORD.ab[k]] = dt_at(D, nt, ta[ORD.ab[k] / NB], tb[ORD.ab[k] % NB]);
 #pragma unroll
       for (int cd = 0; cd < NCD; ++cd) {
         double v = 0.0;
 #pragma unroll
-        for (int ab = AB0; ab < AB1; ++ab) v = fma(Pab[ab], X[(ab - AB0) * NCD + cd], v);
+        for (int k = AB0; k < AB1; ++k) v = fma(Pab[ORD.ab[k]], X[(k - AB0) * NCD + cd], v);
         add_target(ql.jt, nt, tc[cd / ND], td[cd % ND], 0.25 * v);
       }
-      // K'(ad) += 1/8 P(bc) X ; K'(ac) += 1/8 P(bd) X
+      // K'(ad) += 1/8 P(bc) X ; K'(ac) += 1/8 P(bd) X   (in_pass folds at compile time)
 #pragma unroll
-      for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a) {
+      for (int a = 0; a < NA; ++a) {
+        bool a_in = false;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) a_in = a_in || in_pass(a, b);
+        if (!a_in) continue;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
           double v = 0.0;
 #pragma unroll
           for (int b = 0; b < NB; ++b)
+            if (in_pass(a, b))
 #pragma unroll
-            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, tb[b], tc[cc]), XV(a, b, cc, d), v);
+              for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, tb[b], tc[cc]), X[xi(a, b, cc, d)], v);
           add_target(ql.kt, nt, ta[a], td[d], 0.125 * v);
         }
 #pragma unroll
@@ -322,30 +356,37 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
           double v = 0.0;
 #pragma unroll
           for (int b = 0; b < NB; ++b)
+            if (in_pass(a, b))
 #pragma unroll
-            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tb[b], td[d]), XV(a, b, cc, d), v);
+              for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, tb[b], td[d]), X[xi(a, b, cc, d)], v);
           add_target(ql.kt, nt, ta[a], tc[cc], 0.125 * v);
         }
       }
       // K'(bd) += 1/8 P(ac) X ; K'(bc) += 1/8 P(ad) X
 #pragma unroll
       for (int b = 0; b < NB; ++b) {
+        bool b_in = false;
+#pragma unroll
+        for (int a = 0; a < NA; ++a) b_in = b_in || in_pass(a, b);
+        if (!b_in) continue;
 #pragma unroll
         for (int d = 0; d < ND; ++d) {
           double v = 0.0;
 #pragma unroll
-          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
+          for (int a = 0; a < NA; ++a)
+            if (in_pass(a, b))
 #pragma unroll
-            for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, ta[a], tc[cc]), XV(a, b, cc, d), v);
+              for (int cc = 0; cc < NC; ++cc) v = fma(dt_at(D, nt, ta[a], tc[cc]), X[xi(a, b, cc, d)], v);
           add_target(ql.kt, nt, tb[b], td[d], 0.125 * v);
         }
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) {
           double v = 0.0;
 #pragma unroll
-          for (int a = AB0 / NB; a <= (AB1 - 1) / NB; ++a)
+          for (int a = 0; a < NA; ++a)
+            if (in_pass(a, b))
 #pragma unroll
-            for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, ta[a], td[d]), XV(a, b, cc, d), v);
+              for (int d = 0; d < ND; ++d) v = fma(dt_at(D, nt, ta[a], td[d]), X[xi(a, b, cc, d)], v);
           add_target(ql.kt, nt, tb[b], tc[cc], 0.125 * v);
         }
       }
