@@ -15,7 +15,8 @@ CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, '_build')
 LIB = os.path.join(OUT, 'libpolymer_fock.so')
 SOURCES = ['pfe_api.cu', 'pfe_eri.cu', 'pfe_mol.cu', 'pfe_mol_mixed.cu', 'pfe_mol_big1.cu', 'pfe_mol_big2.cu',
-           'pfe_mol_big3.cu', 'pfe_mol_big4.cu', 'pfe_lattice.cu', 'pfe_onee.cu']
+           'pfe_mol_big3.cu', 'pfe_mol_big4.cu', 'pfe_lattice.cu', 'pfe_onee.cu',
+           'pfe_mlp.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550']
@@ -42,7 +43,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     os.makedirs(OUT, exist_ok=True)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cu', '.cuh'))]
     deps += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
-             os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h')]
+             os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h'),
+             os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h')]
     newest = max(os.path.getmtime(d) for d in deps if os.path.exists(d))
     if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not ptxas_info:
         return LIB

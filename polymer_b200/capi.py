@@ -137,6 +137,16 @@ def lib(path: str = LIB_PATH):
     L.pfe_measure_fp64_peak.restype = ctypes.c_int32
     L.pfe_version.argtypes = []
     L.pfe_version.restype = ctypes.c_char_p
+    _vp, _i32, _i64, _f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    for name, args in (('pfe_mlp_gemm', [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _vp]),
+                       ('pfe_mlp_bias_act', [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
+                       ('pfe_mlp_act_grad', [_vp, _vp, _vp, _vp, _i64, _i32, _vp]),
+                       ('pfe_mlp_colsum', [_vp, _vp, _i32, _i32, _vp]),
+                       ('pfe_mlp_mse', [_vp, _vp, _vp, _f32, _vp, _vp, _i64, _vp]),
+                       ('pfe_mlp_adam', [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _f32, _i32, _f32, _vp]),
+                       ('pfe_mlp_to_bf16', [_vp, _vp, _i64, _vp])):
+        getattr(L, name).argtypes = args
+        getattr(L, name).restype = ctypes.c_int32
     _LIB = L
     return L
 
@@ -159,3 +169,7 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
            'pfe_version', 'pfe_overlap_kinetic_noalloc', 'pfe_context_fock_pc',
            'pfe_context_primitive_targets', 'pfe_context_set_screening']
+
+# Exported symbols declared in include/polymer_guess.h (checked by the CPU tests).
+GUESS_EXPORTS = ['pfe_mlp_gemm', 'pfe_mlp_bias_act', 'pfe_mlp_act_grad', 'pfe_mlp_colsum', 'pfe_mlp_mse',
+                 'pfe_mlp_adam', 'pfe_mlp_to_bf16']

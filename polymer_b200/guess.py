@@ -1,0 +1,343 @@
+"""Learned initial guess for water clusters (no counterpart in the reference,
+whose guess is the nuclear-charge diagonal, src/pdensitymatrix.f90:83-127).
+
+An MLP (polymer_b200/mlp.py: the library's BF16 tensor-core kernels) predicts
+the blocks P_AB of the contracted density between atoms A and B, each in the
+frame of the water that owns A (origin O, e1 along the H-O-H bisector, e2
+along H1 - H2), from frame-fixed features of the pair and of A's neighbours.
+Frame blocks are rotated to the laboratory with the exact transformation of
+Cartesian Gaussians (so predictions are rotation-covariant), assembled
+(symmetrised), and purified in FP64: McWeeny iterations in the orthonormal
+(LINDEP) basis, then the occupied natural orbitals.  Training data are
+converged densities of the GPU SCF over seeded water clusters.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+import torch
+
+from .system import System
+
+NEIGHBOURS = 10      # nearest atoms of A used as features
+MAXF = 15            # functions per atom (O in cc-pVDZ: 3s 2p 1d Cartesian = 15)
+R_CUT = 8.0          # bohr: inter-monomer blocks predicted below this A-B distance
+NFEAT = 9 + 6 * NEIGHBOURS   # pair (types 4, frame offset 3, distance, same water) + neighbours
+
+
+def _dfact(n: int) -> int:
+    r = 1
+    while n > 1:
+        r *= n
+        n -= 2
+    return r
+
+
+def _norm(pw) -> float:
+    return 1.0 / math.sqrt(_dfact(2 * pw[0] - 1) * _dfact(2 * pw[1] - 1) * _dfact(2 * pw[2] - 1))
+
+
+def _monomials(L: int):
+    return [(i, j, L - i - j) for i in range(L, -1, -1) for j in range(L - i, -1, -1)]
+
+
+def monomial_transform(L: int, R: np.ndarray) -> Tuple[list, np.ndarray]:
+    """Q with m_i(R u) = sum_j Q_ij m_j(u) for the degree-L monomials (exact: fitted
+    on random points, the relation being polynomial)."""
+    pws = _monomials(L)
+    rng = np.random.default_rng(12345)
+    u = rng.normal(size=(4 * len(pws) + 4, 3))
+    ru = u @ R.T
+
+    def ev(pts):
+        return np.stack([pts[:, 0] ** a * pts[:, 1] ** b * pts[:, 2] ** c for a, b, c in pws], axis=1)
+
+    q, *_ = np.linalg.lstsq(ev(u), ev(ru), rcond=None)
+    return pws, q.T
+
+
+@dataclasses.dataclass
+class AOInfo:
+    live: np.ndarray         # (ncgs,) bool: row of CC not all zero
+    atom: np.ndarray         # (ncgs,) 0-based atom
+    powers: List[tuple]      # Cartesian powers of each contracted function
+    groups: List[List[int]]  # contracted functions of one shell instance (same atom, L, radial part)
+    atom_funcs: List[List[int]]
+
+
+def ao_info(sysm: System) -> AOInfo:
+    b = sysm.basis
+    n = b.ncgs
+    live = np.any(b.cc != 0.0, axis=1)
+    atom = np.zeros(n, dtype=int)
+    powers: List[tuple] = [(0, 0, 0)] * n
+    keys: Dict[tuple, List[int]] = {}
+    for i in range(n):
+        if not live[i]:
+            continue
+        ps = np.nonzero(b.cc[i])[0]
+        p0 = ps[np.argmax(np.abs(b.cc[i, ps]))]
+        pw = (int(b.pax[p0]), int(b.pay[p0]), int(b.paz[p0]))
+        powers[i] = pw
+        atom[i] = int(b.pgs_atom[p0]) - 1
+        radial = tuple(sorted((round(float(b.zt[p]), 10), round(float(b.cc[i, p]) / _norm(pw), 10)) for p in ps))
+        keys.setdefault((atom[i], sum(pw), radial), []).append(i)
+    groups = list(keys.values())
+    natom = sysm.deck.natom
+    atom_funcs = [[i for i in range(n) if live[i] and atom[i] == a] for a in range(natom)]
+    return AOInfo(live, atom, powers, groups, atom_funcs)
+
+
+def frame_transform(info: AOInfo, R: np.ndarray, funcs: List[int]) -> np.ndarray:
+    """U (len(funcs) x len(funcs)) with P_frame = U^T P_lab U for the functions
+    `funcs` (whole shell instances), R mapping frame vectors to lab vectors."""
+    idx = {f: k for k, f in enumerate(funcs)}
+    u = np.zeros((len(funcs), len(funcs)))
+    cache = {}
+    for g in info.groups:
+        if g[0] not in idx:
+            continue
+        L = sum(info.powers[g[0]])
+        if L not in cache:
+            cache[L] = monomial_transform(L, R)
+        pws, q = cache[L]
+        pos = {pw: k for k, pw in enumerate(pws)}
+        for i in g:
+            for j in g:
+                pi, pj = info.powers[i], info.powers[j]
+                u[idx[i], idx[j]] = _norm(pi) * q[pos[pi], pos[pj]] / _norm(pj)
+    return u
+
+
+def water_frames(sysm: System) -> List[Tuple[np.ndarray, np.ndarray, List[int]]]:
+    """(origin, R, atoms) of every water: atoms come as O, H, H in the deck."""
+    d = sysm.deck
+    xyz = np.array(d.coords)
+    out = []
+    for m in range(d.natom // 3):
+        o, h1, h2 = xyz[3 * m], xyz[3 * m + 1], xyz[3 * m + 2]
+        a, c = h1 - o, h2 - o
+        e1 = (a + c) / np.linalg.norm(a + c)
+        e2 = (a - c) - np.dot(a - c, e1) * e1
+        e2 /= np.linalg.norm(e2)
+        e3 = np.cross(e1, e2)
+        out.append((o, np.stack([e1, e2, e3], axis=1), [3 * m, 3 * m + 1, 3 * m + 2]))
+    return out
+
+
+def _type(z: int) -> np.ndarray:
+    return np.array([1.0, 0.0]) if z == 8 else np.array([0.0, 1.0])
+
+
+def pair_list(sysm: System):
+    """(A, B, owner water) of every predicted block: all pairs inside a water and
+    pairs closer than R_CUT, each in the frame of A's water."""
+    d = sysm.deck
+    xyz = np.array(d.coords)
+    pairs = []
+    for a in range(d.natom):
+        for b in range(d.natom):
+            if a // 3 == b // 3 or np.linalg.norm(xyz[a] - xyz[b]) < R_CUT:
+                pairs.append((a, b, a // 3))
+    return pairs
+
+
+def features(sysm: System, frames, pairs) -> np.ndarray:
+    d = sysm.deck
+    xyz = np.array(d.coords)
+    z = d.atoms
+    out = np.zeros((len(pairs), NFEAT))
+    for k, (a, b, m) in enumerate(pairs):
+        o, R, _ = frames[m]
+        rel = R.T @ (xyz[b] - xyz[a])
+        f = [*_type(z[a]), *_type(z[b]), *(rel / 4.0), np.linalg.norm(rel) / 4.0, 1.0 if a // 3 == b // 3 else 0.0]
+        dist = np.linalg.norm(xyz - xyz[a], axis=1)
+        order = [c for c in np.argsort(dist) if c != a and c != b][:NEIGHBOURS]
+        env = []
+        for c in order:
+            rc = R.T @ (xyz[c] - xyz[a])
+            env += [*_type(z[c]), *(rc / 8.0), 1.0 / max(np.linalg.norm(rc), 1e-6)]
+        env += [0.0] * (6 * NEIGHBOURS - len(env))
+        out[k] = np.array(f + env)
+    return out
+
+
+def _u_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
+    key = (a, id(R))
+    if key not in cache:
+        cache[key] = frame_transform(info, R, info.atom_funcs[a])
+    return cache[key]
+
+
+def targets(sysm: System, info: AOInfo, frames, pairs, p_c: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Frame blocks of a converged contracted density, flattened to MAXF x MAXF, and their weights."""
+    t = np.zeros((len(pairs), MAXF * MAXF))
+    w = np.zeros_like(t)
+    cache: dict = {}
+    for k, (a, b, m) in enumerate(pairs):
+        R = frames[m][1]
+        fa, fb = info.atom_funcs[a], info.atom_funcs[b]
+        ua, ub = _u_for_atom(info, R, a, cache), _u_for_atom(info, R, b, cache)
+        blk = ua.T @ p_c[np.ix_(fa, fb)] @ ub
+        full = np.zeros((MAXF, MAXF))
+        full[:len(fa), :len(fb)] = blk
+        t[k] = full.ravel()
+        wm = np.zeros((MAXF, MAXF))
+        wm[:len(fa), :len(fb)] = 1.0
+        w[k] = wm.ravel()
+    return t, w
+
+
+def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.ndarray:
+    """Laboratory contracted density from predicted frame blocks (symmetrised)."""
+    n = sysm.basis.ncgs
+    acc = np.zeros((n, n))
+    cnt = np.zeros((n, n))
+    cache: dict = {}
+    for k, (a, b, m) in enumerate(pairs):
+        R = frames[m][1]
+        fa, fb = info.atom_funcs[a], info.atom_funcs[b]
+        va = np.linalg.inv(_u_for_atom(info, R, a, cache))
+        vb = np.linalg.inv(_u_for_atom(info, R, b, cache))
+        blk = pred[k].reshape(MAXF, MAXF)[:len(fa), :len(fb)]
+        lab = va.T @ blk @ vb
+        acc[np.ix_(fa, fb)] += lab
+        cnt[np.ix_(fa, fb)] += 1.0
+        acc[np.ix_(fb, fa)] += lab.T
+        cnt[np.ix_(fb, fa)] += 1.0
+    return np.where(cnt > 0, acc / np.maximum(cnt, 1.0), 0.0)
+
+
+def purify(st, p_c: torch.Tensor, nocc: int, mcweeny: int = 3) -> torch.Tensor:
+    """FP64: D = P/2 in the orthonormal (LINDEP) basis, McWeeny D <- 3D^2 - 2D^3,
+    then the projector on its nocc leading natural orbitals; returns P_C."""
+    d = st.sys.deck
+    c2s, s0 = st.c2s, st.s_c[0]
+    e_s, v_s = torch.linalg.eigh(c2s @ s0 @ c2s.T)
+    keep = e_s > d.lindep
+    w = c2s.T @ (v_s[:, keep] / torch.sqrt(e_s[keep]))
+    ws = w.T @ s0
+    dm = 0.5 * ws @ p_c @ ws.T
+    for _ in range(mcweeny):
+        d2 = dm @ dm
+        dm = 3.0 * d2 - 2.0 * d2 @ dm
+    ev, vec = torch.linalg.eigh(0.5 * (dm + dm.T))
+    occ = vec[:, -nocc:]
+    co = w @ occ
+    return 2.0 * co @ co.T
+
+
+# ---------------------------------------------------------------- training and use
+
+HIDDEN = (256, 256, 256)
+
+
+def sample_cluster(k: int, seed: int):
+    """A seeded water cluster (cc-pVDZ deck) as used for training and testing."""
+    from . import geometry
+    return geometry.water_deck(k, seed=seed, basis='cc-pVDZ', inttol=1e-12)
+
+
+def cluster_data(sysm: System, p_c: Optional[np.ndarray] = None):
+    info = ao_info(sysm)
+    frames = water_frames(sysm)
+    pairs = pair_list(sysm)
+    x = features(sysm, frames, pairs)
+    if p_c is None:
+        return info, frames, pairs, x
+    t, w = targets(sysm, info, frames, pairs, p_c)
+    return info, frames, pairs, x, t, w
+
+
+def generate(sizes, seeds, device='cuda', log=None):
+    """Converged densities of the GPU SCF for clusters (k, seed): features,
+    frame-block targets and weights, concatenated."""
+    from . import fock, scf, system
+    xs, ts, ws = [], [], []
+    for k, seed in zip(sizes, seeds):
+        s = system.build_system(sample_cluster(k, seed), fock.onee)
+        df = fock.DeviceFock(s)
+        r = scf.run_scf_fast(s, df, opts=scf.FastOptions(incremental=False), device=device)
+        df.close()
+        _, _, _, x, t, w = cluster_data(s, r.p_c[0].cpu().numpy())
+        xs.append(x)
+        ts.append(t)
+        ws.append(w)
+        if log:
+            log('cluster k=%d seed=%d: %d iterations, %d blocks' % (k, seed, len(r.iterations), len(x)))
+    return np.concatenate(xs), np.concatenate(ts), np.concatenate(ws)
+
+
+class LearnedGuess:
+    """The trained network as an initial-guess callable of scf.FastOptions."""
+
+    def __init__(self, net=None, device='cuda'):
+        from .mlp import MLP
+        self.device = torch.device(device)
+        self.net = net or MLP(NFEAT, HIDDEN, MAXF * MAXF, device=device)
+
+    def train(self, x, t, w, steps=2000, batch=512, lr=2e-3, log=None, seed=0):
+        rng = np.random.default_rng(seed)
+        xt = torch.tensor(x, dtype=torch.float32)
+        tt = torch.tensor(t, dtype=torch.float32)
+        wt = torch.tensor(w, dtype=torch.float32)
+        n = len(x)
+        losses = []
+        for step in range(steps):
+            idx = torch.tensor(rng.integers(0, n, size=min(batch, n)))
+            lr_t = lr * 0.5 * (1.0 + math.cos(math.pi * step / steps))
+            loss, gW, gb = self.net.loss_and_grads(xt[idx], tt[idx], wt[idx])
+            self.net.adam_step(gW, gb, lr=lr_t)
+            losses.append(loss)
+            if log and (step % 200 == 0 or step == steps - 1):
+                log('step %d loss %.3e' % (step, loss))
+        return losses
+
+    def predict_blocks(self, x: np.ndarray) -> np.ndarray:
+        out = []
+        for i in range(0, len(x), 4096):
+            out.append(self.net.forward(torch.tensor(x[i:i + 4096], dtype=torch.float32)).double().cpu().numpy())
+        return np.concatenate(out)
+
+    def __call__(self, sysm: System, st) -> torch.Tensor:
+        info, frames, pairs, x = cluster_data(sysm)
+        p = assemble(sysm, info, frames, pairs, self.predict_blocks(x))
+        pc = purify(st, torch.tensor(p, dtype=torch.float64, device=st.device), sysm.deck.nelectrons // 2)
+        return pc.unsqueeze(0)
+
+    def save(self, path: str) -> None:
+        st = self.net.state()
+        st['W'] = [w.to(torch.bfloat16) for w in st['W']]   # the weights the GEMMs use
+        torch.save(st, path)
+
+    @classmethod
+    def load(cls, path: str, device='cuda') -> 'LearnedGuess':
+        from .mlp import MLP
+        st = torch.load(path, map_location='cpu')
+        g = cls(MLP(st['din'], HIDDEN, st['dout'], device=device), device=device)
+        st['W'] = [w.float() for w in st['W']]
+        g.net.load(st)
+        return g
+
+
+MODEL = os.path.join(os.path.dirname(__file__), 'data', 'guess_water_ccpvdz.pt')
+
+
+def train_default(path: str = MODEL, log=print) -> 'LearnedGuess':
+    """The committed network: 60 clusters (k = 2..6, seeds 5000..5059) converged by
+    the GPU SCF, 3000 Adam steps of 1024 blocks (cosine learning rate from 2e-3)."""
+    sizes = [2, 3, 4, 5, 6] * 12
+    seeds = [5000 + i for i in range(len(sizes))]
+    x, t, w = generate(sizes, seeds)
+    lg = LearnedGuess()
+    lg.train(x, t, w, steps=3000, batch=1024, lr=2e-3, log=log)
+    lg.save(path)
+    return lg
+
+
+if __name__ == '__main__':
+    train_default()

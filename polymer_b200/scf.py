@@ -141,7 +141,9 @@ class FastOptions:
     guess: 'nuclear' (the reference's), 'core', or a callable(System, HostState)
       returning a cell-major P_C tensor;
     final_full: once converged, one more iteration with a full FP64 build, whose
-      energy is reported (the fast path is judged by the plain method).
+      energy is reported (the fast path is judged by the plain method);
+    fallback_error: with a callable guess, if max|FPS - SPF| of the first
+      iteration exceeds it, the SCF restarts from the nuclear-charge guess.
     """
     incremental: bool = True
     density_tol: float = 1e-11
@@ -149,6 +151,7 @@ class FastOptions:
     reset_every: int = 8
     guess: object = 'nuclear'
     final_full: bool = True
+    fallback_error: float = 0.5   # a learned guess whose first commutator error exceeds it is replaced
 
 
 def decontract(st: HostState, p_c: torch.Tensor) -> torch.Tensor:
@@ -465,6 +468,8 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
         p_c = opts.guess(sysm, st).to(dtype=torch.float64, device=st.device)
     else:
         p_c = torch.tensor(guess_density(sysm), dtype=torch.float64, device=st.device)
+    learned = callable(opts.guess)
+    fallback = False
     nocc = d.nelectrons // 2
     c2s, s0 = st.c2s, st.s_c[0]
     e_s, v_s = _eigh(c2s @ s0 @ c2s.T)
@@ -516,6 +521,17 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
         vals = e_vals.cpu().numpy()
         e = float(vals[0]) + sysm.e_nuc
         fe = float(vals[1])
+        if learned and iscf == 1 and fe > opts.fallback_error:
+            # the learned guess is judged by the plain one: restart from the nuclear-charge guess
+            fallback = True
+            p_c = torch.tensor(guess_density(sysm), dtype=torch.float64, device=st.device)
+            hist_f.clear()
+            hist_e.clear()
+            ref = None
+            nbuild = 0
+            if log:
+                log('  1  guess error %.3e above %.3e: nuclear-charge guess' % (fe, opts.fallback_error))
+            continue
         if m >= 2:
             bm = np.zeros((m + 1, m + 1))
             k = 2
@@ -550,7 +566,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
         p_c = p_new
     if not converged and raise_on_fail:
         raise SCFError('SCF CONVERGENCE NOT MET')
-    comp = {'total': e}
+    comp = {'total': e, 'guess_fallback': fallback, 'first_error': iters[0].asymmetry if iters else None}
     res = SCFResult(converged, e, comp, iters, p_c, eps, float(iters[-1].fermi) if iters else 0.0, fock_s,
                     time.perf_counter() - t0, e)
     return res

@@ -19,20 +19,24 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, 'include', 'polymer_fock.h')
 
 
-def _declared():
-    txt = open(HEADER).read()
+GUESS_HEADER = os.path.join(ROOT, 'include', 'polymer_guess.h')
+
+
+def _declared(path=HEADER):
+    txt = open(path).read()
     return sorted(set(re.findall(r'\b(pfe_[a-z0-9_]+)\s*\(', txt)))
 
 
 def test_header_declares_the_exports():
     assert _declared() == sorted(capi.EXPORTS)
+    assert _declared(GUESS_HEADER) == sorted(capi.GUESS_EXPORTS)
 
 
 def test_library_exports_every_symbol():
     lib = build.build()
     out = subprocess.run(['nm', '-D', '--defined-only', lib], capture_output=True, text=True, check=True).stdout
     exported = set(ln.split()[-1] for ln in out.splitlines() if ln.strip())
-    missing = [s for s in capi.EXPORTS if s not in exported]
+    missing = [s for s in capi.EXPORTS + capi.GUESS_EXPORTS if s not in exported]
     assert not missing, missing
 
 

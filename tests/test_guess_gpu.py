@@ -1,0 +1,59 @@
+"""The learned initial guess (polymer_b200/guess.py, network in
+polymer_b200/data/guess_water_ccpvdz.pt, trained on clusters of 2-6 waters) on
+held-out water clusters of 8 waters: against the reference's nuclear-charge
+guess it must start the SCF much closer to self-consistency (first commutator
+error below a fifth), need no more iterations, trigger no fallback, and reach
+the same energy (1e-8 Eh).
+"""
+import numpy as np
+import pytest
+import torch
+
+from polymer_b200 import fock, guess, scf, system
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def learned():
+    return guess.LearnedGuess.load(guess.MODEL)
+
+
+@pytest.mark.parametrize('seed', [9100, 9101])
+def test_learned_guess_gains_over_the_nuclear_guess(learned, seed):
+    s = system.build_system(guess.sample_cluster(8, seed), fock.onee)
+    df = fock.DeviceFock(s)
+    plain = scf.run_scf_fast(s, df, opts=scf.FastOptions(guess='nuclear'))
+    lg = scf.run_scf_fast(s, df, opts=scf.FastOptions(guess=learned))
+    df.close()
+    assert not lg.components['guess_fallback']
+    assert lg.components['first_error'] < 0.2 * plain.components['first_error']
+    assert len(lg.iterations) <= len(plain.iterations)
+    assert abs(lg.energy - plain.energy) < 1e-8
+
+
+def test_guess_is_rotation_covariant(learned):
+    """Rotating the whole cluster rotates the predicted density (frames are per water):
+    the guess energies agree up to the BF16 rounding of the network's inputs (the
+    frame machinery itself is exact: tests/test_guess_cpu.py)."""
+    from polymer_b200 import inputdeck
+    s = system.build_system(guess.sample_cluster(4, 9200), fock.onee)
+    st = scf.HostState(s, 'cuda')
+    p1 = learned(s, st)[0].cpu().numpy()
+    d = s.deck
+    th = 0.7
+    rot = np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1.0]])
+    xyz = np.array(d.coords) @ rot.T
+    d2 = inputdeck.make_deck(d.atoms, xyz, 'cc-pVDZ', inttol=1e-12)
+    s2 = system.build_system(d2, fock.onee)
+    p2 = learned(s2, scf.HostState(s2, 'cuda'))[0].cpu().numpy()
+    # energies of the two guesses with their own Fock builds agree: E is invariant
+    e = []
+    for sysm, p in ((s, p1), (s2, p2)):
+        st2 = scf.HostState(sysm, 'cuda')
+        df = fock.DeviceFock(sysm)
+        c, x = df.from_pc(torch.tensor(p, device='cuda'))
+        pt = torch.tensor(p, device='cuda')[None]
+        e.append(scf.energy(st2, pt, c, x, 1.0, sysm.e_nuc, 0.0, None, 0.0, sysm.deck.nelectrons)[0])
+        df.close()
+    assert abs(e[0] - e[1]) < 1e-3
