@@ -122,6 +122,26 @@ int32_t pfe_context_set_screening(pfe_context *ctx, int32_t precision_mode, doub
  * reference. */
 int32_t pfe_context_primitive_targets(pfe_context *ctx, int32_t enable);
 
+/* ---- batches of molecules (no counterpart in the reference) ----
+ * Many molecules whose Fock builds run together: every instance is set up as
+ * by pfe_context_setup, and one build runs one kernel launch per quartet class
+ * (and pass) over every instance's work.  Densities and outputs are packed:
+ * instance k's ncgs x ncgs column-major matrix starts at offset off[k] (in
+ * doubles) of one device buffer; pfe_batch_offsets writes off[0..n] and returns n. */
+typedef struct pfe_batch pfe_batch;
+int32_t pfe_batch_create(int32_t device, pfe_batch **out);
+int32_t pfe_batch_setup(pfe_batch *b, const pfe_args *instances, int32_t n);
+int32_t pfe_batch_offsets(pfe_batch *b, int64_t *off);
+/* pfe_context_set_screening applied to every instance. */
+int32_t pfe_batch_set_screening(pfe_batch *b, int32_t precision_mode, double mixed_cutoff, double density_tol);
+/* The same for instance k alone (0 <= k < n): instances of one build may use
+ * different thresholds; an instance whose density difference is zero and whose
+ * density_tol is positive skips all of its quartets. */
+int32_t pfe_batch_set_instance_screening(pfe_batch *b, int32_t k, int32_t precision_mode, double mixed_cutoff,
+                                         double density_tol);
+int32_t pfe_batch_fock_pc(pfe_batch *b, const double *d_p_c, double *d_c_c, double *d_x_c, void *stream);
+int32_t pfe_batch_destroy(pfe_batch *b);
+
 /* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */
 typedef struct pfe_census {
   double quartets;          /* screened primitive-shell quartets computed per build   */
@@ -132,6 +152,8 @@ typedef struct pfe_census {
   int32_t kernel_launches;  /* kernels launched by one pfe_context_fock call          */
 } pfe_census;
 int32_t pfe_context_census(pfe_context *ctx, pfe_census *out);
+/* The same summed over a batch's instances (kernel_launches: one batched build). */
+int32_t pfe_batch_census(pfe_batch *b, pfe_census *out);
 
 /* Per-kernel timing of pfe_context_fock (diagnostics; no counterpart in the
  * reference).  With profiling on, every quartet-class launch is bracketed by

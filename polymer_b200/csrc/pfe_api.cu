@@ -517,6 +517,103 @@ int32_t pfe_context_set_screening(pfe_context* ctx, int32_t precision_mode, doub
   return PFE_OK;
 }
 
+int32_t pfe_batch_create(int32_t device, pfe_batch** out) {
+  if (!out) { set_error("null output handle"); return PFE_EINVAL; }
+  int ndev = 0;
+  PFE_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) { set_error("no such CUDA device"); return PFE_EINVAL; }
+  pfe_batch* b = new pfe_batch();
+  b->device = device;
+  *out = b;
+  return PFE_OK;
+}
+
+int32_t pfe_batch_destroy(pfe_batch* b) {
+  if (!b) return PFE_OK;
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  for (pfe_context* c : b->inst) pfe_context_destroy(c);
+  b->release_all();
+  delete b;
+  return PFE_OK;
+}
+
+int32_t pfe_batch_setup(pfe_batch* b, const pfe_args* args, int32_t n) {
+  if (!b || !args || n < 1) { set_error("pfe_batch_setup: bad argument"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(b->device));
+  for (pfe_context* c : b->inst) pfe_context_destroy(c);
+  b->inst.clear();
+  b->release_all();
+  b->off.assign(1, 0);
+  for (int k = 0; k < n; ++k) {
+    pfe_context* c = nullptr;
+    int rc = pfe_context_create(b->device, &c);
+    if (rc != PFE_OK) return rc;
+    b->inst.push_back(c);
+    if ((rc = pfe_context_setup(c, &args[k])) != PFE_OK) return rc;
+    if (!c->molecular) { set_error("pfe_batch_setup: batches hold molecules only"); return PFE_EUNSUPPORTED; }
+    if (c->numprocs != 1) { set_error("pfe_batch_setup: one rank per batch (numprocs 1)"); return PFE_EUNSUPPORTED; }
+    b->off.push_back(b->off.back() + (long long)c->ncgs * c->ncgs);
+  }
+  return batch_setup(b);
+}
+
+int32_t pfe_batch_set_screening(pfe_batch* b, int32_t precision_mode, double mixed_cutoff, double density_tol) {
+  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  for (pfe_context* c : b->inst) {
+    int rc = pfe_context_set_screening(c, precision_mode, mixed_cutoff, density_tol);
+    if (rc != PFE_OK) return rc;
+  }
+  b->insts_for = nullptr;   // the launch records carry the thresholds
+  return PFE_OK;
+}
+
+int32_t pfe_batch_set_instance_screening(pfe_batch* b, int32_t k, int32_t precision_mode, double mixed_cutoff,
+                                         double density_tol) {
+  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (k < 0 || k >= (int)b->inst.size()) { set_error("no such instance in the batch"); return PFE_EINVAL; }
+  pfe_context* c = b->inst[k];
+  const double mc = c->mcut, dt = c->dtol;
+  int rc = pfe_context_set_screening(c, precision_mode, mixed_cutoff, density_tol);
+  if (rc != PFE_OK) return rc;
+  if (c->mcut != mc || c->dtol != dt) b->insts_for = nullptr;
+  return PFE_OK;
+}
+
+int32_t pfe_batch_offsets(pfe_batch* b, int64_t* off) {
+  if (!b || !off) { set_error("null argument"); return PFE_EINVAL; }
+  for (size_t k = 0; k < b->off.size(); ++k) off[k] = b->off[k];
+  return (int32_t)b->inst.size();
+}
+
+int32_t pfe_batch_fock_pc(pfe_batch* b, const double* d_p_c, double* d_c_c, double* d_x_c, void* stream) {
+  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!d_p_c || !d_c_c || !d_x_c) { set_error("null device pointer"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(b->device));
+  return batch_fock_pc(b, d_p_c, d_c_c, d_x_c, (cudaStream_t)stream);
+}
+
+int32_t pfe_batch_census(pfe_batch* b, pfe_census* out) {
+  if (!b || !out) { set_error("null argument"); return PFE_EINVAL; }
+  pfe_census tot{};
+  for (pfe_context* c : b->inst) {
+    pfe_census ci{};
+    int rc = pfe_context_census(c, &ci);
+    if (rc != PFE_OK) return rc;
+    tot.quartets += ci.quartets;
+    tot.quartets_ref += ci.quartets_ref;
+    tot.quartets_fp32 += ci.quartets_fp32;
+    tot.flops += ci.flops;
+    tot.pairs += ci.pairs;
+  }
+  int n = 0;
+  for (int i = 0; i < b->nlaunch; ++i)
+    n += (b->launches[i].variant == 0 && b->launches[i].has_straight) ? b->launches[i].npass : 1;
+  tot.kernel_launches = n;
+  *out = tot;
+  return PFE_OK;
+}
+
 int32_t pfe_context_primitive_targets(pfe_context* ctx, int32_t enable) {
   if (!ctx) { set_error("null context"); return PFE_EINVAL; }
   if (ctx->force_primitive != (enable != 0)) {

@@ -174,7 +174,33 @@ struct pfe_context {
   }
 };
 
+// Many molecules whose Fock builds run together (struct pfe_batch of the C ABI):
+// every instance has its own context (set-up, pairs, chunks); the batch joins
+// their chunk lists per quartet class, each chunk tagged with its instance, so
+// one launch per class (and pass) covers every instance.
+struct pfe_batch {
+  int device = 0;
+  std::vector<pfe_context*> inst;
+  std::vector<long long> off;       // packed offsets (doubles) of the ncgs x ncgs matrices, n+1
+  pfe::ClassLaunch launches[64];    // joined chunk lists; ops/tables of the first instance with the class
+  int nlaunch = 0;
+  void* d_insts = nullptr;          // the instances' launch records (MolLaunch), rebuilt per density pointer
+  const double* insts_for = nullptr;
+  std::vector<void*> owned;
+  cudaError_t alloc(void** p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e == cudaSuccess) owned.push_back(*p);
+    return e;
+  }
+  void release_all() {
+    for (void* p : owned) cudaFree(p);
+    owned.clear();
+  }
+};
+
 namespace pfe {
+int batch_setup(pfe_batch* b);
+int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
 int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n);
 void free_pairs(pfe_context* ctx, PairArrays* pa);
 void launch_symmetrize(const double* a, double* out, int n, int ncell, cudaStream_t s);

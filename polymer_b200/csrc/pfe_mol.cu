@@ -519,9 +519,11 @@ __global__ void __launch_bounds__(256) k_gq_warp(MolLaunch ql, OpTableDev tab, i
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   const int nchunks = *ql.nchunks;
   const int stride = gridDim.x * wpb * ql.numprocs;
-  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride)
-    gq_team<LA, LB, LC, LD, false>(ql, tab, ql.chunks[c], smem + (size_t)wid * per_warp, nullptr, s_geo[wid],
-                                   s_prm[wid], s_w + wid, lane, 32);
+  for (int c = (blockIdx.x * wpb + wid) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
+    const int4 ch = ql.chunks[c];
+    gq_team<LA, LB, LC, LD, false>(ql.insts ? ql.insts[ch.w] : ql, tab, ch, smem + (size_t)wid * per_warp, nullptr,
+                                   s_geo[wid], s_prm[wid], s_w + wid, lane, 32);
+  }
 }
 
 // xg: per-block X scratch in global memory (gridDim.x * NI doubles), or null
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(256) k_gq_block(MolLaunch ql, OpTableDev tab, 
   __shared__ double s_w[1];
   const int nchunks = *ql.nchunks;
   for (int c = blockIdx.x * ql.numprocs + ql.myid; c < nchunks; c += gridDim.x * ql.numprocs)
-    gq_team<LA, LB, LC, LD, true>(ql, tab, ql.chunks[c], smem,
+    gq_team<LA, LB, LC, LD, true>(ql.insts ? ql.insts[ql.chunks[c].w] : ql, tab, ql.chunks[c], smem,
                                   xg ? xg + (size_t)blockIdx.x * (ncum(LA) * ncum(LB) * ncum(LC) * ncum(LD)) : nullptr,
                                   s_geo, s_prm, s_w, threadIdx.x, blockDim.x);
 }
@@ -898,13 +900,14 @@ static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   return ql;
 }
 
-static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, int variant, cudaStream_t s) {
+static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, int variant, cudaStream_t s,
+                         bool mixed) {
   ql.chunks = cl.chunks;
   ql.nchunks = cl.d_nchunks;
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
   if ((variant == 0 && cl.has_straight) || !cl.has_table) {
     const int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
-    straight_launcher(cl.cb, cl.ck, ctx->mcut > 0.0)(ql, std::max(grid, 1), s);
+    straight_launcher(cl.cb, cl.ck, mixed)(ql, std::max(grid, 1), s);
     return;
   }
   OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
@@ -950,11 +953,11 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
     int bestv = cl.variant;
     for (int v = 0; v < 3; ++v) {
       if (!variant_ok(cl, v)) continue;
-      launch_class(ctx, cl, ql, v, s);
+      launch_class(ctx, cl, ql, v, s, ctx->mcut > 0.0);
       float t = 1e30f;
       for (int r = 0; r < 2; ++r) {
         PFE_CUDA(cudaEventRecord(e0, s));
-        launch_class(ctx, cl, ql, v, s);
+        launch_class(ctx, cl, ql, v, s, ctx->mcut > 0.0);
         PFE_CUDA(cudaEventRecord(e1, s));
         PFE_CUDA(cudaEventSynchronize(e1));
         float ms = 0.f;
@@ -976,7 +979,9 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
   return PFE_OK;
 }
 
-static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double* d_xc, cudaStream_t s) {
+// Zero the target-space J'/K' and the FP32 counter; block maxima of the density
+// when screening or mixed precision is on.
+static int prepare_build(pfe_context* ctx, const double* d_dt, cudaStream_t s) {
   PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
@@ -987,6 +992,12 @@ static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double*
                                                                (unsigned long long*)ctx->d_bmax);
     PFE_CUDA(cudaGetLastError());
   }
+  return PFE_OK;
+}
+
+static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double* d_xc, cudaStream_t s) {
+  const int rc = prepare_build(ctx, d_dt, s);
+  if (rc != PFE_OK) return rc;
   const MolLaunch ql = make_launch(ctx, d_dt);
   if (ctx->profile) {
     for (int i = 0; i <= ctx->nlaunch && i < 64; ++i)
@@ -996,7 +1007,7 @@ static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double*
   }
   for (int i = 0; i < ctx->nlaunch; ++i) {
     const ClassLaunch& cl = ctx->launches[i];
-    launch_class(ctx, cl, ql, cl.variant, s);
+    launch_class(ctx, cl, ql, cl.variant, s, ctx->mcut > 0.0);
     PFE_CUDA(cudaGetLastError());
     if (ctx->profile) {
       PFE_CUDA(cudaEventRecord(ctx->ev[i + 1], s));
@@ -1049,6 +1060,117 @@ int molecular_density_ok(pfe_context* ctx, cudaStream_t s, bool* ok) {
   PFE_CUDA(cudaMemcpyAsync(&f, ctx->d_flag, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
   PFE_CUDA(cudaStreamSynchronize(s));
   *ok = (f == 0);
+  return PFE_OK;
+}
+
+}  // namespace pfe
+
+// ------------------------------------------------------------------ batches
+
+namespace pfe {
+
+__global__ void k_tag_chunks(int4* __restrict__ chunks, int n, int instance) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) chunks[t].w = instance;
+}
+
+// Join the instances' chunk lists per (bra class, ket class).
+int batch_setup(pfe_batch* b) {
+  b->nlaunch = 0;
+  for (int cb = 0; cb < 6; ++cb)
+    for (int ck = 0; ck <= cb; ++ck) {
+      long long total = 0;
+      const ClassLaunch* tmpl = nullptr;
+      for (pfe_context* c : b->inst)
+        for (int i = 0; i < c->nlaunch; ++i)
+          if (c->launches[i].cb == cb && c->launches[i].ck == ck) {
+            total += c->launches[i].nchunks_host;
+            if (!tmpl) tmpl = &c->launches[i];
+          }
+      if (!tmpl || total == 0) continue;
+      if (total >= (1LL << 31)) { set_error("batch: too many chunks in one quartet class"); return PFE_EINVAL; }
+      ClassLaunch cl = *tmpl;
+      cl.nchunks_host = (int)total;
+      cl.quartets = 0.0;
+      PFE_CUDA(b->alloc((void**)&cl.chunks, sizeof(int4) * total));
+      PFE_CUDA(b->alloc((void**)&cl.d_nchunks, sizeof(int)));
+      PFE_CUDA(cudaMemcpy(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice));
+      long long o = 0;
+      for (size_t k = 0; k < b->inst.size(); ++k) {
+        pfe_context* c = b->inst[k];
+        for (int i = 0; i < c->nlaunch; ++i) {
+          const ClassLaunch& li = c->launches[i];
+          if (li.cb != cb || li.ck != ck) continue;
+          PFE_CUDA(cudaMemcpy(cl.chunks + o, li.chunks, sizeof(int4) * li.nchunks_host, cudaMemcpyDeviceToDevice));
+          k_tag_chunks<<<(li.nchunks_host + 255) / 256, 256>>>(cl.chunks + o, li.nchunks_host, (int)k);
+          PFE_CUDA(cudaGetLastError());
+          o += li.nchunks_host;
+          cl.quartets += li.quartets;
+        }
+      }
+      b->launches[b->nlaunch++] = cl;
+    }
+  PFE_CUDA(b->alloc(&b->d_insts, sizeof(MolLaunch) * b->inst.size()));
+  b->insts_for = nullptr;
+  PFE_CUDA(cudaDeviceSynchronize());
+  return PFE_OK;
+}
+
+// One build of every instance from the packed contracted densities d_pc.
+int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s) {
+  const size_t n = b->inst.size();
+  // target-space densities: P_C itself, or P_P = CC^T P_C CC for primitive targets
+  for (size_t k = 0; k < n; ++k) {
+    pfe_context* c = b->inst[k];
+    if (c->contracted) continue;
+    const int np = c->npgs, nc = c->ncgs;
+    const double one = 1.0, zero = 0.0;
+    cublasSetStream(c->blas, s);
+    if (cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, np, nc, &one, d_pc + b->off[k], nc, c->d_cc, nc, &zero,
+                    c->d_w1, nc) != CUBLAS_STATUS_SUCCESS ||
+        cublasDgemm(c->blas, CUBLAS_OP_T, CUBLAS_OP_N, np, np, nc, &one, c->d_cc, nc, c->d_w1, nc, &zero, c->d_pt,
+                    np) != CUBLAS_STATUS_SUCCESS) {
+      set_error("batch: cublasDgemm (decontraction) failed");
+      return PFE_ECUDA;
+    }
+  }
+  if (b->insts_for != d_pc) {
+    // earlier builds on this stream may still read the records
+    PFE_CUDA(cudaStreamSynchronize(s));
+    std::vector<MolLaunch> h(n);
+    for (size_t k = 0; k < n; ++k) {
+      pfe_context* c = b->inst[k];
+      h[k] = make_launch(c, c->contracted ? d_pc + b->off[k] : c->d_pt);
+    }
+    PFE_CUDA(cudaMemcpy(b->d_insts, h.data(), sizeof(MolLaunch) * n, cudaMemcpyHostToDevice));
+    b->insts_for = d_pc;
+  }
+  for (size_t k = 0; k < n; ++k) {
+    pfe_context* c = b->inst[k];
+    const int rc = prepare_build(c, c->contracted ? d_pc + b->off[k] : c->d_pt, s);
+    if (rc != PFE_OK) return rc;
+  }
+  pfe_context* c0 = b->inst[0];
+  MolLaunch lq = make_launch(c0, c0->d_pt);
+  lq.insts = static_cast<const MolLaunch*>(b->d_insts);
+  bool mixed = false;   // the FP32-capable kernels, when any instance uses them
+  for (pfe_context* c : b->inst) mixed = mixed || c->mcut > 0.0;
+  for (int i = 0; i < b->nlaunch; ++i) {
+    const ClassLaunch& cl = b->launches[i];
+    launch_class(c0, cl, lq, cl.variant, s, mixed);
+    PFE_CUDA(cudaGetLastError());
+  }
+  for (size_t k = 0; k < n; ++k) {
+    pfe_context* c = b->inst[k];
+    if (c->contracted) {
+      launch_symmetrize(c->d_jp, d_cc + b->off[k], c->ncgs, 1, s);
+      launch_symmetrize(c->d_kp, d_xc + b->off[k], c->ncgs, 1, s);
+    } else {
+      int rc = contract_outputs(c, c->d_jp, c->d_kp, d_cc + b->off[k], d_xc + b->off[k], true, 1, s);
+      if (rc != PFE_OK) return rc;
+    }
+  }
+  PFE_CUDA(cudaGetLastError());
   return PFE_OK;
 }
 

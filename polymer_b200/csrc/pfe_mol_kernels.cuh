@@ -68,6 +68,7 @@ struct MolLaunch {
   double inttol;
   int nt;
   int myid, numprocs;
+  const MolLaunch* insts;   // batches: the launch record of every instance (chunk .w), else null
 };
 
 // max|P_T| over the six density blocks a group quartet's digestion reads
@@ -174,7 +175,7 @@ struct GqOccupancy {
 };
 
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
-__global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch ql) {
+__global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch lq) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
   constexpr int NI = NA * NB * NC * ND;
   constexpr int NAB = NA * NB;
@@ -191,12 +192,13 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   auto xi = [&](int a, int b, int cc, int d) { return (ORD.pos[a * NB + b] - AB0) * NCD + cc * ND + d; };
   const int lane = threadIdx.x & 31;
   const int wpb = blockDim.x >> 5;
-  const int nchunks = *ql.nchunks;
-  const int stride = gridDim.x * wpb * ql.numprocs;
+  const int nchunks = *lq.nchunks;
+  const int stride = gridDim.x * wpb * lq.numprocs;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  const int nt = ql.nt;
-  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * ql.numprocs + ql.myid; c < nchunks; c += stride) {
-    const int4 ch = ql.chunks[c];
+  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * lq.numprocs + lq.myid; c < nchunks; c += stride) {
+    const int4 ch = lq.chunks[c];
+    const MolLaunch& ql = lq.insts ? lq.insts[ch.w] : lq;   // this chunk's instance
+    const int nt = ql.nt;
     const int G = ch.x;
     const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
     const int2 ijg = __ldg(reinterpret_cast<const int2*>(&ql.rec[g0].si));

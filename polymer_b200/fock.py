@@ -156,3 +156,80 @@ def host_fock_builder(sysm: System, **kw):
         return (torch.tensor(c, dtype=torch.float64, device=p_p.device),
                 torch.tensor(x, dtype=torch.float64, device=p_p.device))
     return f
+
+
+class DeviceBatch:
+    """Fock builds of many molecules at once (``pfe_batch``): each quartet class
+    is one kernel launch over the work of every molecule.  Densities and outputs
+    live packed in one device buffer each, molecule k's ncgs x ncgs matrix
+    (column-major) at ``off[k]``."""
+
+    def __init__(self, systems, device: int = 0, **kw):
+        self.L = lib()
+        self.systems = list(systems)
+        self.device = device
+        h = ctypes.c_void_p()
+        check(self.L, self.L.pfe_batch_create(device, ctypes.byref(h)))
+        self.handle = h
+        args, self._keep = [], []
+        for s in self.systems:
+            if s.ncell1 != 1:
+                raise ValueError('a batch holds molecules only')
+            a, keep = s.pfe_args(None, None, **kw)
+            args.append(a)
+            self._keep.append(keep)
+        arr = (capi.PfeArgs * len(args))(*args)
+        check(self.L, self.L.pfe_batch_setup(self.handle, arr, len(args)))
+        off = (ctypes.c_int64 * (len(args) + 1))()
+        n = self.L.pfe_batch_offsets(self.handle, off)
+        if n != len(args):
+            raise capi.FockError('pfe_batch_offsets: %d instances, expected %d' % (n, len(args)))
+        self.off = [int(v) for v in off]
+        self.ncgs = [s.basis.ncgs for s in self.systems]
+        dev = torch.device('cuda', device)
+        self.p_c = torch.zeros(self.off[-1], dtype=torch.float64, device=dev)
+        self.out_c = torch.empty_like(self.p_c)
+        self.out_x = torch.empty_like(self.p_c)
+
+    def __len__(self) -> int:
+        return len(self.systems)
+
+    def census(self) -> dict:
+        c = PfeCensus()
+        check(self.L, self.L.pfe_batch_census(self.handle, ctypes.byref(c)))
+        return {'quartets': c.quartets, 'quartets_ref': c.quartets_ref, 'flops': c.flops,
+                'quartets_fp32': c.quartets_fp32, 'pairs': c.pairs, 'kernel_launches': c.kernel_launches}
+
+    def set_screening(self, mixed_cutoff: float = 0.0, density_tol: float = 0.0) -> None:
+        mode = capi.PFE_PREC_MIXED if mixed_cutoff > 0.0 else capi.PFE_PREC_FP64
+        check(self.L, self.L.pfe_batch_set_screening(self.handle, mode, float(mixed_cutoff), float(density_tol)))
+
+    def view(self, packed: torch.Tensor, k: int) -> torch.Tensor:
+        """Molecule k's matrix of a packed buffer (a transposed view: row-major indices)."""
+        n = self.ncgs[k]
+        return packed[self.off[k]:self.off[k + 1]].view(n, n).t()
+
+    def run_packed(self, p_c: torch.Tensor, out_c: torch.Tensor, out_x: torch.Tensor, stream=None) -> None:
+        """Raw call on packed device buffers (pfe_batch_fock_pc), asynchronous."""
+        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
+        check(self.L, self.L.pfe_batch_fock_pc(self.handle, ctypes.c_void_p(p_c.data_ptr()),
+                                               ctypes.c_void_p(out_c.data_ptr()),
+                                               ctypes.c_void_p(out_x.data_ptr()), ctypes.c_void_p(s)))
+
+    def __call__(self, p_list):
+        """List of device P_C (ncgs x ncgs) -> list of (C_C, X_C)."""
+        for k, p in enumerate(p_list):
+            self.view(self.p_c, k).copy_(p)
+        self.run_packed(self.p_c, self.out_c, self.out_x)
+        return [(self.view(self.out_c, k).clone(), self.view(self.out_x, k).clone()) for k in range(len(self))]
+
+    def close(self):
+        if self.handle is not None:
+            self.L.pfe_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
