@@ -1,0 +1,396 @@
+"""Batched closed-shell SCF of many molecules on one GPU (no counterpart in the
+reference, whose SELF_CONSISTENT_FIELD, src/pselfconsistentfield.f90:1-162,
+runs one system).
+
+Every SCF iteration of the whole batch does:
+
+* one batched Fock build (``pfe_batch_fock_pc``: one kernel launch per quartet
+  class over every molecule's work), incremental from the change of each
+  molecule's density with density screening and optional FP32 recursion, as
+  the fast single-molecule SCF (``scf.run_scf_fast``) does; screening is set
+  per molecule, so a converged molecule (zero difference) skips all of its
+  quartets;
+* per group of molecules of equal size, batched FP64 products on the GPU:
+  Fock assembly F = H + J - K/2, Pulay's commutator DIIS (error FPS - SPF in
+  the orthonormal LINDEP basis), and the new density as the spectral projector
+  on the nocc lowest orbitals, computed by second-order spectral projection
+  (SP2: Niklasson, Phys. Rev. B 66, 155115 (2002), with the trace rule of
+  Niklasson, Tymczak and Challacombe) -- products only, no diagonalisation;
+* one device-to-host read of a few numbers per molecule (energy, DIIS error,
+  density change) to decide convergence.
+
+Convergence and energy are those of the single-molecule path: RMS change of
+P_C below SCFCONV, then one more iteration on a full FP64 build whose energy
+E[P] = tr P (H + J/2 - K/4) + E_nuc of the idempotent density is reported.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import time
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import fock as fock_mod
+from .scf import SCFError, guess_density
+from .system import System
+
+F64 = torch.float64
+
+# per-molecule states of one iteration
+_FULL, _INCR, _FINAL, _DONE = 0, 1, 2, 3
+
+
+@dataclasses.dataclass
+class BatchOptions:
+    """incremental / density_tol / mixed_cutoff / reset_every as in scf.FastOptions;
+    guess: 'nuclear' (the reference's GUESS_DENSITYMATRIX), 'core', or an object
+    with ``raw(sysm) -> np.ndarray`` giving an unpurified contracted density per
+    molecule (the learned guess), purified here on the GPU and judged by
+    ``fallback_error`` (first DIIS error above it: restart from 'nuclear')."""
+    incremental: bool = True
+    density_tol: float = 1e-11
+    mixed_cutoff: float = 0.0
+    reset_every: int = 8
+    guess: object = 'nuclear'
+    fallback_error: float = 0.5
+    ndiis: int = 8
+    sp2_tol: float = 1e-12
+    sp2_max: int = 200
+
+
+@dataclasses.dataclass
+class BatchResult:
+    energy: np.ndarray          # E[P] per molecule (Eh), input order
+    converged: np.ndarray       # bool per molecule
+    iterations: np.ndarray      # SCF iterations per molecule (to convergence)
+    builds: int                 # batched Fock builds
+    seconds: float
+    first_error: np.ndarray     # max|FPS - SPF| of the first iteration per molecule
+    fallback: np.ndarray        # the learned guess was rejected
+    p_c: List[torch.Tensor]     # converged contracted densities, input order
+    sp2_steps: int              # SP2 products over the run (per group, summed)
+
+
+def _trace(x: torch.Tensor) -> torch.Tensor:
+    return x.diagonal(dim1=-2, dim2=-1).sum(-1)
+
+
+class _Group:
+    """Molecules of one size (ncgs, nocc), contiguous in the packed buffers."""
+
+    def __init__(self, members: List[int], systems: List[System], lo: int, device):
+        s0 = systems[members[0]]
+        self.members = members
+        self.n = s0.basis.ncgs
+        self.nocc = s0.deck.nelectrons // 2
+        self.B = len(members)
+        self.lo, self.hi = lo, lo + self.B * self.n * self.n
+        n, B = self.n, self.B
+        f64 = dict(dtype=F64, device=device)
+        self.h = torch.empty((B, n, n), **f64)
+        self.w = torch.zeros((B, n, n), **f64)
+        self.ws = torch.zeros((B, n, n), **f64)
+        self.pad = torch.zeros((B, n), dtype=torch.bool, device=device)
+        self.hfx = torch.empty((B, 1, 1), **f64)
+        self.e_nuc = torch.empty(B, **f64)
+        ns = s0.c2s.shape[0]
+        c2s = torch.empty((B, ns, n), **f64)
+        s = torch.empty((B, n, n), **f64)
+        for i, k in enumerate(members):
+            sysm = systems[k]
+            if (sysm.basis.ncgs, sysm.deck.nelectrons // 2, sysm.c2s.shape[0]) != (n, self.nocc, ns):
+                raise SCFError('a batch group holds molecules of one size')
+            c2s[i] = torch.tensor(sysm.c2s, **f64)
+            s[i] = torch.tensor(sysm.s_c[0], **f64)
+            self.h[i] = torch.tensor(sysm.t_c[0] + sysm.n_c[0], **f64)
+            self.hfx[i] = sysm.deck.hfexchange
+            self.e_nuc[i] = sysm.e_nuc
+            lindep = sysm.deck.lindep
+        # canonical orthogonalisation (LINDEP), one batched solver call; dropped
+        # directions become zero columns, marked in `pad`
+        e_s, v_s = torch.linalg.eigh(c2s @ s @ c2s.transpose(1, 2))
+        keep = e_s > lindep
+        if int(keep.sum(-1).min()) < self.nocc:
+            raise SCFError('fewer independent functions than occupied orbitals')
+        scale = torch.where(keep, 1.0 / torch.sqrt(e_s.clamp_min(lindep)), torch.zeros_like(e_s))
+        self.w[:, :, :ns] = c2s.transpose(1, 2) @ (v_s * scale[:, None, :])
+        self.ws = self.w.transpose(1, 2) @ s
+        self.pad[:, :ns] = ~keep
+        self.pad[:, ns:] = True
+        self.nd = 0   # DIIS history slots in use
+        self.slot = 0
+
+    def view(self, packed: torch.Tensor) -> torch.Tensor:
+        return packed[self.lo:self.hi].view(self.B, self.n, self.n)
+
+
+def sp2_projector(f: torch.Tensor, nocc: int, pad: torch.Tensor, tol: float = 1e-12, max_steps: int = 200,
+                  first_check: int = 12):
+    """Projector on the `nocc` lowest eigenvectors of each symmetric f [B, n, n]
+    (slots marked in `pad` [B, n] are decoupled and left empty), by SP2.
+
+    Gershgorin bounds [lo, hi] of the spectrum map f to X0 = (hi - f)/(hi - lo)
+    with eigenvalues in [0, 1], occupied ones nearest 1; each step replaces X by
+    X^2 or 2X - X^2, whichever brings tr X^2 closer to nocc, until the
+    idempotency defect tr(X - X^2) is below `tol` for every matrix (checked
+    after `first_check` steps and then every other step); returns (X, steps)."""
+    B, n, _ = f.shape
+    d = f.diagonal(dim1=-2, dim2=-1)
+    r = f.abs().sum(-1) - d.abs()
+    inf = torch.finfo(F64).max
+    lo = torch.where(pad, torch.full_like(d, inf), d - r).amin(-1)
+    hi = torch.where(pad, torch.full_like(d, -inf), d + r).amax(-1)
+    hi = torch.maximum(hi, lo + 1e-8)
+    eye = torch.eye(n, dtype=F64, device=f.device)
+    # padded slots sit at the top of the spectrum: X0 = 0 there, a fixed point
+    x = (hi[:, None, None] * eye - f - torch.diag_embed(torch.where(pad, hi[:, None] - d, torch.zeros_like(d)))) \
+        / (hi - lo)[:, None, None]
+    x = torch.where(pad[:, :, None] | pad[:, None, :], torch.zeros_like(x), x)
+    steps = 0
+    while True:
+        x2 = torch.bmm(x, x)
+        t1, t2 = _trace(x), _trace(x2)
+        steps += 1
+        up = (t2 - nocc).abs() < (2.0 * t1 - t2 - nocc).abs()
+        if steps >= first_check and steps % 2 == 0:
+            if float((t1 - t2).abs().max()) < tol:
+                return x, steps
+        if steps >= max_steps:
+            raise SCFError('SP2 projection did not converge')
+        x = torch.where(up[:, None, None], x2, 2.0 * x - x2)
+
+
+def _diis(group: _Group, hist_f: torch.Tensor, hist_e: torch.Tensor, valid: torch.Tensor) -> torch.Tensor:
+    """Pulay extrapolation per molecule over the valid history slots [B, D]."""
+    B, D = valid.shape
+    e = hist_e.view(B, D, -1)
+    g = torch.bmm(e, e.transpose(1, 2))
+    scale = g.diagonal(dim1=-2, dim2=-1).amax(-1).clamp_min(1e-300)
+    g = g / scale[:, None, None]
+    vm = valid.to(F64)
+    a = torch.zeros((B, D + 1, D + 1), dtype=F64, device=g.device)
+    a[:, :D, :D] = g * vm[:, :, None] * vm[:, None, :] + torch.diag_embed(1.0 - vm)
+    a[:, :D, :D] += torch.diag_embed(vm * 1e-14)
+    a[:, :D, D] = -vm
+    a[:, D, :D] = -vm
+    rhs = torch.zeros((B, D + 1, 1), dtype=F64, device=g.device)
+    rhs[:, D, 0] = -1.0
+    sol, info = torch.linalg.solve_ex(a, rhs)
+    c = sol[:, :D, 0] * vm
+    ok = (info == 0) & torch.isfinite(c).all(-1)
+    return torch.where(ok[:, None], c, vm * 0.0 + torch.nn.functional.one_hot(
+        torch.full((B,), group.slot, device=g.device, dtype=torch.long), D).to(F64))
+
+
+def _check_system(sysm: System) -> None:
+    d = sysm.deck
+    if sysm.ncell1 != 1:
+        raise SCFError('the batched SCF takes molecules only')
+    if d.temphf > 0.0 or d.nelectrons % 2:
+        raise SCFError('the batched SCF handles zero-temperature closed shells only')
+
+
+def _key(sysm: System):
+    return (sysm.basis.ncgs, sysm.deck.nelectrons // 2, sysm.c2s.shape[0])
+
+
+def sorted_order(systems: Sequence[System]) -> List[int]:
+    """The order the batch keeps molecules in: grouped by size (a DeviceBatch
+    passed to run_batch_scf must hold the systems in this order)."""
+    return sorted(range(len(systems)), key=lambda k: _key(systems[k]))
+
+
+def _projector_density(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions):
+    d, steps = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max)
+    return 2.0 * g.w @ d @ g.w.transpose(1, 2), steps
+
+
+def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None, device=0,
+                  max_cycles: Optional[int] = None, scfconv: Optional[float] = None,
+                  batch: Optional['fock_mod.DeviceBatch'] = None,
+                  log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True) -> BatchResult:
+    """RHF of every molecule of `systems` (zero temperature, closed shells) as one batch.
+
+    ``device``: a CUDA device index (the batch is then built here), or any torch
+    device together with a ``batch`` object offering the DeviceBatch interface
+    (``off``, ``systems``, ``view``, ``run_packed``, ``set_instance_screening``)."""
+    opts = opts or BatchOptions()
+    t0 = time.perf_counter()
+    dev = torch.device('cuda', device) if isinstance(device, int) else torch.device(device)
+    nmol = len(systems)
+    for s in systems:
+        _check_system(s)
+    order = sorted_order(systems)
+    ssys = [systems[k] for k in order]
+    fb = batch if batch is not None else fock_mod.DeviceBatch(ssys, dev.index or 0)
+    if len(fb) != nmol or any(a is not b for a, b in zip(fb.systems, ssys)):
+        raise SCFError('the DeviceBatch must hold the systems in sorted_order')
+    groups: List[_Group] = []
+    k = 0
+    while k < nmol:
+        k1 = k
+        while k1 < nmol and _key(ssys[k1]) == _key(ssys[k]):
+            k1 += 1
+        groups.append(_Group(list(range(k, k1)), ssys, fb.off[k], dev))
+        k = k1
+    conv = np.array([s.deck.scfconv if scfconv is None else scfconv for s in ssys])
+    ncycles = max_cycles or max(s.deck.scfcycles for s in ssys)
+    total = fb.off[-1]
+    f64 = dict(dtype=F64, device=dev)
+    p, p_ref, c_ref, x_ref = (torch.zeros(total, **f64) for _ in range(4))
+    dp, dc, dx, p_new = (torch.zeros(total, **f64) for _ in range(4))
+    learned = not isinstance(opts.guess, str)
+    sp2_steps = 0
+
+    def nuclear(kk: int) -> torch.Tensor:
+        return torch.tensor(guess_density(ssys[kk])[0], **f64)
+
+    # ---- initial densities
+    if opts.guess == 'nuclear':
+        for kk in range(nmol):
+            fb.view(p, kk).copy_(nuclear(kk))
+    elif opts.guess == 'core':
+        for g in groups:
+            pv, st = _projector_density(g, g.w.transpose(1, 2) @ g.h @ g.w, opts)
+            g.view(p).copy_(pv)
+            sp2_steps += st
+    elif learned:
+        # occupied natural orbitals of the predicted density: the projector on the
+        # nocc lowest eigenvectors of -D, D = P/2 in the orthonormal basis
+        for kk in range(nmol):
+            fb.view(p, kk).copy_(torch.tensor(np.asarray(opts.guess.raw(ssys[kk])), **f64))
+        for g in groups:
+            dm = 0.5 * g.ws @ g.view(p) @ g.ws.transpose(1, 2)
+            pv, st = _projector_density(g, -0.5 * (dm + dm.transpose(1, 2)), opts)
+            g.view(p).copy_(pv)
+            sp2_steps += st
+    else:
+        raise SCFError('unknown guess %r' % (opts.guess,))
+
+    D = max(1, opts.ndiis)
+    for g in groups:
+        g.hist_f = torch.zeros((g.B, D, g.n, g.n), **f64)
+        g.hist_e = torch.zeros((g.B, D, g.n, g.n), **f64)
+        g.valid = torch.zeros((g.B, D), dtype=torch.bool, device=dev)
+        g.slot = 0
+    state = np.full(nmol, _FULL)
+    nbuild = np.zeros(nmol, dtype=int)
+    have_ref = np.zeros(nmol, dtype=bool)
+    final_pending = np.zeros(nmol, dtype=bool)
+    done = np.zeros(nmol, dtype=bool)
+    converged = np.zeros(nmol, dtype=bool)
+    first = np.ones(nmol, dtype=bool)
+    fallback = np.zeros(nmol, dtype=bool)
+    first_err = np.zeros(nmol)
+    energy = np.zeros(nmol)
+    iters = np.zeros(nmol, dtype=int)
+    screen = [None] * nmol
+    builds = 0
+    for it in range(1, ncycles + 1):
+        # ---- per-molecule build mode and screening
+        for kk in range(nmol):
+            if done[kk]:
+                st, sc = _DONE, (0.0, max(opts.density_tol, 1e-300))
+            elif final_pending[kk]:
+                st, sc = _FINAL, (0.0, 0.0)
+            elif not have_ref[kk] or not opts.incremental or nbuild[kk] % max(1, opts.reset_every) == 0:
+                st, sc = _FULL, (opts.mixed_cutoff, 0.0)
+            else:
+                st, sc = _INCR, (opts.mixed_cutoff, opts.density_tol)
+            state[kk] = st
+            if screen[kk] != sc:
+                fb.set_instance_screening(kk, *sc)
+                screen[kk] = sc
+        incr = torch.tensor((state == _INCR) | (state == _DONE), **f64)
+        live = torch.tensor(state != _DONE, **f64)
+        for g in groups:
+            sl = slice(g.members[0], g.members[-1] + 1)
+            im, lm = incr[sl][:, None, None], live[sl][:, None, None]
+            g.view(dp).copy_((g.view(p) - g.view(p_ref) * im) * lm)
+        fb.run_packed(dp, dc, dx)
+        builds += 1
+        nbuild[~done] += 1
+        stats = []
+        for g in groups:
+            sl = slice(g.members[0], g.members[-1] + 1)
+            im = incr[sl][:, None, None]
+            cv = g.view(dc) + g.view(c_ref) * im
+            xv = g.view(dx) + g.view(x_ref) * im
+            g.view(c_ref).copy_(cv)
+            g.view(x_ref).copy_(xv)
+            pv = g.view(p)
+            g.view(p_ref).copy_(pv)
+            f = g.h + cv - 0.5 * g.hfx * xv
+            f = 0.5 * (f + f.transpose(1, 2))
+            fo = g.w.transpose(1, 2) @ f @ g.w
+            po = g.ws @ pv @ g.ws.transpose(1, 2)
+            err = fo @ po - po @ fo
+            e = (pv * (g.h + 0.5 * cv - 0.25 * g.hfx * xv)).sum((1, 2)) + g.e_nuc
+            fe = err.abs().amax((1, 2))
+            g.hist_f[:, g.slot] = fo
+            g.hist_e[:, g.slot] = err
+            g.valid[:, g.slot] = True
+            c = _diis(g, g.hist_f, g.hist_e, g.valid)
+            fx = torch.einsum('bd,bdij->bij', c, g.hist_f)
+            pn, st = _projector_density(g, fx, opts)
+            sp2_steps += st
+            g.view(p_new).copy_(pn)
+            dchg = torch.sqrt(((pn - pv) ** 2).sum((1, 2)) / float(g.n * g.n))
+            stats.append(torch.stack([e, fe, dchg], 1))
+            g.slot = (g.slot + 1) % D
+        host = torch.cat(stats).cpu().numpy()
+        take = np.zeros(nmol, dtype=bool)
+        restart = []
+        for kk in range(nmol):
+            if done[kk]:
+                continue
+            e_k, fe_k, dchg_k = host[kk]
+            iters[kk] = it
+            have_ref[kk] = True
+            if first[kk]:
+                first[kk] = False
+                first_err[kk] = fe_k
+                if learned and fe_k > opts.fallback_error:
+                    fallback[kk] = True
+                    restart.append(kk)
+                    continue
+            if final_pending[kk] and dchg_k < conv[kk]:
+                converged[kk] = done[kk] = True
+                energy[kk] = e_k
+                continue
+            final_pending[kk] = dchg_k < conv[kk]
+            take[kk] = True
+        tk = torch.tensor(take, device=dev)
+        for g in groups:
+            sl = slice(g.members[0], g.members[-1] + 1)
+            g.view(p).copy_(torch.where(tk[sl][:, None, None], g.view(p_new), g.view(p)))
+        for kk in restart:
+            # the learned guess is judged by the plain one: restart from the nuclear-charge guess
+            fb.view(p, kk).copy_(nuclear(kk))
+            have_ref[kk] = False
+            nbuild[kk] = 0
+            for g in groups:
+                if g.members[0] <= kk <= g.members[-1]:
+                    g.valid[kk - g.members[0]] = False
+        if log:
+            nd = int(done.sum())
+            log('%3d  done %4d/%d  max DIIS error %.3e  max dP %.3e' % (
+                it, nd, nmol, float(host[~done, 1].max()) if nd < nmol else 0.0,
+                float(host[~done, 2].max()) if nd < nmol else 0.0))
+        if done.all():
+            break
+    if dev.type == 'cuda':
+        torch.cuda.synchronize(dev)
+    if not converged.all() and raise_on_fail:
+        raise SCFError('SCF CONVERGENCE NOT MET for %d of %d molecules' % (int((~converged).sum()), nmol))
+    inv = np.empty(nmol, dtype=int)
+    inv[np.array(order)] = np.arange(nmol)
+    p_out = [fb.view(p, int(inv[k])).t().clone() for k in range(nmol)]
+    res = BatchResult(energy[inv], converged[inv], iters[inv], builds, time.perf_counter() - t0, first_err[inv],
+                      fallback[inv], p_out, sp2_steps)
+    if batch is None:
+        fb.close()
+    return res

@@ -204,6 +204,12 @@ class DeviceBatch:
         mode = capi.PFE_PREC_MIXED if mixed_cutoff > 0.0 else capi.PFE_PREC_FP64
         check(self.L, self.L.pfe_batch_set_screening(self.handle, mode, float(mixed_cutoff), float(density_tol)))
 
+    def set_instance_screening(self, k: int, mixed_cutoff: float = 0.0, density_tol: float = 0.0) -> None:
+        """Screening of molecule k alone (its launch record is rebuilt at the next build)."""
+        mode = capi.PFE_PREC_MIXED if mixed_cutoff > 0.0 else capi.PFE_PREC_FP64
+        check(self.L, self.L.pfe_batch_set_instance_screening(self.handle, int(k), mode, float(mixed_cutoff),
+                                                              float(density_tol)))
+
     def view(self, packed: torch.Tensor, k: int) -> torch.Tensor:
         """Molecule k's matrix of a packed buffer (a transposed view: row-major indices)."""
         n = self.ncgs[k]

@@ -144,3 +144,11 @@ def polyethylene_deck(basis: str = '6-31G', cutoff1: int = 5, cutoff2: int = 10,
     opts.setdefault('inttol', 1.0e-10)
     return make_deck(atoms, xyz / ANG_BOHR, basis, period=(0.0, 0.0, period / ANG_BOHR), helix_deg=180.0,
                      kpoints=(0, 0, kpoints), cutoff1=cutoff1, cutoff2=cutoff2, **opts)
+
+
+def water_batch_decks(n: int = 256, seed: int = 2000, kmax: int = 16, basis: str = 'cc-pVDZ',
+                      **opts) -> List[Deck]:
+    """The batch workload of uneven water clusters: sizes k ~ U{1..kmax} drawn
+    from default_rng(seed), cluster i generated from default_rng(seed + 1 + i)."""
+    ks = np.random.default_rng(seed).integers(1, kmax + 1, size=n)
+    return [water_deck(int(k), seed=seed + 1 + i, basis=basis, **opts) for i, k in enumerate(ks)]
