@@ -14,8 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 OUT = os.path.join(HERE, '_build')
 LIB = os.path.join(OUT, 'libpolymer_fock.so')
-SOURCES = ['pfe_api.cu', 'pfe_eri.cu', 'pfe_mol.cu', 'pfe_mol_mixed.cu', 'pfe_mol_big1.cu', 'pfe_mol_big2.cu',
-           'pfe_mol_big3.cu', 'pfe_mol_big4.cu', 'pfe_lattice.cu', 'pfe_onee.cu',
+# the largest units first: the pool starts them before the small ones
+SOURCES = ['pfe_mol_big2.cu', 'pfe_mol_big6.cu', 'pfe_mol_big4.cu', 'pfe_mol_big8.cu', 'pfe_mol_big3.cu',
+           'pfe_mol_big7.cu', 'pfe_mol_big1.cu', 'pfe_mol_big5.cu', 'pfe_mol.cu', 'pfe_mol_batch.cu',
+           'pfe_mol_mixed.cu', 'pfe_mol_batch_mixed.cu', 'pfe_api.cu', 'pfe_eri.cu', 'pfe_lattice.cu', 'pfe_onee.cu',
            'pfe_mlp.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
@@ -41,25 +43,38 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     """Compile every CUDA source and link the shared library; returns its path."""
     generate()
     os.makedirs(OUT, exist_ok=True)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(('.cu', '.cuh'))]
-    deps += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
-             os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h'),
-             os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h')]
-    newest = max(os.path.getmtime(d) for d in deps if os.path.exists(d))
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= newest and not ptxas_info:
+    # every unit depends on every header (conservative); a unit is rebuilt when
+    # its source or a header is newer than its object
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')]
+    headers += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
+                os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h'),
+                os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h')]
+    newest_header = max(os.path.getmtime(d) for d in headers if os.path.exists(d))
+    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+
+    def stale(src):
+        obj = os.path.join(OUT, src.replace('.cu', '.o'))
+        return ptxas_info or not os.path.exists(obj) or \
+            os.path.getmtime(obj) < max(newest_header, os.path.getmtime(os.path.join(CSRC, src)))
+
+    todo = [s for s in srcs if stale(s)]
+    if os.path.exists(LIB) and not todo and \
+            os.path.getmtime(LIB) >= max(os.path.getmtime(os.path.join(OUT, s.replace('.cu', '.o'))) for s in srcs):
         return LIB
 
     def compile_one(src):
         obj = os.path.join(OUT, src.replace('.cu', '.o'))
+        if src not in todo:
+            return obj
         cmd = [NVCC] + ARCH + FLAGS + (['-Xptxas', '-v'] if ptxas_info else []) + \
-            ['-c', os.path.join(CSRC, src), '-o', obj]
+            ['-c', os.path.join(CSRC, src), '-o', obj + '.tmp']
         log = _run(cmd)
+        os.replace(obj + '.tmp', obj)
         if ptxas_info:
             with open(os.path.join(OUT, src.replace('.cu', '.ptxas.txt')), 'w') as fh:
                 fh.write(log)
         return obj
 
-    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     with cf.ThreadPoolExecutor(max_workers=len(srcs)) as ex:
         objs = list(ex.map(compile_one, srcs))
     tmp = LIB + '.tmp'

@@ -410,6 +410,8 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
   const PairArrays pr = ql.pairs;
   const int nt = ql.nt;
   const double* __restrict__ D = ql.dt;
+  const double* __restrict__ scoef = ql.scoef;   // held in registers (ql may live in global memory)
+  const double* __restrict__ boys = ql.boys;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const int base = LT + 2;
   const int G = ch.x;
@@ -454,7 +456,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       if (sp * hmax < thr) break;
       const int I = pr.si[p], J = pr.sj[p];
       for (int t = tid; t < NA * NB; t += team)
-        cab[t] = ql.scoef[I * MAXCOMP + t / NB] * ql.scoef[J * MAXCOMP + t % NB];
+        cab[t] = scoef[I * MAXCOMP + t / NB] * scoef[J * MAXCOMP + t % NB];
       const double zb = pr.zeta[p];
       const double Px = pr.P[0][p], Py = pr.P[1][p], Pz = pr.P[2][p];
       const int qe = (G == H) ? p + 1 : h0 + hn;
@@ -468,7 +470,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
           const double T = rho * ((Px - Qx) * (Px - Qx) + (Py - Qy) * (Py - Qy) + (Pz - Qz) * (Pz - Qz));
           const double pref = c2pi * pr.S[p] * pr.S[q] * sqrt(rho);
           double F[LT + 1];
-          boys_tab<LT>(T, pref, ql.boys, F);
+          boys_tab<LT>(T, pref, boys, F);
           v[0] = 0.0;
 #pragma unroll
           for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
@@ -484,7 +486,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
           set_geom(geo, PA, WP, QC, WQ, AB, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
         }
         for (int t = tid; t < NCD; t += team)
-          ccd[t] = ql.scoef[K * MAXCOMP + t / ND] * ql.scoef[L * MAXCOMP + t % ND];
+          ccd[t] = scoef[K * MAXCOMP + t / ND] * scoef[L * MAXCOMP + t % ND];
         sync();
         for (int l = 0; l < tab.nlevels; ++l) {
           const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
@@ -542,12 +544,22 @@ __global__ void __launch_bounds__(256) k_gq_block(MolLaunch ql, OpTableDev tab, 
                                   s_geo, s_prm, s_w, threadIdx.x, blockDim.x);
 }
 
-// FP64 straight-line launchers here; the mixed-precision ones in pfe_mol_mixed.cu
+// FP64 straight-line launchers here; the mixed-precision ones in pfe_mol_mixed.cu,
+// those of batches (launch records per chunk) in pfe_mol_batch*.cu
 LaunchFn straight_launcher_mixed(int cb, int ck);
+LaunchFn straight_launcher_batch(int cb, int ck);
+LaunchFn straight_launcher_batch_mixed(int cb, int ck);
 
 // (classes without a mixed instantiation run their FP64 straight-line kernels)
-static LaunchFn straight_launcher(int cb, int ck, bool mixed = false) {
-  LaunchFn f = mixed ? straight_launcher_mixed(cb, ck) : nullptr;
+static LaunchFn straight_launcher(int cb, int ck, bool mixed = false, bool batch = false) {
+  LaunchFn f = nullptr;
+  if (batch) {
+    f = mixed ? straight_launcher_batch_mixed(cb, ck) : nullptr;
+    if (!f) f = straight_launcher_batch(cb, ck);
+    if (!f) f = straight_launcher_big(cb, ck, true);
+    return f;
+  }
+  f = mixed ? straight_launcher_mixed(cb, ck) : nullptr;
   if (!f) f = straight_launcher_t<false>(cb, ck);
   if (!f) f = straight_launcher_big(cb, ck);
   return f;
@@ -907,7 +919,7 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
   if ((variant == 0 && cl.has_straight) || !cl.has_table) {
     const int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
-    straight_launcher(cl.cb, cl.ck, mixed)(ql, std::max(grid, 1), s);
+    straight_launcher(cl.cb, cl.ck, mixed, ql.insts != nullptr)(ql, std::max(grid, 1), s);
     return;
   }
   OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};

@@ -6,6 +6,6 @@
 
 namespace pfe {
 
-template void launch_q<2, 1, 2, 1, 40, false>(const MolLaunch&, int, cudaStream_t);
+template void launch_q<2, 1, 2, 1, 40, false, false>(const MolLaunch&, int, cudaStream_t);
 
 }  // namespace pfe

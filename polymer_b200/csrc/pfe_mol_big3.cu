@@ -6,6 +6,6 @@
 
 namespace pfe {
 
-template void launch_q<2, 2, 2, 0, 25, false>(const MolLaunch&, int, cudaStream_t);
+template void launch_q<2, 2, 2, 0, 25, false, false>(const MolLaunch&, int, cudaStream_t);
 
 }  // namespace pfe

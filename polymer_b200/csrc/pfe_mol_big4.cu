@@ -6,6 +6,6 @@
 
 namespace pfe {
 
-template void launch_q<2, 2, 1, 1, 50, false>(const MolLaunch&, int, cudaStream_t);
+template void launch_q<2, 2, 1, 1, 50, false, false>(const MolLaunch&, int, cudaStream_t);
 
 }  // namespace pfe

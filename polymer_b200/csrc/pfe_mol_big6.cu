@@ -1,0 +1,10 @@
+// Batch instantiation (launch record per chunk) of the large FP64 register-pass
+// class (21|21); dispatch in pfe_mol_big1.cu.
+
+#include "pfe_mol_kernels.cuh"
+
+namespace pfe {
+
+template void launch_q<2, 1, 2, 1, 40, false, true>(const MolLaunch&, int, cudaStream_t);
+
+}  // namespace pfe

@@ -174,7 +174,7 @@ struct GqOccupancy {
   static constexpr int blocks = (NI <= 16 && LA + LB + LC + LD <= 2) ? 4 : 1;
 };
 
-template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch lq) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
   constexpr int NI = NA * NB * NC * ND;
@@ -197,18 +197,28 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   const double c2pi = 2.0 / sqrt(REF_PI);
   for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * lq.numprocs + lq.myid; c < nchunks; c += stride) {
     const int4 ch = lq.chunks[c];
-    const MolLaunch& ql = lq.insts ? lq.insts[ch.w] : lq;   // this chunk's instance
+    // this chunk's instance: batches read its launch record from global memory
+    const MolLaunch& ql = [&]() -> const MolLaunch& {
+      if constexpr (BATCH) return lq.insts[ch.w];
+      else return lq;
+    }();
+    // the tables the loops read, held in registers (ql may live in global memory)
+    const PairRec* __restrict__ rec = ql.rec;
+    const double* __restrict__ scoef = ql.scoef;
+    const double* __restrict__ boys = ql.boys;
+    const int* __restrict__ stidx = ql.stidx;
+    const double mcut = ql.mcut;
     const int nt = ql.nt;
     const int G = ch.x;
     const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
-    const int2 ijg = __ldg(reinterpret_cast<const int2*>(&ql.rec[g0].si));
+    const int2 ijg = __ldg(reinterpret_cast<const int2*>(&rec[g0].si));
     if constexpr (NPASS > 1) {
       // a pass whose bra components all lack a coefficient (the lower components of a
       // pure d or p shell) contributes nothing: skip the chunk (warp-uniform)
       bool live = false;
 #pragma unroll
       for (int k = AB0; k < AB1; ++k)
-        live = live || (ql.stidx[ijg.x * MAXCOMP + ORD.ab[k] / NB] >= 0 && ql.stidx[ijg.y * MAXCOMP + ORD.ab[k] % NB] >= 0);
+        live = live || (stidx[ijg.x * MAXCOMP + ORD.ab[k] / NB] >= 0 && stidx[ijg.y * MAXCOMP + ORD.ab[k] % NB] >= 0);
       if (!live) continue;
     }
     const int li = ch.y + lane;
@@ -217,7 +227,7 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
     const double hmax = act ? ql.gr_max[H] : 0.0;
     const bool dens = ql.dtol > 0.0 || ql.mcut > 0.0;
-    const int2 klh = __ldg(reinterpret_cast<const int2*>(&ql.rec[h0].si));
+    const int2 klh = __ldg(reinterpret_cast<const int2*>(&rec[h0].si));
     const double pmax = dens ? quartet_pmax(ql, ijg.x, ijg.y, klh.x, klh.y) : 0.0;
     const double thr = quartet_threshold(ql, pmax);
     unsigned n32 = 0;
@@ -226,23 +236,23 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
 #pragma unroll
     for (int i = 0; i < XN; ++i) X[i] = 0.0;
     for (int p = g0; p < g0 + gn; ++p) {
-      const double sp = pair_bound(ql.rec, p);
+      const double sp = pair_bound(rec, p);
       if (!__any_sync(0xffffffffu, act && sp * hmax >= thr)) break;   // later bra pairs fail for every lane
-      const PairView bp = load_pair(ql.rec, p);
+      const PairView bp = load_pair(rec, p);
       const int I = bp.si, J = bp.sj;
       double cab[NAB];
 #pragma unroll
       for (int k = AB0; k < AB1; ++k)
-        cab[ORD.ab[k]] = ql.scoef[I * MAXCOMP + ORD.ab[k] / NB] * ql.scoef[J * MAXCOMP + ORD.ab[k] % NB];
+        cab[ORD.ab[k]] = scoef[I * MAXCOMP + ORD.ab[k] / NB] * scoef[J * MAXCOMP + ORD.ab[k] % NB];
       const double zb = bp.zeta;
       const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
       const double Sp = bp.S;
       const double wIJ = (I != J) ? 2.0 : 1.0;
       const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
       for (int q = h0; q < qe; ++q) {
-        const double sq = pair_bound(ql.rec, q);
+        const double sq = pair_bound(rec, q);
         if (sp * sq < thr) break;   // the reference's screen (thr = INTTOL); pairs sorted by bound
-        const PairView kq = load_pair(ql.rec, q);
+        const PairView kq = load_pair(rec, q);
         const double ze = kq.zeta;
         const double Qx = kq.P[0], Qy = kq.P[1], Qz = kq.P[2];
         const double zz = zb + ze;
@@ -252,10 +262,10 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
         const double pref = c2pi * Sp * kq.S * sqrt(rho);
         // FP32 only when every lane running this step qualifies
         bool f32 = false;
-        if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < ql.mcut);
+        if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < mcut);
         n32 += f32 ? 1u : 0u;
         double F[LT + 1];
-        boys_tab<LT>(T, f32 ? 1.0 : pref, ql.boys, F);
+        boys_tab<LT>(T, f32 ? 1.0 : pref, boys, F);
         double out[NI];
         if constexpr (LT == 0) {
           out[0] = F[0];
@@ -282,9 +292,9 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
         double ccd[NCD];
 #pragma unroll
         for (int cc = 0; cc < NC; ++cc) {
-          const double c1 = w * ql.scoef[K * MAXCOMP + cc];
+          const double c1 = w * scoef[K * MAXCOMP + cc];
 #pragma unroll
-          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * ql.scoef[L * MAXCOMP + d];
+          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * scoef[L * MAXCOMP + d];
         }
 #pragma unroll
         for (int k = AB0; k < AB1; ++k)
@@ -306,13 +316,13 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     const int I0 = ijg.x, J0 = ijg.y, K0 = klh.x, L0 = klh.y;
     int ta[NA], tb[NB], tc[NC], td[ND];
 #pragma unroll
-    for (int x = 0; x < NA; ++x) ta[x] = ql.stidx[I0 * MAXCOMP + x];
+    for (int x = 0; x < NA; ++x) ta[x] = stidx[I0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < NB; ++x) tb[x] = ql.stidx[J0 * MAXCOMP + x];
+    for (int x = 0; x < NB; ++x) tb[x] = stidx[J0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < NC; ++x) tc[x] = ql.stidx[K0 * MAXCOMP + x];
+    for (int x = 0; x < NC; ++x) tc[x] = stidx[K0 * MAXCOMP + x];
 #pragma unroll
-    for (int x = 0; x < ND; ++x) td[x] = ql.stidx[L0 * MAXCOMP + x];
+    for (int x = 0; x < ND; ++x) td[x] = stidx[L0 * MAXCOMP + x];
     // J'(ab) += 1/4 sum_cd P(cd) X: the bra is the warp's, reduce over lanes first
 #pragma unroll
     for (int k = AB0; k < AB1; ++k) {
@@ -400,17 +410,17 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
 
 using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
 
-template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED>
+template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 struct Passes {
   static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
-    k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED><<<grid, 128, 0, s>>>(ql);
-    if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1, MIXED>::run(ql, grid, s);
+    k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED, BATCH><<<grid, 128, 0, s>>>(ql);
+    if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1, MIXED, BATCH>::run(ql, grid, s);
   }
 };
 
-template <int LA, int LB, int LC, int LD, int NPASS, bool MIXED>
+template <int LA, int LB, int LC, int LD, int NPASS, bool MIXED, bool BATCH = false>
 void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
-  Passes<LA, LB, LC, LD, NPASS, 0, MIXED>::run(ql, grid, s);
+  Passes<LA, LB, LC, LD, NPASS, 0, MIXED, BATCH>::run(ql, grid, s);
 }
 
 // Launches per straight-line class (its passes); must match the table below.
@@ -421,9 +431,9 @@ static inline int straight_npass(int cb, int ck) {
 }
 
 // straight-line classes and their passes (X of at most 40 integrals per pass)
-template <bool MIXED>
+template <bool MIXED, bool BATCH = false>
 static LaunchFn straight_launcher_t(int cb, int ck) {
-#define Q(A, B, C, D, P) &launch_q<A, B, C, D, P, MIXED>
+#define Q(A, B, C, D, P) &launch_q<A, B, C, D, P, MIXED, BATCH>
   static const LaunchFn table[6][6] = {
       {Q(0, 0, 0, 0, 1), nullptr, nullptr, nullptr, nullptr, nullptr},
       {Q(1, 0, 0, 0, 1), Q(1, 0, 1, 0, 1), nullptr, nullptr, nullptr, nullptr},
@@ -436,7 +446,7 @@ static LaunchFn straight_launcher_t(int cb, int ck) {
 }
 
 // The large classes' FP64 passes, one translation unit each (pfe_mol_big*.cu)
-// so that they compile in parallel.
-LaunchFn straight_launcher_big(int cb, int ck);
+// so that they compile in parallel; `batch`: the instantiations for batches.
+LaunchFn straight_launcher_big(int cb, int ck, bool batch = false);
 
 }  // namespace pfe
