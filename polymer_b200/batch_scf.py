@@ -34,7 +34,7 @@ import numpy as np
 import torch
 
 from . import fock as fock_mod
-from .scf import SCFError, guess_density
+from .scf import SCFError, guess_density, incremental_tol
 from .system import System
 
 F64 = torch.float64
@@ -45,13 +45,16 @@ _FULL, _INCR, _FINAL, _DONE = 0, 1, 2, 3
 
 @dataclasses.dataclass
 class BatchOptions:
-    """incremental / density_tol / mixed_cutoff / reset_every as in scf.FastOptions;
+    """incremental / density_tol(_rel, _max) / mixed_cutoff / reset_every as in
+    scf.FastOptions (per molecule, from its own density change);
     guess: 'nuclear' (the reference's GUESS_DENSITYMATRIX), 'core', or an object
     with ``raw(sysm) -> np.ndarray`` giving an unpurified contracted density per
     molecule (the learned guess), purified here on the GPU and judged by
     ``fallback_error`` (first DIIS error above it: restart from 'nuclear')."""
     incremental: bool = True
     density_tol: float = 1e-11
+    density_tol_rel: float = 1e-4
+    density_tol_max: float = 1e-8
     mixed_cutoff: float = 0.0
     reset_every: int = 8
     guess: object = 'nuclear'
@@ -72,6 +75,7 @@ class BatchResult:
     fallback: np.ndarray        # the learned guess was rejected
     p_c: List[torch.Tensor]     # converged contracted densities, input order
     sp2_steps: int              # SP2 products over the run (per group, summed)
+    phases: Optional[dict] = None   # seconds per phase (guess, build, update) when profiled
 
 
 def _trace(x: torch.Tensor) -> torch.Tensor:
@@ -204,14 +208,18 @@ def sorted_order(systems: Sequence[System]) -> List[int]:
 
 
 def _projector_density(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions):
-    d, steps = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max)
+    # the idempotency test starts a little before the step count the group needed last time
+    d, steps = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max,
+                             first_check=max(8, getattr(g, 'sp2_last', 0) - 2))
+    g.sp2_last = steps
     return 2.0 * g.w @ d @ g.w.transpose(1, 2), steps
 
 
 def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None, device=0,
                   max_cycles: Optional[int] = None, scfconv: Optional[float] = None,
                   batch: Optional['fock_mod.DeviceBatch'] = None,
-                  log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True) -> BatchResult:
+                  log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True,
+                  profile: bool = False) -> BatchResult:
     """RHF of every molecule of `systems` (zero temperature, closed shells) as one batch.
 
     ``device``: a CUDA device index (the batch is then built here), or any torch
@@ -244,6 +252,19 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     dp, dc, dx, p_new = (torch.zeros(total, **f64) for _ in range(4))
     learned = not isinstance(opts.guess, str)
     sp2_steps = 0
+    phases = {'setup': 0.0, 'guess': 0.0, 'build': 0.0, 'update': 0.0, 'host': 0.0}
+    tmark = [time.perf_counter()]
+
+    def mark(name):
+        # with `profile`, wall time per phase (the device is synchronised at each mark)
+        if profile:
+            if dev.type == 'cuda':
+                torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            phases[name] += t - tmark[0]
+            tmark[0] = t
+
+    mark('setup')
 
     def nuclear(kk: int) -> torch.Tensor:
         return torch.tensor(guess_density(ssys[kk])[0], **f64)
@@ -270,6 +291,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     else:
         raise SCFError('unknown guess %r' % (opts.guess,))
 
+    mark('guess')
     D = max(1, opts.ndiis)
     for g in groups:
         g.hist_f = torch.zeros((g.B, D, g.n, g.n), **f64)
@@ -287,6 +309,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     first_err = np.zeros(nmol)
     energy = np.zeros(nmol)
     iters = np.zeros(nmol, dtype=int)
+    last_change = np.full(nmol, np.inf)
     screen = [None] * nmol
     builds = 0
     for it in range(1, ncycles + 1):
@@ -299,7 +322,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             elif not have_ref[kk] or not opts.incremental or nbuild[kk] % max(1, opts.reset_every) == 0:
                 st, sc = _FULL, (opts.mixed_cutoff, 0.0)
             else:
-                st, sc = _INCR, (opts.mixed_cutoff, opts.density_tol)
+                st, sc = _INCR, (opts.mixed_cutoff, incremental_tol(opts, float(last_change[kk])))
             state[kk] = st
             if screen[kk] != sc:
                 fb.set_instance_screening(kk, *sc)
@@ -310,7 +333,9 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             sl = slice(g.members[0], g.members[-1] + 1)
             im, lm = incr[sl][:, None, None], live[sl][:, None, None]
             g.view(dp).copy_((g.view(p) - g.view(p_ref) * im) * lm)
+        mark('host')
         fb.run_packed(dp, dc, dx)
+        mark('build')
         builds += 1
         nbuild[~done] += 1
         stats = []
@@ -342,6 +367,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             stats.append(torch.stack([e, fe, dchg], 1))
             g.slot = (g.slot + 1) % D
         host = torch.cat(stats).cpu().numpy()
+        mark('update')
         take = np.zeros(nmol, dtype=bool)
         restart = []
         for kk in range(nmol):
@@ -349,6 +375,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 continue
             e_k, fe_k, dchg_k = host[kk]
             iters[kk] = it
+            last_change[kk] = dchg_k
             have_ref[kk] = True
             if first[kk]:
                 first[kk] = False
@@ -372,6 +399,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             fb.view(p, kk).copy_(nuclear(kk))
             have_ref[kk] = False
             nbuild[kk] = 0
+            last_change[kk] = np.inf
             for g in groups:
                 if g.members[0] <= kk <= g.members[-1]:
                     g.valid[kk - g.members[0]] = False
@@ -390,7 +418,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     inv[np.array(order)] = np.arange(nmol)
     p_out = [fb.view(p, int(inv[k])).t().clone() for k in range(nmol)]
     res = BatchResult(energy[inv], converged[inv], iters[inv], builds, time.perf_counter() - t0, first_err[inv],
-                      fallback[inv], p_out, sp2_steps)
+                      fallback[inv], p_out, sp2_steps, phases if profile else None)
     if batch is None:
         fb.close()
     return res

@@ -303,6 +303,11 @@ class LearnedGuess:
             out.append(self.net.forward(torch.tensor(x[i:i + 4096], dtype=torch.float32)).double().cpu().numpy())
         return np.concatenate(out)
 
+    def raw(self, sysm: System) -> np.ndarray:
+        """The assembled (unpurified) contracted density of the prediction."""
+        info, frames, pairs, x = cluster_data(sysm)
+        return assemble(sysm, info, frames, pairs, self.predict_blocks(x))
+
     def __call__(self, sysm: System, st) -> torch.Tensor:
         info, frames, pairs, x = cluster_data(sysm)
         p = assemble(sysm, info, frames, pairs, self.predict_blocks(x))

@@ -137,6 +137,10 @@ class FastOptions:
       rebuild every ``reset_every`` builds;
     density_tol: skip quartets with Schwarz*Schwarz*max|dP| below it in the
       incremental builds;
+    density_tol_rel: when positive, the incremental builds' tolerance follows
+      the RMS density change d of the previous iteration:
+      min(max(density_tol, density_tol_rel * d), density_tol_max) -- loose
+      while the density still moves, density_tol near convergence;
     mixed_cutoff: FP32 recursion where Schwarz*Schwarz*max|P| is below it;
     guess: 'nuclear' (the reference's), 'core', or a callable(System, HostState)
       returning a cell-major P_C tensor;
@@ -147,11 +151,21 @@ class FastOptions:
     """
     incremental: bool = True
     density_tol: float = 1e-11
+    density_tol_rel: float = 1e-4
+    density_tol_max: float = 1e-8
     mixed_cutoff: float = 0.0
     reset_every: int = 8
     guess: object = 'nuclear'
     final_full: bool = True
     fallback_error: float = 0.5   # a learned guess whose first commutator error exceeds it is replaced
+
+
+def incremental_tol(opts: FastOptions, last_change: float) -> float:
+    """Density tolerance of an incremental build after an iteration whose RMS
+    density change was `last_change` (see FastOptions.density_tol_rel)."""
+    if opts.density_tol_rel <= 0.0 or not math.isfinite(last_change):
+        return opts.density_tol
+    return min(max(opts.density_tol, opts.density_tol_rel * last_change), max(opts.density_tol_max, opts.density_tol))
 
 
 def decontract(st: HostState, p_c: torch.Tensor) -> torch.Tensor:
@@ -490,6 +504,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
     fock_s = 0.0
     e = 0.0
     eps = None
+    last_change = math.inf
     for iscf in range(1, ncycles + 1):
         ti = time.perf_counter()
         full = final_pending or ref is None or not opts.incremental or nbuild % max(1, opts.reset_every) == 0
@@ -498,7 +513,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
             fock.set_screening(mixed_cutoff=0.0 if final_pending else opts.mixed_cutoff)
             c_c, x_c = fock.from_pc(p_c)
         else:
-            fock.set_screening(mixed_cutoff=opts.mixed_cutoff, density_tol=opts.density_tol)
+            fock.set_screening(mixed_cutoff=opts.mixed_cutoff, density_tol=incremental_tol(opts, last_change))
             dc, dx = fock.from_pc(p_c - ref[0])
             c_c, x_c = ref[1] + dc, ref[2] + dx
         fock.set_screening()
@@ -554,6 +569,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
         eps = torch.full((1, sysm.basis.ncgs), 1.0e99, dtype=torch.float64, device=st.device)
         eps[0, :eo.shape[0]] = eo
         dchg = math.sqrt(float(((p_new - p_c) ** 2).sum()) / denom)
+        last_change = dchg
         it = SCFIteration(iscf, m if m >= 2 else 0, fe, dchg, e, float(eo[nocc - 1]), time.perf_counter() - ti)
         iters.append(it)
         if log:
