@@ -21,7 +21,8 @@ SOURCES = ['pfe_mol_big2.cu', 'pfe_mol_big6.cu', 'pfe_mol_big4.cu', 'pfe_mol_big
            'pfe_mlp.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
-FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550']
+FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550'] + \
+    os.environ.get('PFE_NVCC_FLAGS', '').split()
 
 
 def _run(cmd):

@@ -171,7 +171,11 @@ struct AbOrder {
 template <int LA, int LB, int LC, int LD>
 struct GqOccupancy {
   static constexpr int NI = ncum(LA) * ncum(LB) * ncum(LC) * ncum(LD);
+#ifdef PFE_GQ_MINB
+  static constexpr int blocks = (NI <= 16 && LA + LB + LC + LD <= 2) ? 4 : PFE_GQ_MINB;
+#else
   static constexpr int blocks = (NI <= 16 && LA + LB + LC + LD <= 2) ? 4 : 1;
+#endif
 };
 
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
@@ -225,7 +229,6 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     const bool act = li < ch.z;
     const int H = ql.bk_list[act ? li : ch.y];
     const int h0 = ql.gr_start[H], hn = act ? ql.gr_n[H] : 0;
-    const double hmax = act ? ql.gr_max[H] : 0.0;
     const bool dens = ql.dtol > 0.0 || ql.mcut > 0.0;
     const int2 klh = __ldg(reinterpret_cast<const int2*>(&rec[h0].si));
     const double pmax = dens ? quartet_pmax(ql, ijg.x, ijg.y, klh.x, klh.y) : 0.0;
@@ -235,31 +238,52 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     double X[XN];
 #pragma unroll
     for (int i = 0; i < XN; ++i) X[i] = 0.0;
-    for (int p = g0; p < g0 + gn; ++p) {
-      const double sp = pair_bound(rec, p);
-      if (!__any_sync(0xffffffffu, act && sp * hmax >= thr)) break;   // later bra pairs fail for every lane
-      const PairView bp = load_pair(rec, p);
-      const int I = bp.si, J = bp.sj;
-      double cab[NAB];
+    const double gmax = ql.gr_max[G];
+    // Each lane walks its own ket group's pairs (outer loop, one gather of the ket
+    // record per pair); the warp walks the bra group's pairs in step (inner loop:
+    // every lane reads the same bra record, one L1 wavefront per load).  Both
+    // lists are sorted by Schwarz bound, so the screens end the loops.
+    for (int qi = 0;; ++qi) {
+      const bool lv = qi < hn;
+      const int q = h0 + (lv ? qi : 0);
+      const double sq = lv ? pair_bound(rec, q) : 0.0;
+      const bool qok = lv && sq * gmax >= thr;
+      if (!__any_sync(0xffffffffu, qok)) break;
+      const PairView kq = load_pair(rec, q);
+      const double ze = kq.zeta;
+      const double Qx = kq.P[0], Qy = kq.P[1], Qz = kq.P[2];
+      const double Sq = kq.S;
+      const int K = kq.si, L = kq.sj;
+      const double wKL = (K != L) ? 2.0 : 1.0;
+      // ket coefficients: products held when small, factors otherwise
+      constexpr bool HOLD = NCD <= 16;
+      double ccd[HOLD ? NCD : 1];
+      double sK[NC], sL[ND];
 #pragma unroll
-      for (int k = AB0; k < AB1; ++k)
-        cab[ORD.ab[k]] = scoef[I * MAXCOMP + ORD.ab[k] / NB] * scoef[J * MAXCOMP + ORD.ab[k] % NB];
-      const double zb = bp.zeta;
-      const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
-      const double Sp = bp.S;
-      const double wIJ = (I != J) ? 2.0 : 1.0;
-      const int qe = !act ? h0 : ((G == H) ? p + 1 : h0 + hn);
-      for (int q = h0; q < qe; ++q) {
-        const double sq = pair_bound(rec, q);
-        if (sp * sq < thr) break;   // the reference's screen (thr = INTTOL); pairs sorted by bound
-        const PairView kq = load_pair(rec, q);
-        const double ze = kq.zeta;
-        const double Qx = kq.P[0], Qy = kq.P[1], Qz = kq.P[2];
+      for (int cc = 0; cc < NC; ++cc) sK[cc] = scoef[K * MAXCOMP + cc];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) sL[d] = scoef[L * MAXCOMP + d];
+      if constexpr (HOLD) {
+#pragma unroll
+        for (int cc = 0; cc < NC; ++cc)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = wKL * sK[cc] * sL[d];
+      }
+      for (int p = g0; p < g0 + gn; ++p) {
+        const double sp = pair_bound(rec, p);
+        const bool pass = qok && sp * sq >= thr;
+        if (!__any_sync(0xffffffffu, pass)) break;   // later bra pairs fail for every lane
+        // a group paired with itself: each unordered pair of pairs once (p >= q)
+        if (!pass || (G == H && p < q)) continue;
+        const PairView bp = load_pair(rec, p);
+        const int I = bp.si, J = bp.sj;
+        const double zb = bp.zeta;
+        const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
         const double zz = zb + ze;
         const double rho = zb * ze / zz;
         const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
         const double T = rho * (dx * dx + dy * dy + dz * dz);
-        const double pref = c2pi * Sp * kq.S * sqrt(rho);
+        const double pref = c2pi * bp.S * Sq * sqrt(rho);
         // FP32 only when every lane running this step qualifies
         bool f32 = false;
         if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < mcut);
@@ -287,21 +311,22 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
           }
         }
         any = true;
-        const int K = kq.si, L = kq.sj;
-        const double w = wIJ * ((K != L) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
-        double ccd[NCD];
+        const double w = ((I != J) ? 2.0 : 1.0) * ((p != q) ? 2.0 : 1.0);
 #pragma unroll
-        for (int cc = 0; cc < NC; ++cc) {
-          const double c1 = w * scoef[K * MAXCOMP + cc];
+        for (int k = AB0; k < AB1; ++k) {
+          const double ca = w * scoef[I * MAXCOMP + ORD.ab[k] / NB] * scoef[J * MAXCOMP + ORD.ab[k] % NB];
 #pragma unroll
-          for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = c1 * scoef[L * MAXCOMP + d];
+          for (int cc = 0; cc < NC; ++cc) {
+            double cb;
+            if constexpr (HOLD) cb = ca;
+            else cb = ca * (wKL * sK[cc]);
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+              const double c4 = HOLD ? cb * ccd[cc * ND + d] : cb * sL[d];
+              X[(k - AB0) * NCD + cc * ND + d] = fma(c4, out[ORD.ab[k] * NCD + cc * ND + d], X[(k - AB0) * NCD + cc * ND + d]);
+            }
+          }
         }
-#pragma unroll
-        for (int k = AB0; k < AB1; ++k)
-#pragma unroll
-          for (int cd = 0; cd < NCD; ++cd)
-            X[(k - AB0) * NCD + cd] =
-                fma(cab[ORD.ab[k]] * ccd[cd], out[ORD.ab[k] * NCD + cd], X[(k - AB0) * NCD + cd]);
       }
     }
     if (MIXED && PASS == 0) {
