@@ -14,6 +14,11 @@ One step = one direct J/K build (FOURINDEX_ERI) of all-trans C20H42 in
   over its event-timed duration, against the FP64 FMA-pipe peak measured here.
 * cpu_baseline: the CPU oracle (a restatement of the reference loop) on a
   bounded sample of bra shells, extrapolated to one full build, one core.
+* scf: time to a converged SCF of the same molecule, the reference's loop with
+  full FP64 builds against the time-to-solution path (batch_scf / scf.run_scf_fast).
+* batch (--batch N, default 32; 0 skips it): N uneven water clusters in cc-pVDZ
+  as one batch -- batched Fock builds/s, and the time to converged SCF of the
+  whole set, one plain FP64 GPU SCF per molecule against the batched SCF.
 * N > 1 (torchrun): every rank computes its share of the quartet chunks and the
   J/K matrices are summed with one NCCL all-reduce -- the reference's
   MPI_ALLREDUCE of J/K; total work is fixed (strong scaling).
@@ -233,6 +238,89 @@ def run_reference(args):
     return 0
 
 
+def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
+    """Uneven water clusters (cc-pVDZ, k ~ U{1..16} as geometry.water_batch_decks
+    draws them) as one batch: batched full FP64 Fock builds per second, and the
+    time to converged SCF of the whole set -- one plain FP64 GPU SCF per molecule
+    (the reference's loop, a DeviceFock each) against the batched SCF (set-up of
+    its DeviceBatch included), every molecule judged by E[P] of its final
+    idempotent density with full FP64 J/K."""
+    import numpy as np
+    import torch
+    from polymer_b200 import batch_scf, fock, geometry, guess, scf, system
+    dev = torch.device('cuda', device)
+    decks = geometry.water_batch_decks(n_clusters)
+    t0 = time.perf_counter()
+    systems = [system.build_system(d, fock.onee) for d in decks]
+    t_sys = time.perf_counter() - t0
+    ssys = [systems[k] for k in batch_scf.sorted_order(systems)]
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    fb = fock.DeviceBatch(ssys, device)
+    torch.cuda.synchronize(dev)
+    t_setup = time.perf_counter() - t0
+    cen = fb.census()
+    pc = torch.zeros_like(fb.p_c)
+    for k, s in enumerate(ssys):
+        fb.view(pc, k).copy_(torch.tensor(scf.guess_density(s)[0], device=dev))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(warmup):
+        fb.run_packed(pc, fb.out_c, fb.out_x)
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(float(k))
+        evs[k][0].record()
+        fb.run_packed(pc, fb.out_c, fb.out_x)
+        evs[k][1].record()
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    fb.close()
+
+    # plain: the reference's loop with full FP64 builds, one molecule after another
+    e_plain, it_plain = [], []
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for s in systems:
+        df = fock.DeviceFock(s, device)
+        r = scf.run_scf(s, df, device=dev, variational=True)
+        e_plain.append(r.energy_variational)
+        it_plain.append(len(r.iterations))
+        df.close()
+    torch.cuda.synchronize(dev)
+    t_plain = time.perf_counter() - t0
+    e_plain = np.array(e_plain)
+    lg = guess.LearnedGuess.load(guess.MODEL, device=dev)
+    runs = {}
+    for name, opts in (('batched', batch_scf.BatchOptions()),
+                       ('batched+learned+mixed', batch_scf.BatchOptions(guess=lg, mixed_cutoff=1e-6))):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        b = fock.DeviceBatch(ssys, device)
+        res = batch_scf.run_batch_scf(systems, opts, batch=b, device=device)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter() - t0
+        b.close()
+        runs[name] = {'s': t, 'speedup_vs_plain': t_plain / t, 'builds': res.builds,
+                      'iterations_mean': float(res.iterations.mean()), 'iterations_max': int(res.iterations.max()),
+                      'converged': bool(res.converged.all()),
+                      'max_abs_dE_vs_plain': float(np.abs(res.energy - e_plain).max()),
+                      'guess_fallbacks': int(res.fallback.sum()),
+                      'options': {'density_tol': opts.density_tol, 'density_tol_rel': opts.density_tol_rel,
+                                  'mixed_cutoff': opts.mixed_cutoff, 'reset_every': opts.reset_every,
+                                  'guess': opts.guess if isinstance(opts.guess, str) else 'learned'}}
+    return {'workload': '%d water clusters, cc-pVDZ, k ~ U{1..16} (seed 2000, cluster i from seed 2001+i), '
+                        'INTTOL 1e-10' % n_clusters,
+            'molecules': n_clusters, 'ncgs_total': int(sum(s.basis.ncgs for s in systems)),
+            'systems_s': t_sys, 'batch_setup_s': t_setup,
+            'build_ms': ms, 'builds_per_s': 1000.0 / ms, 'quartets_per_build': cen['quartets'],
+            'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
+            'launches_per_build': int(cen['kernel_launches']),
+            'l2': 'flushed before every timed build (256 MiB write)',
+            'scf': {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)), **runs,
+                    'wall_clock': 'host time around each whole set, GPU synchronised; one-electron set-up excluded'}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -241,6 +329,8 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-scf', action='store_true', help='skip the time-to-converged SCF leg')
+    ap.add_argument('--batch', type=int, default=32,
+                    help='water clusters in the batched leg (0: skip it)')
     ap.add_argument('--autotune', action='store_true',
                     help='time every kernel variant per quartet class and keep the fastest '
                          '(default: the library\'s measured schedule table)')
@@ -389,6 +479,10 @@ def main():
                     'plain_path': "reference loop (nuclear-charge guess, density DIIS), full FP64 builds",
                     'wall_clock': 'host time around each SCF, GPU synchronised'}
 
+    batch = None
+    if rank == 0 and world == 1 and args.batch > 0:
+        batch = batch_leg(args.batch, local, args.steps, args.warmup)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sysm, p_p.cpu().numpy())
@@ -406,7 +500,7 @@ def main():
                 'quartets_per_build': cen['quartets'], 'quartets_per_s': cen['quartets'] * value,
                 'gpu_launches': args.steps * int(cen['kernel_launches']),
                 'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'scf': scf_line,
-                'cpu_baseline': cpu}
+                'batch': batch, 'cpu_baseline': cpu}
         print(json.dumps(line))
     df.close()
     if world > 1:
