@@ -297,7 +297,7 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         b = fock.DeviceBatch(ssys, device)
-        res = batch_scf.run_batch_scf(systems, opts, batch=b, device=device)
+        res = batch_scf.run_batch_scf(systems, opts, batch=b, device=device, graph=True)
         torch.cuda.synchronize(dev)
         t = time.perf_counter() - t0
         b.close()
@@ -308,7 +308,8 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
                       'guess_fallbacks': int(res.fallback.sum()),
                       'options': {'density_tol': opts.density_tol, 'density_tol_rel': opts.density_tol_rel,
                                   'mixed_cutoff': opts.mixed_cutoff, 'reset_every': opts.reset_every,
-                                  'guess': opts.guess if isinstance(opts.guess, str) else 'learned'}}
+                                  'guess': opts.guess if isinstance(opts.guess, str) else 'learned',
+                                  'cuda_graph': 'each iteration from the third on is one graph replay'}}
     return {'workload': '%d water clusters, cc-pVDZ, k ~ U{1..16} (seed 2000, cluster i from seed 2001+i), '
                         'INTTOL 1e-10' % n_clusters,
             'molecules': n_clusters, 'ncgs_total': int(sum(s.basis.ncgs for s in systems)),

@@ -140,6 +140,14 @@ int32_t pfe_batch_set_screening(pfe_batch *b, int32_t precision_mode, double mix
 int32_t pfe_batch_set_instance_screening(pfe_batch *b, int32_t k, int32_t precision_mode, double mixed_cutoff,
                                          double density_tol);
 int32_t pfe_batch_fock_pc(pfe_batch *b, const double *d_p_c, double *d_c_c, double *d_x_c, void *stream);
+/* Graph capture: pfe_batch_fock_pc may be captured into a CUDA graph once its
+ * launch records are current.  Every build uploads the records from a pinned
+ * host copy, so a replay sees screening changed since the capture after this
+ * call rewrites that copy for densities packed at d_p_c (the pointer captured);
+ * call it with no replay in flight.  The kernels able to run FP32 are chosen at
+ * capture: set a mixed cutoff on some instance before capturing if any replay
+ * will use one. */
+int32_t pfe_batch_refresh(pfe_batch *b, const double *d_p_c);
 int32_t pfe_batch_destroy(pfe_batch *b);
 
 /* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */

@@ -132,61 +132,82 @@ class _Group:
 
 
 def sp2_projector(f: torch.Tensor, nocc: int, pad: torch.Tensor, tol: float = 1e-12, max_steps: int = 200,
-                  first_check: int = 12):
+                  first_check: int = 12, fixed_steps: Optional[int] = None):
     """Projector on the `nocc` lowest eigenvectors of each symmetric f [B, n, n]
     (slots marked in `pad` [B, n] are decoupled and left empty), by SP2.
 
     Gershgorin bounds [lo, hi] of the spectrum map f to X0 = (hi - f)/(hi - lo)
     with eigenvalues in [0, 1], occupied ones nearest 1; each step replaces X by
-    X^2 or 2X - X^2, whichever brings tr X^2 closer to nocc, until the
-    idempotency defect tr(X - X^2) is below `tol` for every matrix (checked
-    after `first_check` steps and then every other step); returns (X, steps)."""
+    X^2 or 2X - X^2, whichever brings tr X^2 closer to nocc.  Adaptive mode runs
+    until the idempotency defect tr(X - X^2) is below `tol` for every matrix
+    (checked after `first_check` steps, then every other step); with
+    `fixed_steps` it runs exactly that many steps and reads nothing back (the
+    form a CUDA graph can hold).  Returns (X, steps, defect per matrix)."""
     B, n, _ = f.shape
     d = f.diagonal(dim1=-2, dim2=-1)
     r = f.abs().sum(-1) - d.abs()
-    inf = torch.finfo(F64).max
-    lo = torch.where(pad, torch.full_like(d, inf), d - r).amin(-1)
-    hi = torch.where(pad, torch.full_like(d, -inf), d + r).amax(-1)
+    big = torch.finfo(F64).max
+    lo = torch.where(pad, torch.full_like(d, big), d - r).amin(-1)
+    hi = torch.where(pad, torch.full_like(d, -big), d + r).amax(-1)
     hi = torch.maximum(hi, lo + 1e-8)
     eye = torch.eye(n, dtype=F64, device=f.device)
-    # padded slots sit at the top of the spectrum: X0 = 0 there, a fixed point
-    x = (hi[:, None, None] * eye - f - torch.diag_embed(torch.where(pad, hi[:, None] - d, torch.zeros_like(d)))) \
-        / (hi - lo)[:, None, None]
+    x = (hi[:, None, None] * eye - f) / (hi - lo)[:, None, None]
+    # padded slots: X0 = 0 there, a fixed point of both maps
     x = torch.where(pad[:, :, None] | pad[:, None, :], torch.zeros_like(x), x)
     steps = 0
     while True:
         x2 = torch.bmm(x, x)
         t1, t2 = _trace(x), _trace(x2)
         steps += 1
-        up = (t2 - nocc).abs() < (2.0 * t1 - t2 - nocc).abs()
-        if steps >= first_check and steps % 2 == 0:
-            if float((t1 - t2).abs().max()) < tol:
-                return x, steps
-        if steps >= max_steps:
+        defect = (t1 - t2).abs()
+        if fixed_steps is None and steps >= first_check and steps % 2 == 0:
+            if float(defect.max()) < tol:
+                return x, steps, defect
+        if fixed_steps is None and steps >= max_steps:
             raise SCFError('SP2 projection did not converge')
+        up = (t2 - nocc).abs() < (2.0 * t1 - t2 - nocc).abs()
         x = torch.where(up[:, None, None], x2, 2.0 * x - x2)
+        if fixed_steps is not None and steps >= fixed_steps:
+            return x, steps, defect
 
 
-def _diis(group: _Group, hist_f: torch.Tensor, hist_e: torch.Tensor, valid: torch.Tensor) -> torch.Tensor:
-    """Pulay extrapolation per molecule over the valid history slots [B, D]."""
+def _spd_solve(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    """Solve a x = b for a batch of small symmetric positive definite a [B, m, m]
+    (Cholesky, unrolled over m in tensor operations: no host synchronisation,
+    no solver workspace -- usable inside a CUDA graph)."""
+    m = a.shape[-1]
+    L = torch.zeros_like(a)
+    for j in range(m):
+        s = a[:, j, j] - (L[:, j, :j] ** 2).sum(-1)
+        ljj = torch.sqrt(s.clamp_min(1e-300))
+        L[:, j, j] = ljj
+        if j + 1 < m:
+            L[:, j + 1:, j] = (a[:, j + 1:, j] - (L[:, j + 1:, :j] * L[:, j:j + 1, :j]).sum(-1)) / ljj[:, None]
+    y = torch.zeros_like(b)
+    for j in range(m):
+        y[:, j] = (b[:, j] - (L[:, j, :j] * y[:, :j]).sum(-1)) / L[:, j, j]
+    x = torch.zeros_like(b)
+    for j in reversed(range(m)):
+        x[:, j] = (y[:, j] - (L[:, j + 1:, j] * x[:, j + 1:]).sum(-1)) / L[:, j, j]
+    return x
+
+
+def _diis(hist_e: torch.Tensor, valid: torch.Tensor, slot: torch.Tensor) -> torch.Tensor:
+    """Pulay coefficients per molecule over the valid history slots [B, D]:
+    c = G^-1 1 / (1^T G^-1 1) with G the (scaled, slightly regularised) Gram
+    matrix of the commutators; the newest slot alone when that fails."""
     B, D = valid.shape
     e = hist_e.view(B, D, -1)
     g = torch.bmm(e, e.transpose(1, 2))
-    scale = g.diagonal(dim1=-2, dim2=-1).amax(-1).clamp_min(1e-300)
-    g = g / scale[:, None, None]
     vm = valid.to(F64)
-    a = torch.zeros((B, D + 1, D + 1), dtype=F64, device=g.device)
-    a[:, :D, :D] = g * vm[:, :, None] * vm[:, None, :] + torch.diag_embed(1.0 - vm)
-    a[:, :D, :D] += torch.diag_embed(vm * 1e-14)
-    a[:, :D, D] = -vm
-    a[:, D, :D] = -vm
-    rhs = torch.zeros((B, D + 1, 1), dtype=F64, device=g.device)
-    rhs[:, D, 0] = -1.0
-    sol, info = torch.linalg.solve_ex(a, rhs)
-    c = sol[:, :D, 0] * vm
-    ok = (info == 0) & torch.isfinite(c).all(-1)
-    return torch.where(ok[:, None], c, vm * 0.0 + torch.nn.functional.one_hot(
-        torch.full((B,), group.slot, device=g.device, dtype=torch.long), D).to(F64))
+    scale = (g.diagonal(dim1=-2, dim2=-1) * vm).amax(-1).clamp_min(1e-300)
+    g = g / scale[:, None, None]
+    a = g * vm[:, :, None] * vm[:, None, :] + torch.diag_embed(1.0 - vm + vm * 1e-12)
+    y = _spd_solve(a, vm)
+    c = y / y.sum(-1, keepdim=True)
+    ok = torch.isfinite(c).all(-1)
+    newest = torch.nn.functional.one_hot(slot.expand(B), D).to(F64)
+    return torch.where(ok[:, None], c, newest)
 
 
 def _check_system(sysm: System) -> None:
@@ -207,27 +228,38 @@ def sorted_order(systems: Sequence[System]) -> List[int]:
     return sorted(range(len(systems)), key=lambda k: _key(systems[k]))
 
 
-def _projector_density(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions):
-    # the idempotency test starts a little before the step count the group needed last time
-    d, steps = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max,
-                             first_check=max(8, getattr(g, 'sp2_last', 0) - 2))
-    g.sp2_last = steps
-    return 2.0 * g.w @ d @ g.w.transpose(1, 2), steps
+def _projector_density(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions, fixed: Optional[int] = None):
+    """P_C = 2 W D W^T with D the SP2 projector of f_ortho; adaptive steps unless `fixed`."""
+    d, steps, defect = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max,
+                                     first_check=max(8, g.sp2_last - 2), fixed_steps=fixed)
+    if fixed is None:
+        g.sp2_last = steps
+        g.sp2_seen = max(g.sp2_seen, steps)
+    return 2.0 * g.w @ d @ g.w.transpose(1, 2), steps, defect
 
 
 def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None, device=0,
                   max_cycles: Optional[int] = None, scfconv: Optional[float] = None,
                   batch: Optional['fock_mod.DeviceBatch'] = None,
                   log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True,
-                  profile: bool = False) -> BatchResult:
+                  profile: bool = False, graph: bool = False) -> BatchResult:
     """RHF of every molecule of `systems` (zero temperature, closed shells) as one batch.
 
     ``device``: a CUDA device index (the batch is then built here), or any torch
     device together with a ``batch`` object offering the DeviceBatch interface
-    (``off``, ``systems``, ``view``, ``run_packed``, ``set_instance_screening``)."""
+    (``off``, ``systems``, ``view``, ``run_packed``, ``set_instance_screening``).
+
+    ``graph``: from the third iteration on, the device part of an iteration
+    (outcome of the last one, density differences, the batched build, Fock
+    assembly, DIIS, SP2 with a fixed step count, the statistics) is one CUDA
+    graph replay; the host reads the statistics, sets the per-molecule
+    screening and masks, and replays.  The SP2 step count is the largest the
+    eager iterations needed plus a margin, raised (and the graph recaptured)
+    whenever a replay leaves a projector defect above the tolerance."""
     opts = opts or BatchOptions()
     t0 = time.perf_counter()
     dev = torch.device('cuda', device) if isinstance(device, int) else torch.device(device)
+    graph = graph and dev.type == 'cuda'
     nmol = len(systems)
     for s in systems:
         _check_system(s)
@@ -242,7 +274,11 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         k1 = k
         while k1 < nmol and _key(ssys[k1]) == _key(ssys[k]):
             k1 += 1
-        groups.append(_Group(list(range(k, k1)), ssys, fb.off[k], dev))
+        g = _Group(list(range(k, k1)), ssys, fb.off[k], dev)
+        g.sl = slice(k, k1)
+        g.sp2_last = g.sp2_seen = 0
+        g.sp2_fixed = None
+        groups.append(g)
         k = k1
     conv = np.array([s.deck.scfconv if scfconv is None else scfconv for s in ssys])
     ncycles = max_cycles or max(s.deck.scfcycles for s in ssys)
@@ -251,7 +287,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     p, p_ref, c_ref, x_ref = (torch.zeros(total, **f64) for _ in range(4))
     dp, dc, dx, p_new = (torch.zeros(total, **f64) for _ in range(4))
     learned = not isinstance(opts.guess, str)
-    sp2_steps = 0
+    sp2_steps = [0]
     phases = {'setup': 0.0, 'guess': 0.0, 'build': 0.0, 'update': 0.0, 'host': 0.0}
     tmark = [time.perf_counter()]
 
@@ -259,6 +295,8 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         # with `profile`, wall time per phase (the device is synchronised at each mark)
         if profile:
             if dev.type == 'cuda':
+                if torch.cuda.is_current_stream_capturing():
+                    return
                 torch.cuda.synchronize(dev)
             t = time.perf_counter()
             phases[name] += t - tmark[0]
@@ -275,9 +313,9 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             fb.view(p, kk).copy_(nuclear(kk))
     elif opts.guess == 'core':
         for g in groups:
-            pv, st = _projector_density(g, g.w.transpose(1, 2) @ g.h @ g.w, opts)
+            pv, st, _ = _projector_density(g, g.w.transpose(1, 2) @ g.h @ g.w, opts)
             g.view(p).copy_(pv)
-            sp2_steps += st
+            sp2_steps[0] += st
     elif learned:
         # occupied natural orbitals of the predicted density: the projector on the
         # nocc lowest eigenvectors of -D, D = P/2 in the orthonormal basis
@@ -285,19 +323,73 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             fb.view(p, kk).copy_(torch.tensor(np.asarray(opts.guess.raw(ssys[kk])), **f64))
         for g in groups:
             dm = 0.5 * g.ws @ g.view(p) @ g.ws.transpose(1, 2)
-            pv, st = _projector_density(g, -0.5 * (dm + dm.transpose(1, 2)), opts)
+            pv, st, _ = _projector_density(g, -0.5 * (dm + dm.transpose(1, 2)), opts)
             g.view(p).copy_(pv)
-            sp2_steps += st
+            sp2_steps[0] += st
     else:
         raise SCFError('unknown guess %r' % (opts.guess,))
-
+    p_nuc = None
+    if learned:
+        p_nuc = torch.zeros(total, **f64)
+        for kk in range(nmol):
+            fb.view(p_nuc, kk).copy_(nuclear(kk))
     mark('guess')
+
     D = max(1, opts.ndiis)
     for g in groups:
         g.hist_f = torch.zeros((g.B, D, g.n, g.n), **f64)
         g.hist_e = torch.zeros((g.B, D, g.n, g.n), **f64)
         g.valid = torch.zeros((g.B, D), dtype=torch.bool, device=dev)
-        g.slot = 0
+    # device-side inputs of an iteration (fixed addresses: a captured graph reads them)
+    take_t = torch.zeros(nmol, dtype=torch.bool, device=dev)
+    restart_t = torch.zeros(nmol, dtype=torch.bool, device=dev)
+    incr_t = torch.zeros(nmol, **f64)
+    live_t = torch.ones(nmol, **f64)
+    slot_t = torch.zeros(1, dtype=torch.long, device=dev)
+    stats_t = torch.zeros((nmol, 4), **f64)
+
+    def device_step(fixed: bool):
+        """The device part of one iteration (no host synchronisation when `fixed`)."""
+        for g in groups:
+            sl = g.sl
+            pv = g.view(p)
+            upd = torch.where(take_t[sl][:, None, None], g.view(p_new), pv)
+            if p_nuc is not None:
+                upd = torch.where(restart_t[sl][:, None, None], g.view(p_nuc), upd)
+                g.valid &= ~restart_t[sl][:, None]
+            pv.copy_(upd)
+            g.view(dp).copy_((pv - g.view(p_ref) * incr_t[sl][:, None, None]) * live_t[sl][:, None, None])
+        mark('host')
+        fb.run_packed(dp, dc, dx)
+        mark('build')
+        for g in groups:
+            sl = g.sl
+            im = incr_t[sl][:, None, None]
+            cv = g.view(dc) + g.view(c_ref) * im
+            xv = g.view(dx) + g.view(x_ref) * im
+            g.view(c_ref).copy_(cv)
+            g.view(x_ref).copy_(xv)
+            pv = g.view(p)
+            g.view(p_ref).copy_(pv)
+            f = g.h + cv - 0.5 * g.hfx * xv
+            f = 0.5 * (f + f.transpose(1, 2))
+            fo = g.w.transpose(1, 2) @ f @ g.w
+            po = g.ws @ pv @ g.ws.transpose(1, 2)
+            err = fo @ po - po @ fo
+            e = (pv * (g.h + 0.5 * cv - 0.25 * g.hfx * xv)).sum((1, 2)) + g.e_nuc
+            fe = err.abs().amax((1, 2))
+            g.hist_f.index_copy_(1, slot_t, fo.unsqueeze(1))
+            g.hist_e.index_copy_(1, slot_t, err.unsqueeze(1))
+            g.valid.index_fill_(1, slot_t, True)
+            c = _diis(g.hist_e, g.valid, slot_t)
+            fx = torch.einsum('bd,bdij->bij', c, g.hist_f)
+            pn, st, defect = _projector_density(g, fx, opts, g.sp2_fixed if fixed else None)
+            sp2_steps[0] += st
+            g.view(p_new).copy_(pn)
+            dchg = torch.sqrt(((pn - pv) ** 2).sum((1, 2)) / float(g.n * g.n))
+            stats_t[sl] = torch.stack([e, fe, dchg, defect], 1)
+        slot_t.add_(1).remainder_(D)
+
     state = np.full(nmol, _FULL)
     nbuild = np.zeros(nmol, dtype=int)
     have_ref = np.zeros(nmol, dtype=bool)
@@ -310,8 +402,12 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     energy = np.zeros(nmol)
     iters = np.zeros(nmol, dtype=int)
     last_change = np.full(nmol, np.inf)
+    take = np.zeros(nmol, dtype=bool)
+    restart = np.zeros(nmol, dtype=bool)
     screen = [None] * nmol
     builds = 0
+    cuda_graph = None
+    replays = 0
     for it in range(1, ncycles + 1):
         # ---- per-molecule build mode and screening
         for kk in range(nmol):
@@ -327,53 +423,49 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             if screen[kk] != sc:
                 fb.set_instance_screening(kk, *sc)
                 screen[kk] = sc
-        incr = torch.tensor((state == _INCR) | (state == _DONE), **f64)
-        live = torch.tensor(state != _DONE, **f64)
-        for g in groups:
-            sl = slice(g.members[0], g.members[-1] + 1)
-            im, lm = incr[sl][:, None, None], live[sl][:, None, None]
-            g.view(dp).copy_((g.view(p) - g.view(p_ref) * im) * lm)
-        mark('host')
-        fb.run_packed(dp, dc, dx)
-        mark('build')
+        take_t.copy_(torch.from_numpy(take))
+        restart_t.copy_(torch.from_numpy(restart))
+        incr_t.copy_(torch.from_numpy(((state == _INCR) | (state == _DONE)).astype(np.float64)))
+        live_t.copy_(torch.from_numpy((state != _DONE).astype(np.float64)))
+        if graph and it >= 3:
+            if cuda_graph is None:
+                for g in groups:
+                    g.sp2_fixed = g.sp2_fixed or (g.sp2_seen + 6)
+                fb.refresh(dp)
+                side = torch.cuda.Stream(dev)
+                side.wait_stream(torch.cuda.current_stream(dev))
+                with torch.cuda.stream(side):
+                    device_step(True)            # this iteration, run eagerly on the capture stream
+                torch.cuda.current_stream(dev).wait_stream(side)
+                torch.cuda.synchronize(dev)
+                host_stats = stats_t.cpu().numpy()
+                cuda_graph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(cuda_graph, stream=side):
+                    device_step(True)
+                torch.cuda.synchronize(dev)
+            else:
+                fb.refresh(dp)
+                cuda_graph.replay()
+                replays += 1
+                host_stats = stats_t.cpu().numpy()
+        else:
+            device_step(False)
+            host_stats = stats_t.cpu().numpy()
         builds += 1
         nbuild[~done] += 1
-        stats = []
-        for g in groups:
-            sl = slice(g.members[0], g.members[-1] + 1)
-            im = incr[sl][:, None, None]
-            cv = g.view(dc) + g.view(c_ref) * im
-            xv = g.view(dx) + g.view(x_ref) * im
-            g.view(c_ref).copy_(cv)
-            g.view(x_ref).copy_(xv)
-            pv = g.view(p)
-            g.view(p_ref).copy_(pv)
-            f = g.h + cv - 0.5 * g.hfx * xv
-            f = 0.5 * (f + f.transpose(1, 2))
-            fo = g.w.transpose(1, 2) @ f @ g.w
-            po = g.ws @ pv @ g.ws.transpose(1, 2)
-            err = fo @ po - po @ fo
-            e = (pv * (g.h + 0.5 * cv - 0.25 * g.hfx * xv)).sum((1, 2)) + g.e_nuc
-            fe = err.abs().amax((1, 2))
-            g.hist_f[:, g.slot] = fo
-            g.hist_e[:, g.slot] = err
-            g.valid[:, g.slot] = True
-            c = _diis(g, g.hist_f, g.hist_e, g.valid)
-            fx = torch.einsum('bd,bdij->bij', c, g.hist_f)
-            pn, st = _projector_density(g, fx, opts)
-            sp2_steps += st
-            g.view(p_new).copy_(pn)
-            dchg = torch.sqrt(((pn - pv) ** 2).sum((1, 2)) / float(g.n * g.n))
-            stats.append(torch.stack([e, fe, dchg], 1))
-            g.slot = (g.slot + 1) % D
-        host = torch.cat(stats).cpu().numpy()
         mark('update')
-        take = np.zeros(nmol, dtype=bool)
-        restart = []
+        host = host_stats
+        if cuda_graph is not None and float(host[~done, 3].max() if (~done).any() else 0.0) > 1e3 * opts.sp2_tol:
+            # a replay's projectors are not converged: more SP2 steps, capture again
+            for g in groups:
+                g.sp2_fixed += 8
+            cuda_graph = None
+        take[:] = False
+        restart[:] = False
         for kk in range(nmol):
             if done[kk]:
                 continue
-            e_k, fe_k, dchg_k = host[kk]
+            e_k, fe_k, dchg_k, _ = host[kk]
             iters[kk] = it
             last_change[kk] = dchg_k
             have_ref[kk] = True
@@ -381,8 +473,12 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 first[kk] = False
                 first_err[kk] = fe_k
                 if learned and fe_k > opts.fallback_error:
+                    # the learned guess is judged by the plain one: restart from the nuclear-charge guess
                     fallback[kk] = True
-                    restart.append(kk)
+                    restart[kk] = True
+                    have_ref[kk] = False
+                    nbuild[kk] = 0
+                    last_change[kk] = np.inf
                     continue
             if final_pending[kk] and dchg_k < conv[kk]:
                 converged[kk] = done[kk] = True
@@ -390,26 +486,17 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 continue
             final_pending[kk] = dchg_k < conv[kk]
             take[kk] = True
-        tk = torch.tensor(take, device=dev)
-        for g in groups:
-            sl = slice(g.members[0], g.members[-1] + 1)
-            g.view(p).copy_(torch.where(tk[sl][:, None, None], g.view(p_new), g.view(p)))
-        for kk in restart:
-            # the learned guess is judged by the plain one: restart from the nuclear-charge guess
-            fb.view(p, kk).copy_(nuclear(kk))
-            have_ref[kk] = False
-            nbuild[kk] = 0
-            last_change[kk] = np.inf
-            for g in groups:
-                if g.members[0] <= kk <= g.members[-1]:
-                    g.valid[kk - g.members[0]] = False
         if log:
             nd = int(done.sum())
-            log('%3d  done %4d/%d  max DIIS error %.3e  max dP %.3e' % (
+            log('%3d  done %4d/%d  max DIIS error %.3e  max dP %.3e%s' % (
                 it, nd, nmol, float(host[~done, 1].max()) if nd < nmol else 0.0,
-                float(host[~done, 2].max()) if nd < nmol else 0.0))
+                float(host[~done, 2].max()) if nd < nmol else 0.0, '  (graph)' if cuda_graph is not None else ''))
         if done.all():
             break
+    # apply the last outcome (molecules that did not converge keep their newest density)
+    for g in groups:
+        tk = torch.from_numpy(take[g.sl]).to(dev)
+        g.view(p).copy_(torch.where(tk[:, None, None], g.view(p_new), g.view(p)))
     if dev.type == 'cuda':
         torch.cuda.synchronize(dev)
     if not converged.all() and raise_on_fail:
@@ -417,8 +504,10 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     inv = np.empty(nmol, dtype=int)
     inv[np.array(order)] = np.arange(nmol)
     p_out = [fb.view(p, int(inv[k])).t().clone() for k in range(nmol)]
+    if profile:
+        phases['graph_replays'] = replays
     res = BatchResult(energy[inv], converged[inv], iters[inv], builds, time.perf_counter() - t0, first_err[inv],
-                      fallback[inv], p_out, sp2_steps, phases if profile else None)
+                      fallback[inv], p_out, sp2_steps[0], phases if profile else None)
     if batch is None:
         fb.close()
     return res

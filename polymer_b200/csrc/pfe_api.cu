@@ -580,6 +580,13 @@ int32_t pfe_batch_set_instance_screening(pfe_batch* b, int32_t k, int32_t precis
   return PFE_OK;
 }
 
+int32_t pfe_batch_refresh(pfe_batch* b, const double* d_p_c) {
+  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!d_p_c) { set_error("null device pointer"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(b->device));
+  return batch_refresh(b, d_p_c);
+}
+
 int32_t pfe_batch_offsets(pfe_batch* b, int64_t* off) {
   if (!b || !off) { set_error("null argument"); return PFE_EINVAL; }
   for (size_t k = 0; k < b->off.size(); ++k) off[k] = b->off[k];

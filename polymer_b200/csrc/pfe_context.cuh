@@ -184,8 +184,13 @@ struct pfe_batch {
   std::vector<long long> off;       // packed offsets (doubles) of the ncgs x ncgs matrices, n+1
   pfe::ClassLaunch launches[64];    // joined chunk lists; ops/tables of the first instance with the class
   int nlaunch = 0;
-  void* d_insts = nullptr;          // the instances' launch records (MolLaunch), rebuilt per density pointer
-  const double* insts_for = nullptr;
+  void* d_insts = nullptr;          // the instances' launch records (MolLaunch) on the device
+  void* h_insts = nullptr;          // ... and their pinned host copy, uploaded by every build (so a
+                                    // captured graph re-reads it at each replay)
+  cudaEvent_t ev_insts = nullptr;   // the last upload of h_insts
+  bool ev_pending = false;
+  const double* insts_for = nullptr;  // density the records point at (null: rewrite them)
+  bool mixed = false;               // FP32-capable kernels (sticky once any instance asked for them)
   std::vector<void*> owned;
   cudaError_t alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
@@ -195,12 +200,20 @@ struct pfe_batch {
   void release_all() {
     for (void* p : owned) cudaFree(p);
     owned.clear();
+    if (h_insts) cudaFreeHost(h_insts);
+    h_insts = nullptr;
+    if (ev_insts) cudaEventDestroy(ev_insts);
+    ev_insts = nullptr;
+    ev_pending = false;
+    d_insts = nullptr;
+    insts_for = nullptr;
   }
 };
 
 namespace pfe {
 int batch_setup(pfe_batch* b);
 int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
+int batch_refresh(pfe_batch* b, const double* d_pc);
 int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n);
 void free_pairs(pfe_context* ctx, PairArrays* pa);
 void launch_symmetrize(const double* a, double* out, int n, int ncell, cudaStream_t s);

@@ -993,11 +993,11 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
 
 // Zero the target-space J'/K' and the FP32 counter; block maxima of the density
 // when screening or mixed precision is on.
-static int prepare_build(pfe_context* ctx, const double* d_dt, cudaStream_t s) {
+static int prepare_build(pfe_context* ctx, const double* d_dt, cudaStream_t s, bool always_bmax = false) {
   PFE_CUDA(cudaMemsetAsync(ctx->d_jp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_kp, 0, target_bytes(ctx), s));
   PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
-  if (ctx->dtol > 0.0 || ctx->mcut > 0.0) {
+  if (always_bmax || ctx->dtol > 0.0 || ctx->mcut > 0.0) {
     const long long nt2 = (long long)ctx->nt * ctx->nt;
     PFE_CUDA(cudaMemsetAsync(ctx->d_bmax, 0, sizeof(double) * (size_t)ctx->nblk * ctx->nblk, s));
     k_block_dmax<<<(unsigned)((nt2 + 255) / 256), 256, 0, s>>>(d_dt, ctx->nt, ctx->d_tblk, ctx->nblk,
@@ -1123,8 +1123,27 @@ int batch_setup(pfe_batch* b) {
       b->launches[b->nlaunch++] = cl;
     }
   PFE_CUDA(b->alloc(&b->d_insts, sizeof(MolLaunch) * b->inst.size()));
+  PFE_CUDA(cudaMallocHost(&b->h_insts, sizeof(MolLaunch) * b->inst.size()));
+  PFE_CUDA(cudaEventCreateWithFlags(&b->ev_insts, cudaEventDisableTiming));
   b->insts_for = nullptr;
+  b->mixed = false;
+  for (pfe_context* c : b->inst) b->mixed = b->mixed || c->mcut > 0.0;
   PFE_CUDA(cudaDeviceSynchronize());
+  return PFE_OK;
+}
+
+// Rewrite the pinned launch records for densities packed at d_pc with the
+// instances' current screening (waits for the previous upload to finish).
+int batch_refresh(pfe_batch* b, const double* d_pc) {
+  if (b->ev_pending) PFE_CUDA(cudaEventSynchronize(b->ev_insts));
+  b->ev_pending = false;
+  MolLaunch* h = static_cast<MolLaunch*>(b->h_insts);
+  for (size_t k = 0; k < b->inst.size(); ++k) {
+    pfe_context* c = b->inst[k];
+    h[k] = make_launch(c, c->contracted ? d_pc + b->off[k] : c->d_pt);
+    b->mixed = b->mixed || c->mcut > 0.0;
+  }
+  b->insts_for = d_pc;
   return PFE_OK;
 }
 
@@ -1146,30 +1165,36 @@ int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, 
       return PFE_ECUDA;
     }
   }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  PFE_CUDA(cudaStreamIsCapturing(s, &cap));
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
   if (b->insts_for != d_pc) {
-    // earlier builds on this stream may still read the records
-    PFE_CUDA(cudaStreamSynchronize(s));
-    std::vector<MolLaunch> h(n);
-    for (size_t k = 0; k < n; ++k) {
-      pfe_context* c = b->inst[k];
-      h[k] = make_launch(c, c->contracted ? d_pc + b->off[k] : c->d_pt);
+    if (capturing) {
+      set_error("batch: launch records are stale inside a stream capture (call pfe_batch_refresh first)");
+      return PFE_EINVAL;
     }
-    PFE_CUDA(cudaMemcpy(b->d_insts, h.data(), sizeof(MolLaunch) * n, cudaMemcpyHostToDevice));
-    b->insts_for = d_pc;
+    const int rc = batch_refresh(b, d_pc);
+    if (rc != PFE_OK) return rc;
+  }
+  // the records travel with every build: a captured graph uploads what the host
+  // last wrote into the pinned copy
+  PFE_CUDA(cudaMemcpyAsync(b->d_insts, b->h_insts, sizeof(MolLaunch) * n, cudaMemcpyHostToDevice, s));
+  if (!capturing) {
+    PFE_CUDA(cudaEventRecord(b->ev_insts, s));
+    b->ev_pending = true;
   }
   for (size_t k = 0; k < n; ++k) {
     pfe_context* c = b->inst[k];
-    const int rc = prepare_build(c, c->contracted ? d_pc + b->off[k] : c->d_pt, s);
+    // block maxima for every instance: its screening may change between graph replays
+    const int rc = prepare_build(c, c->contracted ? d_pc + b->off[k] : c->d_pt, s, true);
     if (rc != PFE_OK) return rc;
   }
   pfe_context* c0 = b->inst[0];
   MolLaunch lq = make_launch(c0, c0->d_pt);
   lq.insts = static_cast<const MolLaunch*>(b->d_insts);
-  bool mixed = false;   // the FP32-capable kernels, when any instance uses them
-  for (pfe_context* c : b->inst) mixed = mixed || c->mcut > 0.0;
   for (int i = 0; i < b->nlaunch; ++i) {
     const ClassLaunch& cl = b->launches[i];
-    launch_class(c0, cl, lq, cl.variant, s, mixed);
+    launch_class(c0, cl, lq, cl.variant, s, b->mixed);
     PFE_CUDA(cudaGetLastError());
   }
   for (size_t k = 0; k < n; ++k) {

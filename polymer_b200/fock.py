@@ -215,6 +215,11 @@ class DeviceBatch:
         n = self.ncgs[k]
         return packed[self.off[k]:self.off[k + 1]].view(n, n).t()
 
+    def refresh(self, p_c: torch.Tensor) -> None:
+        """Rewrite the launch records for densities packed in p_c with the current
+        screening (before replaying a captured build; no replay may be in flight)."""
+        check(self.L, self.L.pfe_batch_refresh(self.handle, ctypes.c_void_p(p_c.data_ptr())))
+
     def run_packed(self, p_c: torch.Tensor, out_c: torch.Tensor, out_x: torch.Tensor, stream=None) -> None:
         """Raw call on packed device buffers (pfe_batch_fock_pc), asynchronous."""
         s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream

@@ -3,7 +3,9 @@ as the Fock builder of every molecule.
 
 * SP2 projection gives the spectral projector of a symmetric matrix (checked
   against eigh), leaving decoupled padded slots empty;
-* the batched DIIS reduces to the single-molecule Pulay solution;
+* the batched DIIS (a Cholesky solve in tensor operations, usable in a CUDA
+  graph) gives the Pulay coefficients of the bordered system, over the valid
+  history slots only; SP2 with a fixed step count matches the adaptive one;
 * a batch of molecules of two sizes converges every molecule to the energy of
   the reference loop within 1e-8 Eh (the oracle ignores the screening knobs,
   so incremental builds are exact up to rounding), including the core guess.
@@ -26,7 +28,10 @@ def test_sp2_projector_matches_eigh():
     pad[1, -2:] = True
     f[1, -2:, :] = 0.0
     f[1, :, -2:] = 0.0
-    x, steps = batch_scf.sp2_projector(f, nocc, pad, tol=1e-13)
+    x, steps, defect = batch_scf.sp2_projector(f, nocc, pad, tol=1e-13)
+    xf, steps_f, defect_f = batch_scf.sp2_projector(f, nocc, pad, fixed_steps=steps + 4)
+    assert float(defect.max()) < 1e-13 and float(defect_f.max()) < 1e-12
+    assert float((xf - x).abs().max()) < 1e-11
     for b in range(B):
         m = n - int(pad[b].sum())
         e, v = np.linalg.eigh(f[b, :m, :m].numpy())
@@ -35,6 +40,30 @@ def test_sp2_projector_matches_eigh():
         if m < n:
             assert np.abs(x[b, m:, :].numpy()).max() == 0.0
     assert steps < 100
+
+
+def test_diis_coefficients_match_the_pulay_system():
+    rng = np.random.default_rng(3)
+    B, D, n = 4, 6, 5
+    e = torch.tensor(rng.normal(size=(B, D, n, n)))
+    valid = torch.ones((B, D), dtype=torch.bool)
+    valid[1, 4:] = False
+    valid[2, :] = False
+    valid[2, 3] = True
+    slot = torch.tensor([3])
+    c = batch_scf._diis(e, valid, slot).numpy()
+    for b in range(B):
+        idx = np.nonzero(valid[b].numpy())[0]
+        m = len(idx)
+        ev = e[b].reshape(D, -1).numpy()[idx]
+        a = np.zeros((m + 1, m + 1))
+        a[:m, :m] = ev @ ev.T
+        a[:m, m] = a[m, :m] = -1.0
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1.0
+        ref = np.linalg.solve(a, rhs)[:m]
+        assert np.abs(c[b, idx] - ref).max() < 1e-9
+        assert np.abs(np.delete(c[b], idx)).max(initial=0.0) == 0.0
 
 
 class OracleBatch:
