@@ -148,6 +148,11 @@ int32_t pfe_batch_fock_pc(pfe_batch *b, const double *d_p_c, double *d_c_c, doub
  * capture: set a mixed cutoff on some instance before capturing if any replay
  * will use one. */
 int32_t pfe_batch_refresh(pfe_batch *b, const double *d_p_c);
+/* The schedule autotuner over a batch: times every execution variant of every
+ * quartet class on the batch's densities d_p_c (packed) and keeps the fastest;
+ * pfe_batch_schedule reports the classes (cls, chosen variant, tuned_ms,
+ * quartets, flops; ms = 0) and returns their number. */
+int32_t pfe_batch_autotune(pfe_batch *b, const double *d_p_c, void *stream);
 int32_t pfe_batch_destroy(pfe_batch *b);
 
 /* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */
@@ -179,6 +184,8 @@ typedef struct pfe_kernel_stat {
   double flops;
 } pfe_kernel_stat;
 int32_t pfe_context_kernel_stats(pfe_context *ctx, pfe_kernel_stat *out, int32_t cap);
+/* A batch's quartet classes and their schedule (see pfe_batch_autotune). */
+int32_t pfe_batch_schedule(pfe_batch *b, pfe_kernel_stat *out, int32_t cap);
 
 /* Schedule autotuning (no counterpart in the reference): time every execution
  * variant of every quartet class on this context's screened work lists with the

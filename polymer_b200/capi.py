@@ -128,6 +128,10 @@ def lib(path: str = LIB_PATH):
     L.pfe_batch_set_instance_screening.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                                    ctypes.c_double]
     L.pfe_batch_set_instance_screening.restype = ctypes.c_int32
+    L.pfe_batch_autotune.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.pfe_batch_autotune.restype = ctypes.c_int32
+    L.pfe_batch_schedule.argtypes = [ctypes.c_void_p, ctypes.POINTER(PfeKernelStat), ctypes.c_int32]
+    L.pfe_batch_schedule.restype = ctypes.c_int32
     L.pfe_batch_refresh.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
     L.pfe_batch_refresh.restype = ctypes.c_int32
     L.pfe_batch_fock_pc.argtypes = [ctypes.c_void_p] * 5
@@ -188,7 +192,8 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_measure_fp64_peak', 'pfe_context_autotune', 'pfe_context_force_variant',
            'pfe_version', 'pfe_overlap_kinetic_noalloc', 'pfe_context_fock_pc',
            'pfe_context_primitive_targets', 'pfe_context_set_screening', 'pfe_batch_create', 'pfe_batch_setup',
-           'pfe_batch_set_screening', 'pfe_batch_set_instance_screening', 'pfe_batch_offsets', 'pfe_batch_refresh', 'pfe_batch_fock_pc', 'pfe_batch_census', 'pfe_batch_destroy']
+           'pfe_batch_set_screening', 'pfe_batch_set_instance_screening', 'pfe_batch_offsets', 'pfe_batch_refresh',
+           'pfe_batch_autotune', 'pfe_batch_schedule', 'pfe_batch_fock_pc', 'pfe_batch_census', 'pfe_batch_destroy']
 
 # Exported symbols declared in include/polymer_guess.h (checked by the CPU tests).
 GUESS_EXPORTS = ['pfe_mlp_gemm', 'pfe_mlp_bias_act', 'pfe_mlp_act_grad', 'pfe_mlp_colsum', 'pfe_mlp_mse',

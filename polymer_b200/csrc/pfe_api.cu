@@ -587,6 +587,34 @@ int32_t pfe_batch_refresh(pfe_batch* b, const double* d_p_c) {
   return batch_refresh(b, d_p_c);
 }
 
+// (la lb lc ld) of a (bra class, ket class) pair as a four-digit code
+static int class_code(int cb, int ck) {
+  static const int t[6][2] = {{0, 0}, {1, 0}, {1, 1}, {2, 0}, {2, 1}, {2, 2}};
+  return 1000 * t[cb][0] + 100 * t[cb][1] + 10 * t[ck][0] + t[ck][1];
+}
+
+int32_t pfe_batch_autotune(pfe_batch* b, const double* d_p_c, void* stream) {
+  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!d_p_c) { set_error("null device pointer"); return PFE_EINVAL; }
+  PFE_CUDA(cudaSetDevice(b->device));
+  return batch_autotune(b, d_p_c, (cudaStream_t)stream);
+}
+
+int32_t pfe_batch_schedule(pfe_batch* b, pfe_kernel_stat* out, int32_t cap) {
+  if (!b || !out) { set_error("null argument"); return PFE_EINVAL; }
+  int n = 0;
+  for (int i = 0; i < b->nlaunch && n < cap; ++i, ++n) {
+    const ClassLaunch& cl = b->launches[i];
+    out[n].cls = class_code(cl.cb, cl.ck);
+    out[n].variant = cl.variant;
+    for (int v = 0; v < 3; ++v) out[n].tuned_ms[v] = cl.tuned_ms[v];
+    out[n].ms = 0.f;
+    out[n].quartets = cl.quartets;
+    out[n].flops = cl.quartets * class_flops(cl.cb, cl.ck);
+  }
+  return n;
+}
+
 int32_t pfe_batch_offsets(pfe_batch* b, int64_t* off) {
   if (!b || !off) { set_error("null argument"); return PFE_EINVAL; }
   for (size_t k = 0; k < b->off.size(); ++k) off[k] = b->off[k];

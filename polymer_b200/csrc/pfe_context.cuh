@@ -214,6 +214,7 @@ namespace pfe {
 int batch_setup(pfe_batch* b);
 int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
 int batch_refresh(pfe_batch* b, const double* d_pc);
+int batch_autotune(pfe_batch* b, const double* d_pc, cudaStream_t s);
 int alloc_pairs(pfe_context* ctx, PairArrays* pa, long long n);
 void free_pairs(pfe_context* ctx, PairArrays* pa);
 void launch_symmetrize(const double* a, double* out, int n, int ncell, cudaStream_t s);

@@ -1147,11 +1147,9 @@ int batch_refresh(pfe_batch* b, const double* d_pc) {
   return PFE_OK;
 }
 
-// One build of every instance from the packed contracted densities d_pc.
-int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s) {
-  const size_t n = b->inst.size();
-  // target-space densities: P_C itself, or P_P = CC^T P_C CC for primitive targets
-  for (size_t k = 0; k < n; ++k) {
+// Target-space densities of the instances with primitive targets: P_P = CC^T P_C CC.
+static int batch_decontract(pfe_batch* b, const double* d_pc, cudaStream_t s) {
+  for (size_t k = 0; k < b->inst.size(); ++k) {
     pfe_context* c = b->inst[k];
     if (c->contracted) continue;
     const int np = c->npgs, nc = c->ncgs;
@@ -1164,6 +1162,16 @@ int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, 
       set_error("batch: cublasDgemm (decontraction) failed");
       return PFE_ECUDA;
     }
+  }
+  return PFE_OK;
+}
+
+// One build of every instance from the packed contracted densities d_pc.
+int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s) {
+  const size_t n = b->inst.size();
+  {
+    const int rc = batch_decontract(b, d_pc, s);
+    if (rc != PFE_OK) return rc;
   }
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   PFE_CUDA(cudaStreamIsCapturing(s, &cap));
@@ -1208,6 +1216,54 @@ int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, 
     }
   }
   PFE_CUDA(cudaGetLastError());
+  return PFE_OK;
+}
+
+// The schedule autotuner over a batch: every execution variant of every joined
+// class is timed on the batch's densities d_pc and the fastest kept.
+int batch_autotune(pfe_batch* b, const double* d_pc, cudaStream_t s) {
+  int rc = batch_decontract(b, d_pc, s);
+  if (rc != PFE_OK) return rc;
+  if (b->insts_for != d_pc && (rc = batch_refresh(b, d_pc)) != PFE_OK) return rc;
+  PFE_CUDA(cudaMemcpyAsync(b->d_insts, b->h_insts, sizeof(MolLaunch) * b->inst.size(), cudaMemcpyHostToDevice, s));
+  PFE_CUDA(cudaEventRecord(b->ev_insts, s));
+  b->ev_pending = true;
+  for (size_t k = 0; k < b->inst.size(); ++k) {
+    pfe_context* c = b->inst[k];
+    if ((rc = prepare_build(c, c->contracted ? d_pc + b->off[k] : c->d_pt, s, true)) != PFE_OK) return rc;
+  }
+  pfe_context* c0 = b->inst[0];
+  MolLaunch lq = make_launch(c0, c0->d_pt);
+  lq.insts = static_cast<const MolLaunch*>(b->d_insts);
+  cudaEvent_t e0, e1;
+  PFE_CUDA(cudaEventCreate(&e0));
+  PFE_CUDA(cudaEventCreate(&e1));
+  for (int i = 0; i < b->nlaunch; ++i) {
+    ClassLaunch& cl = b->launches[i];
+    float best = 1e30f;
+    int bestv = cl.variant;
+    for (int v = 0; v < 3; ++v) {
+      if (!variant_ok(cl, v)) continue;
+      launch_class(c0, cl, lq, v, s, b->mixed);
+      float t = 1e30f;
+      for (int r = 0; r < 2; ++r) {
+        PFE_CUDA(cudaEventRecord(e0, s));
+        launch_class(c0, cl, lq, v, s, b->mixed);
+        PFE_CUDA(cudaEventRecord(e1, s));
+        PFE_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t = std::min(t, ms);
+      }
+      PFE_CUDA(cudaGetLastError());
+      cl.tuned_ms[v] = t;
+      if (t < best) { best = t; bestv = v; }
+    }
+    cl.variant = bestv;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  PFE_CUDA(cudaStreamSynchronize(s));
   return PFE_OK;
 }
 

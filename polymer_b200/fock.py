@@ -215,6 +215,20 @@ class DeviceBatch:
         n = self.ncgs[k]
         return packed[self.off[k]:self.off[k + 1]].view(n, n).t()
 
+    def autotune(self, p_c: torch.Tensor) -> None:
+        """Time every execution variant per quartet class on packed densities p_c; keep the fastest."""
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(self.L, self.L.pfe_batch_autotune(self.handle, ctypes.c_void_p(p_c.data_ptr()), ctypes.c_void_p(s)))
+
+    def schedule(self) -> list:
+        """(class, variant, tuned ms per variant, quartets) of every joined quartet class."""
+        st = (capi.PfeKernelStat * 64)()
+        n = self.L.pfe_batch_schedule(self.handle, st, 64)
+        if n < 0:
+            check(self.L, n)
+        return [{'cls': '%04d' % x.cls, 'variant': x.variant, 'tuned_ms': list(x.tuned_ms),
+                 'quartets': x.quartets} for x in st[:n]]
+
     def refresh(self, p_c: torch.Tensor) -> None:
         """Rewrite the launch records for densities packed in p_c with the current
         screening (before replaying a captured build; no replay may be in flight)."""

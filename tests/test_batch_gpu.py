@@ -3,14 +3,15 @@ over the work of every molecule in the batch.
 
 * each molecule's C_C/X_C from the batched build equals its own
   pfe_context_fock_pc build to 1e-11 of max|C_C| (only the order of the FP64
-  atomics differs), for water clusters of several sizes in cc-pVDZ (primitive
-  targets, a general contraction), alkanes in 6-31G** (contracted targets) and
-  a batch that mixes both;
+  atomics differs), for water clusters of several sizes in cc-pVDZ, alkanes in
+  6-31G** and a batch that mixes both;
 * a second build from another packed buffer (the per-molecule launch records
   are rebuilt for the new pointer) and screening set on the whole batch match
   the per-molecule builds the same way;
 * the census of a batch sums its molecules' quartets while the class launches
-  do not grow with the number of molecules.
+  do not grow with the number of molecules;
+* after the batch autotuner has timed every variant of every class, builds
+  still match the per-molecule ones.
 """
 import numpy as np
 import pytest
@@ -115,4 +116,20 @@ def test_batch_census():
     assert c['flops'] == pytest.approx(sum(x['flops'] for x in singles), rel=1e-12)
     assert c['pairs'] == sum(x['pairs'] for x in singles)
     assert c['kernel_launches'] <= max(x['kernel_launches'] for x in singles)
+    b.close()
+
+
+def test_batch_autotune_keeps_results():
+    systems = [_sys(geometry.water_deck(k, seed=3400 + k)) for k in (2, 3)]
+    pcs = [_pc(s, 90 + k) for k, s in enumerate(systems)]
+    ref = _singles(systems, pcs)
+    b = fock.DeviceBatch(systems)
+    for k, pc in enumerate(pcs):
+        b.view(b.p_c, k).copy_(torch.tensor(pc, device='cuda'))
+    b.autotune(b.p_c)
+    sched = b.schedule()
+    assert sched and all(max(x['tuned_ms']) > 0.0 for x in sched)
+    got = b([torch.tensor(pc, device='cuda') for pc in pcs])
+    torch.cuda.synchronize()
+    _check(got, ref, 'autotuned')
     b.close()

@@ -2,7 +2,8 @@
 density-screened / mixed-precision builds of the molecular path.
 
 * pfe_context_fock_pc(P_C) equals pfe_context_fock(CC^T P_C CC) for contracted
-  targets (6-31G**) and for primitive targets (cc-pVDZ, a general contraction);
+  targets, in 6-31G** and in cc-pVDZ (whose shared primitives READ3 copies
+  once per contracted function);
 * a P_P that is not a decontracted density is refused by the device path,
   handled (primitive targets) by the host path, to the oracle's tolerance;
 * the FP32 recursion (PFE_PREC_MIXED) stays within 1e-10 * max|C_C| of the
