@@ -238,7 +238,7 @@ def run_reference(args):
     return 0
 
 
-def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
+def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: bool = False):
     """Uneven water clusters (cc-pVDZ, k ~ U{1..16} as geometry.water_batch_decks
     draws them) as one batch: batched full FP64 Fock builds per second, and the
     time to converged SCF of the whole set -- one plain FP64 GPU SCF per molecule
@@ -275,16 +275,18 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
         evs[k][1].record()
     torch.cuda.synchronize(dev)
     ms = sum(a.elapsed_time(b) for a, b in evs) / steps
-    # the same builds after the batch autotuner picked each class's variant on them
-    fb.autotune(pc)
-    for k in range(steps):
-        flush.fill_(float(k))
-        evs[k][0].record()
-        fb.run_packed(pc, fb.out_c, fb.out_x)
-        evs[k][1].record()
-    torch.cuda.synchronize(dev)
-    ms_tuned = sum(a.elapsed_time(b) for a, b in evs) / steps
-    sched = fb.schedule()
+    ms_tuned, sched = None, fb.schedule()
+    if autotune:
+        # the same builds after the batch autotuner picked each class's variant on them
+        fb.autotune(pc)
+        for k in range(steps):
+            flush.fill_(float(k))
+            evs[k][0].record()
+            fb.run_packed(pc, fb.out_c, fb.out_x)
+            evs[k][1].record()
+        torch.cuda.synchronize(dev)
+        ms_tuned = sum(a.elapsed_time(b) for a, b in evs) / steps
+        sched = fb.schedule()
     fb.close()
 
     # plain: the reference's loop with full FP64 builds, one molecule after another
@@ -303,6 +305,7 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
     lg = guess.LearnedGuess.load(guess.MODEL, device=dev)
     runs = {}
     for name, opts in (('batched', batch_scf.BatchOptions()),
+                       ('batched+learned', batch_scf.BatchOptions(guess=lg)),
                        ('batched+learned+mixed', batch_scf.BatchOptions(guess=lg, mixed_cutoff=1e-6))):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
@@ -328,7 +331,8 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int):
             'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
             'launches_per_build': int(cen['kernel_launches']),
             'build_ms_autotuned': ms_tuned,
-            'autotuned_variants': {x['cls']: x['variant'] for x in sched},
+            'variants': {x['cls']: x['variant'] for x in sched},
+            'schedule': 'autotuned on the batch' if autotune else 'default table',
             'l2': 'flushed before every timed build (256 MiB write)',
             'scf': {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)), **runs,
                     'wall_clock': 'host time around each whole set, GPU synchronised; one-electron set-up excluded'}}
@@ -494,7 +498,7 @@ def main():
 
     batch = None
     if rank == 0 and world == 1 and args.batch > 0:
-        batch = batch_leg(args.batch, local, args.steps, args.warmup)
+        batch = batch_leg(args.batch, local, args.steps, args.warmup, args.autotune)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -48,8 +48,9 @@ class BatchOptions:
     """incremental / density_tol(_rel, _max) / mixed_cutoff / reset_every as in
     scf.FastOptions (per molecule, from its own density change);
     guess: 'nuclear' (the reference's GUESS_DENSITYMATRIX), 'core', or an object
-    with ``raw(sysm) -> np.ndarray`` giving an unpurified contracted density per
-    molecule (the learned guess), purified here on the GPU and judged by
+    with ``raw(sysm) -> np.ndarray`` (and optionally ``raw_many(systems)``)
+    giving an unpurified contracted density per molecule (the learned guess),
+    purified here on the GPU and judged by
     ``fallback_error`` (first DIIS error above it: restart from 'nuclear')."""
     incremental: bool = True
     density_tol: float = 1e-11
@@ -319,8 +320,9 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     elif learned:
         # occupied natural orbitals of the predicted density: the projector on the
         # nocc lowest eigenvectors of -D, D = P/2 in the orthonormal basis
+        raws = opts.guess.raw_many(ssys) if hasattr(opts.guess, 'raw_many') else [opts.guess.raw(s) for s in ssys]
         for kk in range(nmol):
-            fb.view(p, kk).copy_(torch.tensor(np.asarray(opts.guess.raw(ssys[kk])), **f64))
+            fb.view(p, kk).copy_(torch.tensor(np.asarray(raws[kk]), **f64))
         for g in groups:
             dm = 0.5 * g.ws @ g.view(p) @ g.ws.transpose(1, 2)
             pv, st, _ = _projector_density(g, -0.5 * (dm + dm.transpose(1, 2)), opts)

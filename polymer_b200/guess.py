@@ -92,12 +92,13 @@ def ao_info(sysm: System) -> AOInfo:
     return AOInfo(live, atom, powers, groups, atom_funcs)
 
 
-def frame_transform(info: AOInfo, R: np.ndarray, funcs: List[int]) -> np.ndarray:
+def frame_transform(info: AOInfo, R: np.ndarray, funcs: List[int], qcache: Optional[dict] = None) -> np.ndarray:
     """U (len(funcs) x len(funcs)) with P_frame = U^T P_lab U for the functions
-    `funcs` (whole shell instances), R mapping frame vectors to lab vectors."""
+    `funcs` (whole shell instances), R mapping frame vectors to lab vectors;
+    `qcache` keeps the monomial transforms of R per degree across calls."""
     idx = {f: k for k, f in enumerate(funcs)}
     u = np.zeros((len(funcs), len(funcs)))
-    cache = {}
+    cache = qcache if qcache is not None else {}
     for g in info.groups:
         if g[0] not in idx:
             continue
@@ -135,41 +136,73 @@ def _type(z: int) -> np.ndarray:
 
 def pair_list(sysm: System):
     """(A, B, owner water) of every predicted block: all pairs inside a water and
-    pairs closer than R_CUT, each in the frame of A's water."""
+    pairs closer than R_CUT, each in the frame of A's water (A outer, B inner)."""
     d = sysm.deck
     xyz = np.array(d.coords)
-    pairs = []
-    for a in range(d.natom):
-        for b in range(d.natom):
-            if a // 3 == b // 3 or np.linalg.norm(xyz[a] - xyz[b]) < R_CUT:
-                pairs.append((a, b, a // 3))
-    return pairs
+    w = np.arange(d.natom) // 3
+    dist = np.linalg.norm(xyz[:, None, :] - xyz[None, :, :], axis=2)
+    a, b = np.nonzero((w[:, None] == w[None, :]) | (dist < R_CUT))
+    return [(int(i), int(j), int(i) // 3) for i, j in zip(a, b)]
 
 
 def features(sysm: System, frames, pairs) -> np.ndarray:
+    """Per pair (A, B): the types of A and B, B - A in the frame (/4 bohr), its
+    length, same-water flag, then the NEIGHBOURS atoms nearest A (other than A
+    and B), each as type, offset from A in the frame (/8 bohr) and inverse
+    distance; missing neighbours are zero."""
     d = sysm.deck
     xyz = np.array(d.coords)
-    z = d.atoms
-    out = np.zeros((len(pairs), NFEAT))
-    for k, (a, b, m) in enumerate(pairs):
-        o, R, _ = frames[m]
-        rel = R.T @ (xyz[b] - xyz[a])
-        f = [*_type(z[a]), *_type(z[b]), *(rel / 4.0), np.linalg.norm(rel) / 4.0, 1.0 if a // 3 == b // 3 else 0.0]
-        dist = np.linalg.norm(xyz - xyz[a], axis=1)
-        order = [c for c in np.argsort(dist) if c != a and c != b][:NEIGHBOURS]
-        env = []
-        for c in order:
-            rc = R.T @ (xyz[c] - xyz[a])
-            env += [*_type(z[c]), *(rc / 8.0), 1.0 / max(np.linalg.norm(rc), 1e-6)]
-        env += [0.0] * (6 * NEIGHBOURS - len(env))
-        out[k] = np.array(f + env)
+    z = np.array(d.atoms)
+    npair = len(pairs)
+    out = np.zeros((npair, NFEAT))
+    if npair == 0:
+        return out
+    A = np.array([q[0] for q in pairs])
+    B = np.array([q[1] for q in pairs])
+    R = np.stack([fr[1] for fr in frames])[np.array([q[2] for q in pairs])]
+    typ = np.where((z == 8)[:, None], np.array([1.0, 0.0]), np.array([0.0, 1.0]))
+    rel = np.einsum('pji,pj->pi', R, xyz[B] - xyz[A])
+    out[:, 0:2] = typ[A]
+    out[:, 2:4] = typ[B]
+    out[:, 4:7] = rel / 4.0
+    out[:, 7] = np.linalg.norm(rel, axis=1) / 4.0
+    out[:, 8] = (A // 3 == B // 3)
+    # neighbours of A by distance (each row sorted on its own, as np.argsort of that row)
+    order = np.argsort(np.linalg.norm(xyz[:, None, :] - xyz[None, :, :], axis=2), axis=1)[A]
+    keep = (order != A[:, None]) & (order != B[:, None])
+    pos = np.argsort(~keep, axis=1, kind='stable')[:, :NEIGHBOURS]
+    sel = np.take_along_axis(order, pos, 1)
+    ok = np.take_along_axis(keep, pos, 1)
+    rc = np.einsum('pji,pcj->pci', R, xyz[sel] - xyz[A][:, None, :])
+    env = np.concatenate([typ[sel], rc / 8.0, (1.0 / np.maximum(np.linalg.norm(rc, axis=2), 1e-6))[..., None]], axis=2)
+    env *= ok[..., None]
+    out[:, 9:9 + 6 * sel.shape[1]] = env.reshape(npair, -1)
     return out
 
 
-def _u_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
-    key = (a, id(R))
+def _layout(info: AOInfo, a: int, cache: dict):
+    """Atom a's functions as (shell instances by relative index, powers): atoms
+    with equal layouts share their frame transforms."""
+    key = ('layout', a)
     if key not in cache:
-        cache[key] = frame_transform(info, R, info.atom_funcs[a])
+        funcs = info.atom_funcs[a]
+        idx = {f: k for k, f in enumerate(funcs)}
+        cache[key] = (tuple(tuple(idx[i] for i in g) for g in info.groups if g[0] in idx),
+                      tuple(info.powers[f] for f in funcs))
+    return cache[key]
+
+
+def _u_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
+    key = (_layout(info, a, cache), id(R))
+    if key not in cache:
+        cache[key] = frame_transform(info, R, info.atom_funcs[a], cache.setdefault(('q', id(R)), {}))
+    return cache[key]
+
+
+def _v_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
+    key = ('inv', _layout(info, a, cache), id(R))
+    if key not in cache:
+        cache[key] = np.linalg.inv(_u_for_atom(info, R, a, cache))
     return cache[key]
 
 
@@ -193,22 +226,27 @@ def targets(sysm: System, info: AOInfo, frames, pairs, p_c: np.ndarray) -> Tuple
 
 
 def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.ndarray:
-    """Laboratory contracted density from predicted frame blocks (symmetrised)."""
+    """Laboratory contracted density from predicted frame blocks (symmetrised:
+    each block enters at (A,B) and, transposed, at (B,A); entries are averaged)."""
     n = sysm.basis.ncgs
     acc = np.zeros((n, n))
     cnt = np.zeros((n, n))
     cache: dict = {}
+    by_shape: Dict[tuple, List[int]] = {}
     for k, (a, b, m) in enumerate(pairs):
-        R = frames[m][1]
-        fa, fb = info.atom_funcs[a], info.atom_funcs[b]
-        va = np.linalg.inv(_u_for_atom(info, R, a, cache))
-        vb = np.linalg.inv(_u_for_atom(info, R, b, cache))
-        blk = pred[k].reshape(MAXF, MAXF)[:len(fa), :len(fb)]
-        lab = va.T @ blk @ vb
-        acc[np.ix_(fa, fb)] += lab
-        cnt[np.ix_(fa, fb)] += 1.0
-        acc[np.ix_(fb, fa)] += lab.T
-        cnt[np.ix_(fb, fa)] += 1.0
+        by_shape.setdefault((len(info.atom_funcs[a]), len(info.atom_funcs[b])), []).append(k)
+    for (na, nb), ks in by_shape.items():
+        va = np.stack([_v_for_atom(info, frames[pairs[k][2]][1], pairs[k][0], cache) for k in ks])
+        vb = np.stack([_v_for_atom(info, frames[pairs[k][2]][1], pairs[k][1], cache) for k in ks])
+        blk = pred[ks].reshape(-1, MAXF, MAXF)[:, :na, :nb]
+        lab = np.einsum('kia,kab->kib', va.transpose(0, 2, 1), np.einsum('kij,kjb->kib', blk, vb))
+        rows = np.array([info.atom_funcs[pairs[k][0]] for k in ks])
+        cols = np.array([info.atom_funcs[pairs[k][1]] for k in ks])
+        r, c = rows[:, :, None], cols[:, None, :]
+        np.add.at(acc, (r, c), lab)
+        np.add.at(cnt, (r, c), 1.0)
+        np.add.at(acc, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), lab.transpose(0, 2, 1))
+        np.add.at(cnt, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), 1.0)
     return np.where(cnt > 0, acc / np.maximum(cnt, 1.0), 0.0)
 
 
@@ -299,14 +337,24 @@ class LearnedGuess:
 
     def predict_blocks(self, x: np.ndarray) -> np.ndarray:
         out = []
-        for i in range(0, len(x), 4096):
-            out.append(self.net.forward(torch.tensor(x[i:i + 4096], dtype=torch.float32)).double().cpu().numpy())
-        return np.concatenate(out)
+        for i in range(0, len(x), 16384):
+            out.append(self.net.forward(torch.tensor(x[i:i + 16384], dtype=torch.float32)).double())
+        return torch.cat(out).cpu().numpy()
 
     def raw(self, sysm: System) -> np.ndarray:
         """The assembled (unpurified) contracted density of the prediction."""
         info, frames, pairs, x = cluster_data(sysm)
         return assemble(sysm, info, frames, pairs, self.predict_blocks(x))
+
+    def raw_many(self, systems) -> List[np.ndarray]:
+        """raw() of several molecules with one network evaluation over all their blocks."""
+        data = [cluster_data(s) for s in systems]
+        pred = self.predict_blocks(np.concatenate([d[3] for d in data]))
+        out, o = [], 0
+        for s, (info, frames, pairs, x) in zip(systems, data):
+            out.append(assemble(s, info, frames, pairs, pred[o:o + len(pairs)]))
+            o += len(pairs)
+        return out
 
     def __call__(self, sysm: System, st) -> torch.Tensor:
         info, frames, pairs, x = cluster_data(sysm)
