@@ -238,7 +238,7 @@ def run_reference(args):
     return 0
 
 
-def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: bool = False):
+def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: bool = False, scf_runs: bool = True):
     """Uneven water clusters (cc-pVDZ, k ~ U{1..16} as geometry.water_batch_decks
     draws them) as one batch: batched full FP64 Fock builds per second, and the
     time to converged SCF of the whole set -- one plain FP64 GPU SCF per molecule
@@ -289,6 +289,19 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
         sched = fb.schedule()
     fb.close()
 
+    out = {'workload': '%d water clusters, cc-pVDZ, k ~ U{1..16} (seed 2000, cluster i from seed 2001+i), '
+                       'INTTOL 1e-10' % n_clusters,
+           'molecules': n_clusters, 'ncgs_total': int(sum(s.basis.ncgs for s in systems)),
+           'systems_s': t_sys, 'batch_setup_s': t_setup,
+           'build_ms': ms, 'builds_per_s': 1000.0 / ms, 'quartets_per_build': cen['quartets'],
+           'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
+           'launches_per_build': int(cen['kernel_launches']),
+           'build_ms_autotuned': ms_tuned,
+           'variants': {x['cls']: x['variant'] for x in sched},
+           'schedule': 'autotuned on the batch' if autotune else 'default table',
+           'l2': 'flushed before every timed build (256 MiB write)'}
+    if not scf_runs:
+        return out
     # plain: the reference's loop with full FP64 builds, one molecule after another
     e_plain, it_plain = [], []
     torch.cuda.synchronize(dev)
@@ -323,19 +336,9 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
                                   'mixed_cutoff': opts.mixed_cutoff, 'reset_every': opts.reset_every,
                                   'guess': opts.guess if isinstance(opts.guess, str) else 'learned',
                                   'cuda_graph': 'each iteration from the third on is one graph replay'}}
-    return {'workload': '%d water clusters, cc-pVDZ, k ~ U{1..16} (seed 2000, cluster i from seed 2001+i), '
-                        'INTTOL 1e-10' % n_clusters,
-            'molecules': n_clusters, 'ncgs_total': int(sum(s.basis.ncgs for s in systems)),
-            'systems_s': t_sys, 'batch_setup_s': t_setup,
-            'build_ms': ms, 'builds_per_s': 1000.0 / ms, 'quartets_per_build': cen['quartets'],
-            'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
-            'launches_per_build': int(cen['kernel_launches']),
-            'build_ms_autotuned': ms_tuned,
-            'variants': {x['cls']: x['variant'] for x in sched},
-            'schedule': 'autotuned on the batch' if autotune else 'default table',
-            'l2': 'flushed before every timed build (256 MiB write)',
-            'scf': {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)), **runs,
-                    'wall_clock': 'host time around each whole set, GPU synchronised; one-electron set-up excluded'}}
+    out['scf'] = {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)), **runs,
+                  'wall_clock': 'host time around each whole set, GPU synchronised; one-electron set-up excluded'}
+    return out
 
 
 def main():
@@ -348,6 +351,8 @@ def main():
     ap.add_argument('--no-scf', action='store_true', help='skip the time-to-converged SCF leg')
     ap.add_argument('--batch', type=int, default=32,
                     help='water clusters in the batched leg (0: skip it)')
+    ap.add_argument('--no-batch-scf', action='store_true',
+                    help='batched leg: the batched builds only, no SCF of the set')
     ap.add_argument('--autotune', action='store_true',
                     help='time every kernel variant per quartet class and keep the fastest '
                          '(default: the library\'s measured schedule table)')
@@ -498,7 +503,7 @@ def main():
 
     batch = None
     if rank == 0 and world == 1 and args.batch > 0:
-        batch = batch_leg(args.batch, local, args.steps, args.warmup, args.autotune)
+        batch = batch_leg(args.batch, local, args.steps, args.warmup, args.autotune, not args.no_batch_scf)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

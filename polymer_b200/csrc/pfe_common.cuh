@@ -37,22 +37,42 @@ void set_error(const std::string& msg);
 static __constant__ const double c_TF[22] = {33, 37, 41, 43, 46, 49, 51, 54, 56, 58, 61,
                                              63, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84};
 
+// Doubles of one IGAMMA row a Boys evaluation of orders 0..L reads (L+7 rounded
+// up to even: whole 16-byte loads; rows are 28 doubles, so this stays inside one).
+template <int L>
+struct BoysRow {
+  static constexpr int NV = (L + 8) / 2;
+  static constexpr int N = 2 * NV;
+};
+
+// Gather the IGAMMA row nearest T (row-major [T][m], 16-byte aligned rows); the
+// index is clamped to the table so a row can be fetched before knowing whether
+// the Taylor branch will read it.
+template <int L>
+__device__ __forceinline__ void boys_row(double T, const double* __restrict__ tab, double* __restrict__ gv) {
+  int ts = (int)floor(T * 20.0 + 0.5);
+  ts = ts < NIG_T - 1 ? ts : NIG_T - 1;
+  const double2* g2 = reinterpret_cast<const double2*>(tab + ts * NIG_M);
+#pragma unroll
+  for (int k = 0; k < BoysRow<L>::NV; ++k) {
+    const double2 v = __ldg(g2 + k);
+    gv[2 * k] = v.x;
+    gv[2 * k + 1] = v.y;
+  }
+}
+
 // F_m(T)*pref for m = 0..L exactly as the reference evaluates it
 // (src/pfourindexdirect.f90:543-553): below TF(m) a 6-term Taylor series about
-// the nearest tabulated point of IGAMMA (row-major [T][m] here), above it the
-// asymptotic form.  The asymptotic power T^(-m-1/2) is formed as
+// the nearest tabulated point of IGAMMA (its row gv, from boys_row), above it
+// the asymptotic form.  The asymptotic power T^(-m-1/2) is formed as
 // rsqrt(T)*(1/T)^m instead of exp((-m-1/2) log T): same function, rounding
 // differs in the last bit.
 template <int L>
-__device__ __forceinline__ void boys_tab(double T, double pref, const double* __restrict__ tab,
-                                         double* __restrict__ F) {
+__device__ __forceinline__ void boys_eval(double T, double pref, const double* __restrict__ gv,
+                                          double* __restrict__ F) {
   if (T < c_TF[L]) {
     const int ts = (int)floor(T * 20.0 + 0.5);  // NINT for T >= 0
     const double h = 0.05 * (double)ts - T;
-    const double* g = tab + ts * NIG_M;
-    double gv[L + 7];
-#pragma unroll
-    for (int k = 0; k < L + 7; ++k) gv[k] = __ldg(g + k);
 #pragma unroll
     for (int m = 0; m <= L; ++m) {
       if (T < c_TF[m]) {
@@ -76,6 +96,15 @@ __device__ __forceinline__ void boys_tab(double T, double pref, const double* __
       F[m] = v;
     }
   }
+}
+
+// Both steps; the row is read only on the Taylor branch.
+template <int L>
+__device__ __forceinline__ void boys_tab(double T, double pref, const double* __restrict__ tab,
+                                         double* __restrict__ F) {
+  double gv[BoysRow<L>::N];
+  if (T < c_TF[L]) boys_row<L>(T, tab, gv);
+  boys_eval<L>(T, pref, gv, F);
 }
 
 }  // namespace pfe
