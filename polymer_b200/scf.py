@@ -335,7 +335,8 @@ def variational_energy(st: HostState, fock, p_c: torch.Tensor, eps, mu) -> Tuple
 def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.ndarray] = None,
             max_cycles: Optional[int] = None, scfconv: Optional[float] = None,
             log: Optional[Callable[[str], None]] = None, raise_on_fail: bool = True,
-            fast: Optional[FastOptions] = None, variational: bool = False) -> SCFResult:
+            fast: Optional[FastOptions] = None, variational: bool = False,
+            chk: Optional[str] = None) -> SCFResult:
     """SELF_CONSISTENT_FIELD with the Fock build supplied by ``fock``.
 
     ``fock(P_P, P_P_HELIX)`` maps cell-major primitive densities to cell-major
@@ -345,14 +346,27 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
     and the J/K of the previous one; ``variational`` adds E[P] of the density of
     the last diagonalisation (idempotent, so E[P] is second order in its error)
     with its own full FP64 J/K: one more build, the energy two runs are compared by.
+    ``chk``: the reference's JOBNAME.chk (polymer_b200/chk.py): the initial
+    density is restored from it when it holds a compatible block
+    (RESTORE_DENSITYMATRIX at SINGLEPOINT; otherwise the guess), and every
+    iteration's block is written to it as STORE_DENSITYMATRIX does, so the
+    Fortran driver can resume from this run and this run from the driver's.
     """
     t0 = time.perf_counter()
     d = sysm.deck
     st = HostState(sysm, device)
     if fast is not None and (sysm.ncell1 != 1 or not hasattr(fock, 'from_pc')):
         raise SCFError('the fast SCF options need a molecule and a device Fock builder')
+    restored = None
+    if chk is not None and p_c0 is None:
+        from . import chk as chk_mod
+        restored, msg = chk_mod.restore(chk, sysm.basis.ncgs, d.cel1)
+        if log:
+            log(msg)
     if p_c0 is not None:
         p_c = torch.tensor(p_c0, dtype=torch.float64, device=st.device)
+    elif restored is not None:
+        p_c = torch.tensor(restored, dtype=torch.float64, device=st.device)
     elif fast is not None and fast.guess == 'core':
         p_c = core_guess(st)
     elif fast is not None and callable(fast.guess):
@@ -409,6 +423,9 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
         dchg = math.sqrt(pulay[iscf, iscf] / denom)
         hist_in.append(p_c.clone())
         hist_d.append(dp.clone())
+        if chk is not None:
+            from . import chk as chk_mod
+            chk_mod.store(chk, iscf, p_c.cpu().numpy(), p_out.cpu().numpy(), d.cel1, pulay=False)
         if d.diis != 0 and iscf >= d.diis and (iscf - d.diis) % 2 == 0:
             iterm = min(8, iscf)
             bm = np.zeros((iterm + 1, iterm + 1))
