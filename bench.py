@@ -142,23 +142,30 @@ def ncu_traffic_per_launch():
 
 
 def cpu_baseline(sysm, p_p_np, budget_s: float = 15.0):
-    """Oracle on bra shells I = 0 (mod stride), extrapolated to a full build, 1 thread."""
+    """Oracle on bra shells I = 0 (mod stride), extrapolated to a full build, 1 thread.
+
+    The cost per bra shell varies by orders of magnitude (s shells against d
+    shells), so the stride is sized from a first sample spread over the whole
+    shell list (every n/8-th shell), not from one shell."""
     import oracle
     n = sysm.basis.npshell
     t0 = time.perf_counter()
     oracle.fourindex_eri_sample(sysm, p_p_np, n + 1, n)   # no bra shell: the fixed KL/Schwarz part
     t_fixed = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    oracle.fourindex_eri_sample(sysm, p_p_np, n, 0)       # one bra shell
-    t_one = time.perf_counter() - t0 - t_fixed
-    per = max(t_one, 1e-3)
-    nsamp = max(1, min(n, int((budget_s - t_fixed) / per)))
-    stride = max(1, n // nsamp)
-    t0 = time.perf_counter()
-    oracle.fourindex_eri_sample(sysm, p_p_np, stride, 0)
-    t_s = time.perf_counter() - t0
-    sampled = len(range(0, n, stride))
-    t_full = t_fixed + (t_s - t_fixed) * n / sampled
+
+    def sample(stride):
+        t = time.perf_counter()
+        oracle.fourindex_eri_sample(sysm, p_p_np, stride, 0)
+        return time.perf_counter() - t - t_fixed, len(range(0, n, stride))
+
+    stride = max(1, n // 8)
+    t_s, sampled = sample(stride)
+    per = max(t_s, 1e-6) / sampled                 # mean seconds per bra shell
+    want = int(max(1.0, (budget_s - t_fixed) / per))
+    if want > sampled:
+        stride = max(1, -(-n // want))
+        t_s, sampled = sample(stride)
+    t_full = t_fixed + max(t_s, 0.0) * n / sampled
     return {'value': 1.0 / t_full, 'unit': 'Fock builds/s', 'cores': 1, 'kind': 'port',
             'sample': 'oracle FOURINDEX_ERI restatement over bra shells I = 0 mod %d (%d of %d), '
                       'extrapolated: %.1f s per full build' % (stride, sampled, n, t_full),
