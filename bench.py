@@ -366,7 +366,7 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     t_main = time.perf_counter()
-    walls = {}
+    legs = {}
     if args.impl == 'reference':
         return run_reference(args)
 
@@ -485,7 +485,7 @@ def main():
     # ---- time to a converged SCF (1e-8 RMS density): the reference's loop with full FP64
     # builds against the time-to-solution path (commutator DIIS, incremental density-screened
     # builds), both judged by E[P] of the final idempotent density with full FP64 J/K
-    walls['build_leg_s'] = time.perf_counter() - t_main
+    legs['build_leg_s'] = time.perf_counter() - t_main
     t_leg = time.perf_counter()
     scf_line = None
     if rank == 0 and world == 1 and not args.no_scf:
@@ -512,19 +512,19 @@ def main():
                     'plain_path': "reference loop (nuclear-charge guess, density DIIS), full FP64 builds",
                     'wall_clock': 'host time around each SCF, GPU synchronised'}
 
-    walls['scf_leg_s'] = time.perf_counter() - t_leg
+    legs['scf_leg_s'] = time.perf_counter() - t_leg
     t_leg = time.perf_counter()
     batch = None
     if rank == 0 and world == 1 and args.batch > 0:
         batch = batch_leg(args.batch, local, args.steps, args.warmup, args.autotune, not args.no_batch_scf)
-    walls['batch_leg_s'] = time.perf_counter() - t_leg
+    legs['batch_leg_s'] = time.perf_counter() - t_leg
     t_leg = time.perf_counter()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(sysm, p_p.cpu().numpy())
-    walls['cpu_baseline_s'] = time.perf_counter() - t_leg
-    walls['total_s'] = time.perf_counter() - t_main
+    legs['cpu_baseline_s'] = time.perf_counter() - t_leg
+    legs['total_s'] = time.perf_counter() - t_main
 
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': 'Fock builds/s', 'n_gpus': world, 'steps': args.steps,
@@ -539,7 +539,7 @@ def main():
                 'quartets_per_build': cen['quartets'], 'quartets_per_s': cen['quartets'] * value,
                 'gpu_launches': args.steps * int(cen['kernel_launches']),
                 'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'scf': scf_line,
-                'batch': batch, 'cpu_baseline': cpu, 'wall_clock_s': walls}
+                'batch': batch, 'cpu_baseline': cpu, 'wall_clock_s': legs}
         print(json.dumps(line))
     df.close()
     if world > 1:
