@@ -134,3 +134,37 @@ def test_malformed_shell_map_is_rejected(water):
     import ctypes
     rc = L.pfe_fourindex_eri(ctypes.byref(a), capi.dptr(c), capi.dptr(x))
     assert rc == -1 and 'cumulative' in capi.last_error(L)
+
+
+def _zero_onee(sysm):
+    n = sysm.basis.npgs
+    z = np.zeros((sysm.ncell1, n, n))
+    return z, z.copy(), z.copy()
+
+
+def test_f_shells_are_refused():
+    # cc-pVDZ with an f polarization shell added on oxygen (P_SHELL_ANG = 3): the
+    # kernels stop at d and the C ABI says so
+    from polymer_b200 import basis
+    lib = {k: list(v) for k, v in basis.load_basis_library('cc-pVDZ').items()}
+    lib['O'] = lib['O'] + [['F', 1.0, [[1.428, 1.0]]]]
+    s = system.build_system(geometry.water_deck(1, seed=1), _zero_onee, library=lib)
+    assert int(np.max(s.basis.p_shell_ang)) == 3
+    n = s.basis.npgs
+    with pytest.raises(capi.FockError) as e:
+        fock.fourindex_eri(s, np.zeros((1, n, n)))
+    assert e.value.code == -3
+
+
+def test_helix_in_more_than_one_dimension_is_refused():
+    # the reference's 'HELICAL SYMMETRY FOR 1D CRYSTAL ONLY'
+    s = system.build_system(geometry.polyethylene_deck('STO-3G', cutoff1=1, cutoff2=1, kpoints=2), oracle.onee)
+    n = s.basis.npgs
+    pp = np.zeros((s.ncell1, n, n))
+    a, keep = s.pfe_args(pp, np.zeros_like(pp))
+    a.cel1[1] = 1
+    c = np.zeros(s.basis.ncgs ** 2 * s.ncell1 * 3)
+    x = np.zeros_like(c)
+    import ctypes
+    L = capi.lib()
+    assert L.pfe_fourindex_eri(ctypes.byref(a), capi.dptr(c), capi.dptr(x)) == -1
