@@ -437,8 +437,8 @@ def main():
     stats = (capi.PfeKernelStat * 64)()
     nst = L.pfe_context_kernel_stats(df.ctx, stats, 64)
     capi.check(L, L.pfe_context_profile(df.ctx, 0))
-    kern = [{'cls': '%04d' % s.cls, 'variant': s.variant, 'ms': s.ms, 'tuned_ms': list(s.tuned_ms),
-             'quartets': s.quartets, 'flops': s.flops} for s in stats[:max(nst, 0)]]
+    kern = [{'cls': '%04d' % s.cls, 'variant': s.variant, 'grid_mult': s.grid_mult, 'ms': s.ms,
+             'tuned_ms': list(s.tuned_ms), 'quartets': s.quartets, 'flops': s.flops} for s in stats[:max(nst, 0)]]
     tot_ms = sum(k['ms'] for k in kern) or 1.0
     dom = max(kern, key=lambda k: k['ms']) if kern else None
     peak = measure_fp64_peak(local)

@@ -182,6 +182,8 @@ typedef struct pfe_kernel_stat {
   float tuned_ms[3];  /* autotuner timing of each variant, 0 where not run */
   double quartets;
   double flops;
+  int32_t grid_mult;  /* straight-line variant: blocks per SM of its persistent grid */
+  int32_t pad_;
 } pfe_kernel_stat;
 int32_t pfe_context_kernel_stats(pfe_context *ctx, pfe_kernel_stat *out, int32_t cap);
 /* A batch's quartet classes and their schedule (see pfe_batch_autotune). */

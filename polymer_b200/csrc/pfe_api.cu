@@ -611,6 +611,8 @@ int32_t pfe_batch_schedule(pfe_batch* b, pfe_kernel_stat* out, int32_t cap) {
     out[n].ms = 0.f;
     out[n].quartets = cl.quartets;
     out[n].flops = cl.quartets * class_flops(cl.cb, cl.ck);
+    out[n].grid_mult = cl.gmul;
+    out[n].pad_ = 0;
   }
   return n;
 }
@@ -705,6 +707,8 @@ int32_t pfe_context_kernel_stats(pfe_context* ctx, pfe_kernel_stat* out, int32_t
     out[n].ms = ms;
     out[n].quartets = ctx->ev_quartets[i];
     out[n].flops = ctx->ev_flops[i];
+    out[n].grid_mult = ctx->ev_gmul[i];
+    out[n].pad_ = 0;
   }
   return n;
 }

@@ -55,6 +55,7 @@ struct ClassLaunch {
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
   double* xg;                // block variant: per-block X scratch in global memory, or null
   int npass;                 // launches of the straight-line variant
+  int gmul = 32;             // straight-line variant: persistent grid of up to gmul blocks per SM
 };
 
 }  // namespace pfe
@@ -143,6 +144,7 @@ struct pfe_context {
   int ev_variant[64] = {0};
   float ev_tuned[64][3] = {};
   double ev_quartets[64] = {0}, ev_flops[64] = {0};
+  int ev_gmul[64] = {0};
   int nprof = 0;
 
   std::vector<void*> owned;    // freed on reset/destroy

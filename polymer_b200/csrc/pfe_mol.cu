@@ -809,6 +809,7 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
       PFE_CUDA(cudaStreamSynchronize(s));
       if (total == 0) continue;
       ClassLaunch cl{};
+      cl.gmul = 32;   // what the autotuner picks for most classes on C20H42 and the water batch
       cl.cb = cb;
       cl.ck = ck;
       cl.nchunks_host = total;
@@ -918,7 +919,7 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
   ql.nchunks = cl.d_nchunks;
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
   if ((variant == 0 && cl.has_straight) || !cl.has_table) {
-    const int grid = std::min((work + 3) / 4, ctx->num_sms * 16);
+    const int grid = std::min((work + 3) / 4, ctx->num_sms * cl.gmul);
     straight_launcher(cl.cb, cl.ck, mixed, ql.insts != nullptr)(ql, std::max(grid, 1), s);
     return;
   }
@@ -953,6 +954,42 @@ static bool variant_ok(const ClassLaunch& cl, int v) {
   return cl.has_table;
 }
 
+// Time every execution variant of one class -- and, for the straight-line
+// variant, its persistent grid (4, 8, 16 or 32 blocks per SM) -- and keep the
+// fastest (best of two launches after one warm-up each).
+static int tune_class(pfe_context* ctx, ClassLaunch& cl, const MolLaunch& ql, cudaStream_t s, bool mixed,
+                      cudaEvent_t e0, cudaEvent_t e1) {
+  float best = 1e30f;
+  int bestv = cl.variant, bestg = cl.gmul;
+  for (int v = 0; v < 3; ++v) {
+    if (!variant_ok(cl, v)) continue;
+    static const int kGmul[4] = {4, 8, 16, 32};
+    const int ng = v == 0 ? 4 : 1;
+    float tv = 1e30f;
+    for (int gi = 0; gi < ng; ++gi) {
+      if (v == 0) cl.gmul = kGmul[gi];
+      launch_class(ctx, cl, ql, v, s, mixed);
+      float t = 1e30f;
+      for (int r = 0; r < 2; ++r) {
+        PFE_CUDA(cudaEventRecord(e0, s));
+        launch_class(ctx, cl, ql, v, s, mixed);
+        PFE_CUDA(cudaEventRecord(e1, s));
+        PFE_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        t = std::min(t, ms);
+      }
+      PFE_CUDA(cudaGetLastError());
+      tv = std::min(tv, t);
+      if (t < best) { best = t; bestv = v; bestg = cl.gmul; }
+    }
+    cl.tuned_ms[v] = tv;
+  }
+  cl.variant = bestv;
+  cl.gmul = bestg;
+  return PFE_OK;
+}
+
 int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
   const MolLaunch ql = make_launch(ctx, target_density(ctx, d_pp, s));
   PFE_CUDA(cudaGetLastError());
@@ -961,26 +998,8 @@ int autotune(pfe_context* ctx, const double* d_pp, cudaStream_t s) {
   PFE_CUDA(cudaEventCreate(&e1));
   for (int i = 0; i < ctx->nlaunch; ++i) {
     ClassLaunch& cl = ctx->launches[i];
-    float best = 1e30f;
-    int bestv = cl.variant;
-    for (int v = 0; v < 3; ++v) {
-      if (!variant_ok(cl, v)) continue;
-      launch_class(ctx, cl, ql, v, s, ctx->mcut > 0.0);
-      float t = 1e30f;
-      for (int r = 0; r < 2; ++r) {
-        PFE_CUDA(cudaEventRecord(e0, s));
-        launch_class(ctx, cl, ql, v, s, ctx->mcut > 0.0);
-        PFE_CUDA(cudaEventRecord(e1, s));
-        PFE_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        t = std::min(t, ms);
-      }
-      PFE_CUDA(cudaGetLastError());
-      cl.tuned_ms[v] = t;
-      if (t < best) { best = t; bestv = v; }
-    }
-    cl.variant = bestv;
+    const int rc = tune_class(ctx, cl, ql, s, ctx->mcut > 0.0, e0, e1);
+    if (rc != PFE_OK) return rc;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1026,6 +1045,7 @@ static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double*
       ctx->ev_cls[i] = 1000 * kCL[cl.cb][0] + 100 * kCL[cl.cb][1] + 10 * kCL[cl.ck][0] + kCL[cl.ck][1];
       ctx->ev_quartets[i] = cl.quartets;
       ctx->ev_flops[i] = cl.quartets * class_flops(cl.cb, cl.ck);
+      ctx->ev_gmul[i] = cl.gmul;
       ctx->ev_variant[i] = cl.variant;
       for (int v = 0; v < 3; ++v) ctx->ev_tuned[i][v] = cl.tuned_ms[v];
     }
@@ -1240,26 +1260,8 @@ int batch_autotune(pfe_batch* b, const double* d_pc, cudaStream_t s) {
   PFE_CUDA(cudaEventCreate(&e1));
   for (int i = 0; i < b->nlaunch; ++i) {
     ClassLaunch& cl = b->launches[i];
-    float best = 1e30f;
-    int bestv = cl.variant;
-    for (int v = 0; v < 3; ++v) {
-      if (!variant_ok(cl, v)) continue;
-      launch_class(c0, cl, lq, v, s, b->mixed);
-      float t = 1e30f;
-      for (int r = 0; r < 2; ++r) {
-        PFE_CUDA(cudaEventRecord(e0, s));
-        launch_class(c0, cl, lq, v, s, b->mixed);
-        PFE_CUDA(cudaEventRecord(e1, s));
-        PFE_CUDA(cudaEventSynchronize(e1));
-        float ms = 0.f;
-        PFE_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        t = std::min(t, ms);
-      }
-      PFE_CUDA(cudaGetLastError());
-      cl.tuned_ms[v] = t;
-      if (t < best) { best = t; bestv = v; }
-    }
-    cl.variant = bestv;
+    const int rc = tune_class(c0, cl, lq, s, b->mixed, e0, e1);
+    if (rc != PFE_OK) return rc;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

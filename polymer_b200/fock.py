@@ -226,8 +226,8 @@ class DeviceBatch:
         n = self.L.pfe_batch_schedule(self.handle, st, 64)
         if n < 0:
             check(self.L, n)
-        return [{'cls': '%04d' % x.cls, 'variant': x.variant, 'tuned_ms': list(x.tuned_ms),
-                 'quartets': x.quartets} for x in st[:n]]
+        return [{'cls': '%04d' % x.cls, 'variant': x.variant, 'grid_mult': x.grid_mult,
+                 'tuned_ms': list(x.tuned_ms), 'quartets': x.quartets} for x in st[:n]]
 
     def refresh(self, p_c: torch.Tensor) -> None:
         """Rewrite the launch records for densities packed in p_c with the current
