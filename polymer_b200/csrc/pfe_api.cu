@@ -432,16 +432,9 @@ int32_t pfe_context_create(int32_t device, pfe_context** out) {
   PFE_CUDA(cudaSetDevice(device));
   pfe_context* ctx = new pfe_context();
   ctx->device = device;
-  cudaDeviceProp prop;
-  PFE_CUDA(cudaGetDeviceProperties(&prop, device));
-  ctx->num_sms = prop.multiProcessorCount;
+  PFE_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
   PFE_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-  if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) {
-    set_error("cublasCreate failed");
-    delete ctx;
-    return PFE_ECUDA;
-  }
-  *out = ctx;
+  *out = ctx;   // the cuBLAS handle comes with the first call that needs it (ensure_blas)
   return PFE_OK;
 }
 

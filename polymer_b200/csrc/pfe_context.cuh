@@ -213,6 +213,16 @@ struct pfe_batch {
 };
 
 namespace pfe {
+// The context's cuBLAS handle, created on first use: molecules with contracted
+// targets never call cuBLAS, and a batch holds hundreds of contexts.
+inline bool ensure_blas(pfe_context* ctx) {
+  if (ctx->blas) return true;
+  if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) {
+    ctx->blas = nullptr;
+    return false;
+  }
+  return true;
+}
 int batch_setup(pfe_batch* b);
 int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
 int batch_refresh(pfe_batch* b, const double* d_pc);

@@ -7,6 +7,8 @@
 // on cuBLAS, and the FP64 peak probe.  The molecular path is pfe_mol.cu, the
 // lattice / helical path pfe_lattice.cu.
 
+#include <map>
+#include <mutex>
 #include <cublas_v2.h>
 
 #include <algorithm>
@@ -81,13 +83,26 @@ const OpTableHost* host_optable(int cb, int ck) {
   }
 }
 
-// Upload an op table once per context; returns the device view.
+// The op tables are immutable: each is uploaded once per device and shared by
+// every context on it (a batch holds hundreds of contexts).  The copies live as
+// long as the process.
+static std::mutex g_optable_mu;
+static std::map<std::pair<int, const OpTableHost*>, OpTableDev> g_optables;
+
+// The device view of an op table on the context's device (uploaded on first use).
 int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
+  std::lock_guard<std::mutex> lock(g_optable_mu);
+  const auto key = std::make_pair(ctx->device, h);
+  const auto it = g_optables.find(key);
+  if (it != g_optables.end()) {
+    *d = it->second;
+    return PFE_OK;
+  }
   unsigned short *ops = nullptr, *out = nullptr;
   int* lev = nullptr;
-  PFE_CUDA(ctx->alloc((void**)&ops, sizeof(unsigned short) * 8 * (h->nops + 1)));
-  PFE_CUDA(ctx->alloc((void**)&out, sizeof(unsigned short) * h->nout));
-  PFE_CUDA(ctx->alloc((void**)&lev, sizeof(int) * (h->nlevels + 1)));
+  PFE_CUDA(cudaMalloc((void**)&ops, sizeof(unsigned short) * 8 * (h->nops + 1)));
+  PFE_CUDA(cudaMalloc((void**)&out, sizeof(unsigned short) * (h->nout ? h->nout : 1)));
+  PFE_CUDA(cudaMalloc((void**)&lev, sizeof(int) * (h->nlevels + 1)));
   {  // 16-byte records: the six generated fields and two zero pads
     std::vector<unsigned short> rec((size_t)8 * (h->nops + 1), 0);
     for (int o = 0; o < h->nops; ++o)
@@ -102,6 +117,7 @@ int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   d->nlevels = h->nlevels;
   d->nout = h->nout;
   d->nslots = h->nslots;
+  g_optables[key] = *d;
   return PFE_OK;
 }
 
@@ -109,6 +125,7 @@ int contract_outputs(pfe_context* ctx, const double* jp, const double* kp, doubl
                      bool symmetrize, int ncell, cudaStream_t s) {
   const int np = ctx->npgs, nc = ctx->ncgs;
   const double one = 1.0, zero = 0.0;
+  if (!ensure_blas(ctx)) { set_error("cublasCreate failed"); return PFE_ECUDA; }
   cublasSetStream(ctx->blas, s);
   const double* src[2] = {jp, kp};
   double* dst[2] = {d_cc, d_xc};

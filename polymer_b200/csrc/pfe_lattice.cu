@@ -781,6 +781,7 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
     // C_C(:,:,q) <- C_C(:,:,q) C2H(:,:,q)^T along the screw axis (cells are x only)
     const int nc = ctx->ncgs, nx = 2 * ctx->cel1[0] + 1, h3 = ctx->cel2[0] + ctx->cel1[0];
     const double one = 1.0, zero = 0.0;
+    if (!ensure_blas(ctx)) { set_error("cublasCreate failed"); return PFE_ECUDA; }
     cublasSetStream(ctx->blas, s);
     double* outs[2] = {d_cc, d_xc};
     for (int o = 0; o < 2; ++o) {

@@ -1072,6 +1072,7 @@ int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double
   if (ctx->contracted) return run_build(ctx, d_pc, d_cc, d_xc, s);
   const int np = ctx->npgs, nc = ctx->ncgs;
   const double one = 1.0, zero = 0.0;
+  if (!ensure_blas(ctx)) { set_error("cublasCreate failed"); return PFE_ECUDA; }
   cublasSetStream(ctx->blas, s);
   // W1 = P_C . CC (nc x np); P_P = CC^T . W1 (np x np) into the target-density buffer
   cublasStatus_t st = cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, np, nc, &one, d_pc, nc, ctx->d_cc, nc, &zero,
@@ -1106,9 +1107,16 @@ __global__ void k_tag_chunks(int4* __restrict__ chunks, int n, int instance) {
   if (t < n) chunks[t].w = instance;
 }
 
-// Join the instances' chunk lists per (bra class, ket class).
+// Join the instances' chunk lists per (bra class, ket class): device copies and
+// tags queued on one stream, one synchronisation at the end.
 int batch_setup(pfe_batch* b) {
   b->nlaunch = 0;
+  cudaStream_t st = nullptr;
+  PFE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); } }
+  } guard{st};
   for (int cb = 0; cb < 6; ++cb)
     for (int ck = 0; ck <= cb; ++ck) {
       long long total = 0;
@@ -1126,15 +1134,16 @@ int batch_setup(pfe_batch* b) {
       cl.quartets = 0.0;
       PFE_CUDA(b->alloc((void**)&cl.chunks, sizeof(int4) * total));
       PFE_CUDA(b->alloc((void**)&cl.d_nchunks, sizeof(int)));
-      PFE_CUDA(cudaMemcpy(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice));
+      PFE_CUDA(cudaMemcpy(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice));   // pageable: synchronous
       long long o = 0;
       for (size_t k = 0; k < b->inst.size(); ++k) {
         pfe_context* c = b->inst[k];
         for (int i = 0; i < c->nlaunch; ++i) {
           const ClassLaunch& li = c->launches[i];
           if (li.cb != cb || li.ck != ck) continue;
-          PFE_CUDA(cudaMemcpy(cl.chunks + o, li.chunks, sizeof(int4) * li.nchunks_host, cudaMemcpyDeviceToDevice));
-          k_tag_chunks<<<(li.nchunks_host + 255) / 256, 256>>>(cl.chunks + o, li.nchunks_host, (int)k);
+          PFE_CUDA(cudaMemcpyAsync(cl.chunks + o, li.chunks, sizeof(int4) * li.nchunks_host, cudaMemcpyDeviceToDevice,
+                                   st));
+          k_tag_chunks<<<(li.nchunks_host + 255) / 256, 256, 0, st>>>(cl.chunks + o, li.nchunks_host, (int)k);
           PFE_CUDA(cudaGetLastError());
           o += li.nchunks_host;
           cl.quartets += li.quartets;
@@ -1148,6 +1157,7 @@ int batch_setup(pfe_batch* b) {
   b->insts_for = nullptr;
   b->mixed = false;
   for (pfe_context* c : b->inst) b->mixed = b->mixed || c->mcut > 0.0;
+  PFE_CUDA(cudaStreamSynchronize(st));
   PFE_CUDA(cudaDeviceSynchronize());
   return PFE_OK;
 }
@@ -1174,6 +1184,7 @@ static int batch_decontract(pfe_batch* b, const double* d_pc, cudaStream_t s) {
     if (c->contracted) continue;
     const int np = c->npgs, nc = c->ncgs;
     const double one = 1.0, zero = 0.0;
+    if (!ensure_blas(c)) { set_error("cublasCreate failed"); return PFE_ECUDA; }
     cublasSetStream(c->blas, s);
     if (cublasDgemm(c->blas, CUBLAS_OP_N, CUBLAS_OP_N, nc, np, nc, &one, d_pc + b->off[k], nc, c->d_cc, nc, &zero,
                     c->d_w1, nc) != CUBLAS_STATUS_SUCCESS ||
