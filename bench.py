@@ -329,11 +329,9 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
                        ('batched+learned+mixed', batch_scf.BatchOptions(guess=lg, mixed_cutoff=1e-6))):
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
-        b = fock.DeviceBatch(ssys, device)
-        res = batch_scf.run_batch_scf(systems, opts, batch=b, device=device, graph=True)
+        res = batch_scf.run_batch_scf(systems, opts, device=device, graph=True)   # builds (and frees) its batch
         torch.cuda.synchronize(dev)
         t = time.perf_counter() - t0
-        b.close()
         runs[name] = {'s': t, 'speedup_vs_plain': t_plain / t, 'builds': res.builds,
                       'iterations_mean': float(res.iterations.mean()), 'iterations_max': int(res.iterations.max()),
                       'converged': bool(res.converged.all()),
