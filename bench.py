@@ -250,7 +250,7 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
     draws them) as one batch: batched full FP64 Fock builds per second, and the
     time to converged SCF of the whole set -- one plain FP64 GPU SCF per molecule
     (the reference's loop, a DeviceFock each) against the batched SCF (set-up of
-    its DeviceBatch included), every molecule judged by E[P] of its final
+    its DeviceBatch included), every molecule compared by E[P] of its final
     idempotent density with full FP64 J/K."""
     import numpy as np
     import torch
@@ -482,7 +482,7 @@ def main():
 
     # ---- time to a converged SCF (1e-8 RMS density): the reference's loop with full FP64
     # builds against the time-to-solution path (commutator DIIS, incremental density-screened
-    # builds), both judged by E[P] of the final idempotent density with full FP64 J/K
+    # builds), both compared by E[P] of the final idempotent density with full FP64 J/K
     legs['build_leg_s'] = time.perf_counter() - t_main
     t_leg = time.perf_counter()
     scf_line = None

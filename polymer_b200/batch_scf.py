@@ -51,7 +51,7 @@ class BatchOptions:
     guess: 'nuclear' (the reference's GUESS_DENSITYMATRIX), 'core', or an object
     with ``raw(sysm) -> np.ndarray`` (and optionally ``raw_many(systems)``)
     giving an unpurified contracted density per molecule (the learned guess),
-    purified here on the GPU and judged by
+    purified here on the GPU and checked by
     ``fallback_error`` (first DIIS error above it: restart from 'nuclear')."""
     incremental: bool = True
     density_tol: float = 1e-11
@@ -495,7 +495,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 first[kk] = False
                 first_err[kk] = fe_k
                 if learned and fe_k > opts.fallback_error:
-                    # the learned guess is judged by the plain one: restart from the nuclear-charge guess
+                    # the learned guess is checked against the plain one: restart from the nuclear-charge guess
                     fallback[kk] = True
                     restart[kk] = True
                     have_ref[kk] = False

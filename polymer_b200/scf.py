@@ -145,7 +145,7 @@ class FastOptions:
     guess: 'nuclear' (the reference's), 'core', or a callable(System, HostState)
       returning a cell-major P_C tensor;
     final_full: once converged, one more iteration with a full FP64 build, whose
-      energy is reported (the fast path is judged by the plain method);
+      energy is reported (the fast path is checked against the plain method);
     fallback_error: with a callable guess, if max|FPS - SPF| of the first
       iteration exceeds it, the SCF restarts from the nuclear-charge guess.
     """
@@ -453,7 +453,7 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
                                                                    e - e_old if iscf > 1 else 0.0, it.seconds))
         if dchg < conv:
             if fast is not None and fast.final_full and not final_pending:
-                final_pending = True      # one more iteration on a full FP64 build judges the result
+                final_pending = True      # one more iteration on a full FP64 build checks the result
                 e_old = e
                 continue
             converged = True
@@ -554,7 +554,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
         e = float(vals[0]) + sysm.e_nuc
         fe = float(vals[1])
         if learned and iscf == 1 and fe > opts.fallback_error:
-            # the learned guess is judged by the plain one: restart from the nuclear-charge guess
+            # the learned guess is checked against the plain one: restart from the nuclear-charge guess
             fallback = True
             p_c = torch.tensor(guess_density(sysm), dtype=torch.float64, device=st.device)
             hist_f.clear()
