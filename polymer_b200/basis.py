@@ -152,7 +152,7 @@ def build_basis(deck: Deck, library: Optional[dict] = None) -> Basis:
                 raise ValueError('ANGULAR MOMENTUM NOT YET SUPPORTED: %s' % typ)
     nreal_pgs, nreal_cgs = len(zt), len(cgs)
     if nreal_pgs > 1024 or nreal_cgs > 1024:
-        # The reference caps both at 1024 (src/pread.f90:625,632); this build does
+        # The reference caps both at 1024 (src/pread.f90:625,632); this library does
         # not, but records the fact for callers comparing against it.
         pass
 

@@ -192,7 +192,7 @@ def parse(text: str) -> Deck:
         raise InputError('UNIT OF LENGTH MUST BE BOHR OR ANGSTROM')
     d.helix = d.helix * PI / 180.0
     # THEORY presets (src/pread.f90:309-374): HF forces HFEXCHANGE=1; the DFT
-    # presets need exchange-correlation code that is outside this build; any
+    # presets need exchange-correlation code that this package does not have; any
     # other name (e.g. MP2FC, a post-SCF method) sets no preset.
     if d.theory == 'HF':
         d.hfexchange = 1.0

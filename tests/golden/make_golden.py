@@ -11,7 +11,7 @@ is present) extracts, for every Hartree-Fock-relevant sample:
 * the converged energy components (nuclear repulsion, kinetic, nuclear
   attraction, Coulomb, HF exchange, total);
 * for the helical polyethylene sample, the per-cell maximum contracted overlap
-  and the nuclear repulsion (its SCF is B3LYP, outside this build).
+  and the nuclear repulsion (its SCF is B3LYP, which this package does not implement).
 
 Usage: python make_golden.py <reference-data-dir> [out.json]
 """
