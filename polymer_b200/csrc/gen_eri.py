@@ -166,7 +166,7 @@ class Gen:
 OPS_THRESHOLD = 1600  # classes with more integrals have no straight-line function (op tables only)
 
 
-def gen_optable(LA, LB, LC, LD):
+def gen_optable(LA, LB, LC, LD, pure_bra=False):
     """Level-scheduled op table of one class for the block-cooperative interpreter.
 
     Slot 0 holds zero, slots 1..L+1 the Boys values F[m]; every recursion node
@@ -238,7 +238,14 @@ def gen_optable(LA, LB, LC, LD):
         order.append(key)
         return key
 
-    outs = [hk(a, b, c, d) for a in comps(LA) for b in comps(LB) for c in comps(LC) for d in comps(LD)]
+    def kept(a, b):
+        # pure_bra: only the top-level components of the bra shells, for bra shells
+        # whose lower components carry no coefficient (the d shells of 6-31G** and
+        # cc-pVDZ); the other outputs read slot 0, which holds zero
+        return not pure_bra or ((LA == 0 or tot(a) == LA) and (LB == 0 or tot(b) == LB))
+
+    outs = [hk(a, b, c, d) if kept(a, b) else None
+            for a in comps(LA) for b in comps(LB) for c in comps(LC) for d in comps(LD)]
     level = {}
     for k in order:   # 'order' is a valid topological order (post-order)
         lv = 0
@@ -261,15 +268,15 @@ def gen_optable(LA, LB, LC, LD):
         lev_start[level[k] + 1] += 1
     for i in range(nlev):
         lev_start[i + 1] += lev_start[i]
-    out_slots = [slot[o] for o in outs]
+    out_slots = [slot[o] if o is not None else 0 for o in outs]
     nslots = base + len(sorted_keys)
     assert nslots < 65536
     return ops, lev_start, out_slots, nslots
 
 
-def emit_optable(LA, LB, LC, LD):
-    ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD)
-    name = 'op_%d%d%d%d' % (LA, LB, LC, LD)
+def emit_optable(LA, LB, LC, LD, pure_bra=False):
+    ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD, pure_bra)
+    name = 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure' if pure_bra else '')
     lines = ['// (%d%d|%d%d): %d ops in %d levels, %d slots' % (LA, LB, LC, LD, len(ops), len(lev) - 1, nslots)]
     flat = [v for op in ops for v in op] or [0] * 6
     lines.append('static const unsigned short %s_ops[%d] = {%s};' % (name, len(flat), ','.join(map(str, flat))))
@@ -344,6 +351,8 @@ def main():
                 continue   # the kernels put the higher pair class on the bra side
             n = ncomp_class = (len(comps(LA)) * len(comps(LB)) * len(comps(LC)) * len(comps(LD)))
             big.append(emit_optable(LA, LB, LC, LD))   # every class can run interpreted
+            if LA >= 1:
+                big.append(emit_optable(LA, LB, LC, LD, pure_bra=True))
             if n > OPS_THRESHOLD:
                 g = Gen(LA, LB, LC, LD)
                 g.build()

@@ -50,6 +50,10 @@ struct ClassLaunch {
   const int* levels;
   const unsigned short* out;
   int nlevels, nout, nslots;
+  const unsigned short* ops_p;   // pure-bra table (see OpTableDev), or null
+  const int* levels_p;
+  const unsigned short* out_p;
+  int nlevels_p;
   int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
   size_t smem_big, smem_warp;
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
@@ -241,6 +245,7 @@ int molecular_density_ok(pfe_context* ctx, cudaStream_t s, bool* ok);
 int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s);
 struct OpTableDev;
 const struct OpTableHost* host_optable(int cb, int ck);
+const struct OpTableHost* host_optable_pure(int cb, int ck);
 int upload_optable(pfe_context* ctx, const struct OpTableHost* h, OpTableDev* d);
 double class_flops(int cb, int ck);
 int lattice_setup(pfe_context* ctx, const pfe_args* a);

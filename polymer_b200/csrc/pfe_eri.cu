@@ -83,6 +83,35 @@ const OpTableHost* host_optable(int cb, int ck) {
   }
 }
 
+// The pure-bra variant of a class's table (bra classes with a p or d shell),
+// or null.
+const OpTableHost* host_optable_pure(int cb, int ck) {
+  switch (cb * 8 + ck) {
+    case 1 * 8 + 0: return &op_1000_pure;
+    case 1 * 8 + 1: return &op_1010_pure;
+    case 2 * 8 + 0: return &op_1100_pure;
+    case 2 * 8 + 1: return &op_1110_pure;
+    case 2 * 8 + 2: return &op_1111_pure;
+    case 3 * 8 + 0: return &op_2000_pure;
+    case 3 * 8 + 1: return &op_2010_pure;
+    case 3 * 8 + 2: return &op_2011_pure;
+    case 3 * 8 + 3: return &op_2020_pure;
+    case 4 * 8 + 0: return &op_2100_pure;
+    case 4 * 8 + 1: return &op_2110_pure;
+    case 4 * 8 + 2: return &op_2111_pure;
+    case 4 * 8 + 3: return &op_2120_pure;
+    case 4 * 8 + 4: return &op_2121_pure;
+    case 5 * 8 + 0: return &op_2200_pure;
+    case 5 * 8 + 1: return &op_2210_pure;
+    case 5 * 8 + 2: return &op_2211_pure;
+    case 5 * 8 + 3: return &op_2220_pure;
+    case 5 * 8 + 4: return &op_2221_pure;
+    case 5 * 8 + 5: return &op_2222_pure;
+    case 0: return nullptr;
+    default: return nullptr;
+  }
+}
+
 // The op tables are immutable: each is uploaded once per device and shared by
 // every context on it (a batch holds hundreds of contexts).  The copies live as
 // long as the process.

@@ -13,6 +13,13 @@ struct OpTableDev {
   const int* levels;
   const unsigned short* out;
   int nlevels, nout, nslots;
+  // the class's pure-bra variant (only the top-level components of the bra
+  // shells; at most nslots slots), or null: the molecular interpreter runs it
+  // for chunks whose bra shells have coefficient-free lower components
+  const unsigned short* ops_p;
+  const int* levels_p;
+  const unsigned short* out_p;
+  int nlevels_p;
 };
 
 // Geometry multipliers of the four op kinds, in shared memory.

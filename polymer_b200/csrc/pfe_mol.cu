@@ -422,6 +422,17 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
     for (int x = tid; x < NB; x += team) prm[DG::SB + x] = ql.stidx[J0 * MAXCOMP + x];
   }
   sync();
+  // bra shells whose lower components carry no coefficient (pure p or d) take
+  // the pure-bra table: the outputs it drops would be weighted by zero
+  bool pure = tab.ops_p != nullptr;
+  for (int x = 0; pure && x < NA; ++x)
+    if (comp_tot(LA, x) < LA && prm[x] >= 0) pure = false;
+  for (int x = 0; pure && x < NB; ++x)
+    if (comp_tot(LB, x) < LB && prm[DG::SB + x] >= 0) pure = false;
+  const unsigned short* __restrict__ t_ops = pure ? tab.ops_p : tab.ops;
+  const int* __restrict__ t_levels = pure ? tab.levels_p : tab.levels;
+  const unsigned short* __restrict__ t_out = pure ? tab.out_p : tab.out;
+  const int t_nlevels = pure ? tab.nlevels_p : tab.nlevels;
   for (int t = tid; t < NA * NB; t += team)
     P[DG::OAB + t] = dt_at(D, nt, prm[t / NB], prm[DG::SB + t % NB]);
   for (int k = ch.y; k < ch.z; ++k) {
@@ -488,15 +499,15 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
         for (int t = tid; t < NCD; t += team)
           ccd[t] = scoef[K * MAXCOMP + t / ND] * scoef[L * MAXCOMP + t % ND];
         sync();
-        for (int l = 0; l < tab.nlevels; ++l) {
-          const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
+        for (int l = 0; l < t_nlevels; ++l) {
+          const int o0 = t_levels[l], o1 = t_levels[l + 1];
           for (int o = o0 + tid; o < o1; o += team) {
-            v[base + o] = eval_op(tab.ops, o, v, geo);
+            v[base + o] = eval_op(t_ops, o, v, geo);
           }
           sync();
         }
         const double w = sw[0];
-        for (int i = tid; i < NI; i += team) X[i] = fma(w * cab[i / NCD] * ccd[i % NCD], v[tab.out[i]], X[i]);
+        for (int i = tid; i < NI; i += team) X[i] = fma(w * cab[i / NCD] * ccd[i % NCD], v[t_out[i]], X[i]);
         any = true;
         sync();
       }
@@ -838,6 +849,14 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
         cl.has_table = true;
         cl.ops = d.ops; cl.levels = d.levels; cl.out = d.out;
         cl.nlevels = d.nlevels; cl.nout = d.nout; cl.nslots = d.nslots;
+        cl.ops_p = nullptr; cl.levels_p = nullptr; cl.out_p = nullptr; cl.nlevels_p = 0;
+        if (const OpTableHost* hp = host_optable_pure(cb, ck)) {
+          OpTableDev dp{};
+          if ((rc = upload_optable(ctx, hp, &dp)) != PFE_OK) return rc;
+          if (dp.nslots <= d.nslots) {   // runs inside the full table's shared-memory layout
+            cl.ops_p = dp.ops; cl.levels_p = dp.levels; cl.out_p = dp.out; cl.nlevels_p = dp.nlevels;
+          }
+        }
         cl.per_warp = vv.doubles(h->nslots, true);
         cl.smem_big = sizeof(double) * (size_t)cl.per_warp;
         {  // warps per block that fit the most warps per SM in shared memory (228 KB, ~3 KB static per block)
@@ -923,7 +942,8 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
     straight_launcher(cl.cb, cl.ck, mixed, ql.insts != nullptr)(ql, std::max(grid, 1), s);
     return;
   }
-  OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots};
+  OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots, cl.ops_p, cl.levels_p, cl.out_p,
+               cl.nlevels_p};
   if (variant == 1) {
     const int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
     variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);
