@@ -27,7 +27,6 @@ from __future__ import annotations
 
 import dataclasses
 import math
-import threading
 import time
 from typing import Callable, List, Optional, Sequence
 
@@ -268,19 +267,6 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     order = sorted_order(systems)
     ssys = [systems[k] for k in order]
     learned = not isinstance(opts.guess, str)
-    # the learned guess's host work (features, assembly) overlaps the batch set-up
-    # (a C call that releases the interpreter lock) when this call builds the batch
-    raw_box: dict = {}
-    worker = None
-    if learned and batch is None:
-        def predict():
-            try:
-                g = opts.guess
-                raw_box['raw'] = g.raw_many(ssys) if hasattr(g, 'raw_many') else [g.raw(x) for x in ssys]
-            except BaseException as exc:     # re-raised in the caller's thread
-                raw_box['error'] = exc
-        worker = threading.Thread(target=predict, daemon=True)
-        worker.start()
     fb = batch if batch is not None else fock_mod.DeviceBatch(ssys, dev.index or 0)
     if len(fb) != nmol or any(a is not b for a, b in zip(fb.systems, ssys)):
         raise SCFError('the DeviceBatch must hold the systems in sorted_order')
@@ -334,13 +320,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     elif learned:
         # occupied natural orbitals of the predicted density: the projector on the
         # nocc lowest eigenvectors of -D, D = P/2 in the orthonormal basis
-        if worker is not None:
-            worker.join()
-            if 'error' in raw_box:
-                raise raw_box['error']
-            raws = raw_box['raw']
-        else:
-            raws = opts.guess.raw_many(ssys) if hasattr(opts.guess, 'raw_many') else [opts.guess.raw(s) for s in ssys]
+        raws = opts.guess.raw_many(ssys) if hasattr(opts.guess, 'raw_many') else [opts.guess.raw(s) for s in ssys]
         for kk in range(nmol):
             fb.view(p, kk).copy_(torch.tensor(np.asarray(raws[kk]), **f64))
         for g in groups:
