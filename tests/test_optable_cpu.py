@@ -1,0 +1,78 @@
+"""The generated op tables of the interpreters (polymer_b200/csrc/gen_eri.py),
+evaluated on the CPU with the op semantics the kernels use (eval_op):
+
+* a table's levels order its ops by dependency (every source slot of an op is
+  a Boys slot or the result of an earlier level);
+* the pure-bra table of a class reproduces, bit for bit, every output of the
+  full table whose bra components are all top-level, and reads the zero slot
+  for the others -- so a chunk whose lower bra components carry no
+  coefficient gets the same X from either table.
+"""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), '..', 'polymer_b200', 'csrc'))
+import gen_eri  # noqa: E402
+
+
+def _geometry(rng):
+    g = {k: rng.normal(size=3) for k in ('PA', 'WP', 'QC', 'WQ', 'AB', 'CD')}
+    z, h = rng.uniform(0.3, 2.0, size=2)
+    rho = z * h / (z + h)
+    G1 = [g['PA'], g['QC'], np.ones(3), np.ones(3)]
+    G2 = [g['WP'], g['WQ'], g['AB'], g['CD']]
+    X = [0.5 / z, 0.5 / h, 0.0, 0.0]
+    Y = [rho / z, rho / h, 0.0, 0.0]
+    Z = 0.5 / (z + h)
+    return G1, G2, X, Y, Z
+
+
+def _run(table, L, geo, F):
+    ops, lev, outs, nslots = table
+    G1, G2, X, Y, Z = geo
+    v = np.full(nslots, np.nan)
+    v[0] = 0.0
+    v[1:L + 2] = F
+    base = L + 2
+    for lv in range(len(lev) - 1):
+        for o in range(lev[lv], lev[lv + 1]):
+            h, s1, s2, s3, s4, s5 = ops[o]
+            kind, ax, cA, cB = h >> 12, (h >> 10) & 3, (h >> 5) & 31, h & 31
+            srcs = [s1, s2] + ([s3, s4] if cA else []) + ([s5] if cB else [])
+            assert all(not np.isnan(v[x]) for x in srcs), 'op reads a slot of a later level'
+            val = G1[kind][ax] * v[s1] + G2[kind][ax] * v[s2]
+            if cA:
+                val += cA * X[kind] * (v[s3] - Y[kind] * v[s4])
+            if cB:
+                val += cB * Z * v[s5]
+            v[base + o] = val
+    return np.array([v[x] for x in outs])
+
+
+@pytest.mark.parametrize('cls', [(1, 0, 1, 0), (1, 1, 1, 0), (2, 1, 1, 0), (2, 0, 2, 0), (2, 2, 1, 0)])
+def test_pure_bra_table_matches_the_full_table(cls):
+    LA, LB, LC, LD = cls
+    L = sum(cls)
+    rng = np.random.default_rng(sum(cls))
+    geo = _geometry(rng)
+    F = rng.uniform(0.1, 1.0, size=L + 1)
+    full = _run(gen_eri.gen_optable(*cls), L, geo, F)
+    pure_table = gen_eri.gen_optable(*cls, pure_bra=True)
+    assert len(pure_table[0]) < len(gen_eri.gen_optable(*cls)[0])
+    pure = _run(pure_table, L, geo, F)
+    ca, cb, cc, cd = (gen_eri.comps(x) for x in cls)
+    k = 0
+    for a in ca:
+        for b in cb:
+            top = (LA == 0 or gen_eri.tot(a) == LA) and (LB == 0 or gen_eri.tot(b) == LB)
+            for _ in cc:
+                for _ in cd:
+                    if top:
+                        assert pure[k] == full[k]
+                    else:
+                        assert pure[k] == 0.0 and pure_table[2][k] == 0
+                    k += 1
+    assert k == len(full)
