@@ -166,6 +166,20 @@ struct AbOrder {
   }
 };
 
+// Bra component pairs below the top level (|a| < LA or |b| < LB): in AbOrder
+// they come first.
+template <int LA, int LB>
+struct LowerPairs {
+  static constexpr int count() {
+    int c = 0;
+    for (int a = 0; a < ncum(LA); ++a)
+      for (int b = 0; b < ncum(LB); ++b)
+        if (comp_tot(LA, a) < LA || comp_tot(LB, b) < LB) ++c;
+    return c;
+  }
+  static constexpr int n = count();
+};
+
 // resident blocks of 128 threads the register allocation aims at: 4 (at most
 // 128 registers) for the classes whose working set fits, else the compiler's choice
 template <int LA, int LB, int LC, int LD>
@@ -185,12 +199,17 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   constexpr int NAB = NA * NB;
   constexpr int NCD = NC * ND;
   constexpr int LT = LA + LB + LC + LD;
+  constexpr AbOrder<LA, LB> ORD{};
   constexpr int ABP = (NAB + NPASS - 1) / NPASS;
-  constexpr int AB0 = PASS * ABP;
-  constexpr int AB1 = (AB0 + ABP < NAB) ? AB0 + ABP : NAB;
+  // two-pass (d s| classes split at the level boundary: the lower components of
+  // the d shell first, the top-level ones second, so that a pure d shell (lower
+  // components coefficient-free) skips the first pass entirely
+  constexpr int NLOW = LowerPairs<LA, LB>::n;
+  constexpr bool LSPLIT = NPASS == 2 && LA == 2 && LB == 0 && NLOW * NCD <= 40 && (NAB - NLOW) * NCD <= 40;
+  constexpr int AB0 = LSPLIT ? (PASS == 0 ? 0 : NLOW) : PASS * ABP;
+  constexpr int AB1 = LSPLIT ? (PASS == 0 ? NLOW : NAB) : ((AB0 + ABP < NAB) ? AB0 + ABP : NAB);
   constexpr int XN = (AB1 - AB0) * NCD;
   static_assert(AB0 < NAB, "every pass keeps at least one bra component pair");
-  constexpr AbOrder<LA, LB> ORD{};
   // the pass keeps the pairs ab at positions [AB0, AB1) of ORD; X(k, cd) is pair ORD.ab[AB0 + k]
   auto in_pass = [&](int a, int b) { const int k = ORD.pos[a * NB + b]; return k >= AB0 && k < AB1; };
   auto xi = [&](int a, int b, int cc, int d) { return (ORD.pos[a * NB + b] - AB0) * NCD + cc * ND + d; };
@@ -451,7 +470,7 @@ void launch_q(const MolLaunch& ql, int grid, cudaStream_t s) {
 // Launches per straight-line class (its passes); must match the table below.
 static inline int straight_npass(int cb, int ck) {
   static const int np[6][6] = {{1, 0, 0, 0, 0, 0}, {1, 1, 0, 0, 0, 0}, {1, 2, 8, 0, 0, 0},
-                               {1, 1, 5, 3, 0, 0}, {1, 4, 14, 10, 40, 0}, {3, 10, 50, 25, 0, 0}};
+                               {2, 2, 5, 3, 0, 0}, {1, 4, 14, 10, 40, 0}, {3, 10, 50, 25, 0, 0}};
   return np[cb][ck];
 }
 
@@ -463,7 +482,7 @@ static LaunchFn straight_launcher_t(int cb, int ck) {
       {Q(0, 0, 0, 0, 1), nullptr, nullptr, nullptr, nullptr, nullptr},
       {Q(1, 0, 0, 0, 1), Q(1, 0, 1, 0, 1), nullptr, nullptr, nullptr, nullptr},
       {Q(1, 1, 0, 0, 1), Q(1, 1, 1, 0, 2), Q(1, 1, 1, 1, 8), nullptr, nullptr, nullptr},
-      {Q(2, 0, 0, 0, 1), Q(2, 0, 1, 0, 1), Q(2, 0, 1, 1, 5), Q(2, 0, 2, 0, 3), nullptr, nullptr},
+      {Q(2, 0, 0, 0, 2), Q(2, 0, 1, 0, 2), Q(2, 0, 1, 1, 5), Q(2, 0, 2, 0, 3), nullptr, nullptr},
       {Q(2, 1, 0, 0, 1), Q(2, 1, 1, 0, 4), nullptr, nullptr, nullptr, nullptr},
       {Q(2, 2, 0, 0, 3), nullptr, nullptr, nullptr, nullptr, nullptr}};
 #undef Q
