@@ -166,7 +166,7 @@ class Gen:
 OPS_THRESHOLD = 1600  # classes with more integrals have no straight-line function (op tables only)
 
 
-def gen_optable(LA, LB, LC, LD, pure_bra=False):
+def gen_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
     """Level-scheduled op table of one class for the block-cooperative interpreter.
 
     Slot 0 holds zero, slots 1..L+1 the Boys values F[m]; every recursion node
@@ -244,7 +244,11 @@ def gen_optable(LA, LB, LC, LD, pure_bra=False):
         # cc-pVDZ); the other outputs read slot 0, which holds zero
         return not pure_bra or ((LA == 0 or tot(a) == LA) and (LB == 0 or tot(b) == LB))
 
-    outs = [hk(a, b, c, d) if kept(a, b) else None
+    def kept_ket(c, d):
+        # pure_ket: the same on the ket shells
+        return not pure_ket or ((LC == 0 or tot(c) == LC) and (LD == 0 or tot(d) == LD))
+
+    outs = [hk(a, b, c, d) if kept(a, b) and kept_ket(c, d) else None
             for a in comps(LA) for b in comps(LB) for c in comps(LC) for d in comps(LD)]
     level = {}
     for k in order:   # 'order' is a valid topological order (post-order)
@@ -274,9 +278,16 @@ def gen_optable(LA, LB, LC, LD, pure_bra=False):
     return ops, lev_start, out_slots, nslots
 
 
-def emit_optable(LA, LB, LC, LD, pure_bra=False):
-    ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD, pure_bra)
-    name = 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure' if pure_bra else '')
+def pure_ket_gains(LA, LB, LC, LD):
+    """Whether dropping the ket's lower components too saves ops over the
+    pure-bra table (not where the ket's top outputs need them all anyway)."""
+    return (len(gen_optable(LA, LB, LC, LD, True, True)[0]) <
+            len(gen_optable(LA, LB, LC, LD, True, False)[0]))
+
+
+def emit_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
+    ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD, pure_bra, pure_ket)
+    name = 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure2' if pure_ket else ('_pure' if pure_bra else ''))
     lines = ['// (%d%d|%d%d): %d ops in %d levels, %d slots' % (LA, LB, LC, LD, len(ops), len(lev) - 1, nslots)]
     flat = [v for op in ops for v in op] or [0] * 6
     lines.append('static const unsigned short %s_ops[%d] = {%s};' % (name, len(flat), ','.join(map(str, flat))))
@@ -353,6 +364,8 @@ def main():
             big.append(emit_optable(LA, LB, LC, LD))   # every class can run interpreted
             if LA >= 1:
                 big.append(emit_optable(LA, LB, LC, LD, pure_bra=True))
+            if LA >= 1 and LC >= 1 and pure_ket_gains(LA, LB, LC, LD):
+                big.append(emit_optable(LA, LB, LC, LD, pure_bra=True, pure_ket=True))
             if n > OPS_THRESHOLD:
                 g = Gen(LA, LB, LC, LD)
                 g.build()

@@ -54,6 +54,10 @@ struct ClassLaunch {
   const int* levels_p;
   const unsigned short* out_p;
   int nlevels_p;
+  const unsigned short* ops_p2;  // pure bra and pure ket table, or null
+  const int* levels_p2;
+  const unsigned short* out_p2;
+  int nlevels_p2;
   int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
   size_t smem_big, smem_warp;
   float tuned_ms[3];         // autotuner timings per variant (0 = not run)
@@ -246,6 +250,7 @@ int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double
 struct OpTableDev;
 const struct OpTableHost* host_optable(int cb, int ck);
 const struct OpTableHost* host_optable_pure(int cb, int ck);
+const struct OpTableHost* host_optable_pure2(int cb, int ck);
 int upload_optable(pfe_context* ctx, const struct OpTableHost* h, OpTableDev* d);
 double class_flops(int cb, int ck);
 int lattice_setup(pfe_context* ctx, const pfe_args* a);

@@ -112,6 +112,26 @@ const OpTableHost* host_optable_pure(int cb, int ck) {
   }
 }
 
+// The variant with pure bra and pure ket shells, or null (ket classes with no
+// p or d shell, and classes where it saves no op over the pure-bra table).
+const OpTableHost* host_optable_pure2(int cb, int ck) {
+  switch (cb * 8 + ck) {
+    case 2 * 8 + 1: return &op_1110_pure2;
+    case 2 * 8 + 2: return &op_1111_pure2;
+    case 3 * 8 + 2: return &op_2011_pure2;
+    case 4 * 8 + 1: return &op_2110_pure2;
+    case 4 * 8 + 2: return &op_2111_pure2;
+    case 4 * 8 + 3: return &op_2120_pure2;
+    case 4 * 8 + 4: return &op_2121_pure2;
+    case 5 * 8 + 1: return &op_2210_pure2;
+    case 5 * 8 + 2: return &op_2211_pure2;
+    case 5 * 8 + 3: return &op_2220_pure2;
+    case 5 * 8 + 4: return &op_2221_pure2;
+    case 5 * 8 + 5: return &op_2222_pure2;
+    default: return nullptr;
+  }
+}
+
 // The op tables are immutable: each is uploaded once per device and shared by
 // every context on it (a batch holds hundreds of contexts).  The copies live as
 // long as the process.

@@ -20,6 +20,12 @@ struct OpTableDev {
   const int* levels_p;
   const unsigned short* out_p;
   int nlevels_p;
+  // the variant with pure bra and pure ket shells, for (G|H) whose ket shells
+  // are pure too, or null
+  const unsigned short* ops_p2;
+  const int* levels_p2;
+  const unsigned short* out_p2;
+  int nlevels_p2;
 };
 
 // Geometry multipliers of the four op kinds, in shared memory.

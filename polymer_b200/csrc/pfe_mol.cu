@@ -429,10 +429,11 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
     if (comp_tot(LA, x) < LA && prm[x] >= 0) pure = false;
   for (int x = 0; pure && x < NB; ++x)
     if (comp_tot(LB, x) < LB && prm[DG::SB + x] >= 0) pure = false;
-  const unsigned short* __restrict__ t_ops = pure ? tab.ops_p : tab.ops;
-  const int* __restrict__ t_levels = pure ? tab.levels_p : tab.levels;
-  const unsigned short* __restrict__ t_out = pure ? tab.out_p : tab.out;
-  const int t_nlevels = pure ? tab.nlevels_p : tab.nlevels;
+  const unsigned short* __restrict__ b_ops = pure ? tab.ops_p : tab.ops;
+  const int* __restrict__ b_levels = pure ? tab.levels_p : tab.levels;
+  const unsigned short* __restrict__ b_out = pure ? tab.out_p : tab.out;
+  const int b_nlevels = pure ? tab.nlevels_p : tab.nlevels;
+  pure = pure && tab.ops_p2 != nullptr;   // from here: the bra-and-ket table may apply
   for (int t = tid; t < NA * NB; t += team)
     P[DG::OAB + t] = dt_at(D, nt, prm[t / NB], prm[DG::SB + t % NB]);
   for (int k = ch.y; k < ch.z; ++k) {
@@ -461,6 +462,17 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
       for (int t = tid; t < NB * ND; t += team) P[DG::OBD + t] = dt_at(D, nt, pb[t / ND], pd[t % ND]);
     }
     sync();   // the blocks are read by the digestion, which may follow with no quartet in between
+    // pure bra and pure ket shells take the table that drops both sides' lower
+    // components (team-uniform: prm is shared)
+    bool pure2 = pure;
+    for (int x = 0; pure2 && x < NC; ++x)
+      if (comp_tot(LC, x) < LC && prm[DG::SC + x] >= 0) pure2 = false;
+    for (int x = 0; pure2 && x < ND; ++x)
+      if (comp_tot(LD, x) < LD && prm[DG::SD + x] >= 0) pure2 = false;
+    const unsigned short* __restrict__ t_ops = pure2 ? tab.ops_p2 : b_ops;
+    const int* __restrict__ t_levels = pure2 ? tab.levels_p2 : b_levels;
+    const unsigned short* __restrict__ t_out = pure2 ? tab.out_p2 : b_out;
+    const int t_nlevels = pure2 ? tab.nlevels_p2 : b_nlevels;
     bool any = false;   // team-uniform: every loop decision below is
     for (int p = g0; p < g0 + gn; ++p) {
       const double sp = pr.schwarz[p];
@@ -857,6 +869,14 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
             cl.ops_p = dp.ops; cl.levels_p = dp.levels; cl.out_p = dp.out; cl.nlevels_p = dp.nlevels;
           }
         }
+        cl.ops_p2 = nullptr; cl.levels_p2 = nullptr; cl.out_p2 = nullptr; cl.nlevels_p2 = 0;
+        if (const OpTableHost* hp = host_optable_pure2(cb, ck)) {
+          OpTableDev dp{};
+          if ((rc = upload_optable(ctx, hp, &dp)) != PFE_OK) return rc;
+          if (dp.nslots <= d.nslots && cl.ops_p) {   // taken only where the pure-bra table is
+            cl.ops_p2 = dp.ops; cl.levels_p2 = dp.levels; cl.out_p2 = dp.out; cl.nlevels_p2 = dp.nlevels;
+          }
+        }
         cl.per_warp = vv.doubles(h->nslots, true);
         cl.smem_big = sizeof(double) * (size_t)cl.per_warp;
         {  // warps per block that fit the most warps per SM in shared memory (228 KB, ~3 KB static per block)
@@ -942,8 +962,8 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
     straight_launcher(cl.cb, cl.ck, mixed, ql.insts != nullptr)(ql, std::max(grid, 1), s);
     return;
   }
-  OpTableDev t{cl.ops, cl.levels, cl.out, cl.nlevels, cl.nout, cl.nslots, cl.ops_p, cl.levels_p, cl.out_p,
-               cl.nlevels_p};
+  OpTableDev t{cl.ops,   cl.levels,   cl.out,     cl.nlevels,   cl.nout,   cl.nslots,     cl.ops_p,
+               cl.levels_p, cl.out_p, cl.nlevels_p, cl.ops_p2, cl.levels_p2, cl.out_p2, cl.nlevels_p2};
   if (variant == 1) {
     const int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
     variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);

@@ -71,9 +71,15 @@ def test_alkane_screened_matches_oracle(n, inttol):
 
 
 @pytest.mark.parametrize('variant', [0, 1, 2])
-def test_every_execution_variant_matches_oracle(variant):
-    """Straight-line, warp-per-quartet and block-per-quartet schedules all agree."""
-    s = _sys(geometry.alkane_deck(2, inttol=1e-12))
+@pytest.mark.parametrize('mol', ['alkane', 'water'])
+def test_every_execution_variant_matches_oracle(variant, mol, reference_runs):
+    """Straight-line, warp-per-quartet and block-per-quartet schedules all agree:
+    6-31G** alkane (cumulative sp and d shells: the full op tables) and cc-pVDZ
+    water (pure p and d shells: the pure-bra and bra-and-ket tables)."""
+    if mol == 'alkane':
+        s = _sys(geometry.alkane_deck(2, inttol=1e-12))
+    else:
+        s = _sys(deck_of(reference_runs['H2O_CCSD_ccpVDZ']))
     _, pp = _random_density(s, seed=5)
     c_ref, x_ref = oracle.fourindex_eri(s, pp)
     df = fock.DeviceFock(s)

@@ -6,7 +6,9 @@ evaluated on the CPU with the op semantics the kernels use (eval_op):
 * the pure-bra table of a class reproduces, bit for bit, every output of the
   full table whose bra components are all top-level, and reads the zero slot
   for the others -- so a chunk whose lower bra components carry no
-  coefficient gets the same X from either table.
+  coefficient gets the same X from either table; the bra-and-ket table does
+  the same for outputs whose bra and ket components are all top-level, and
+  drops ops beyond the pure-bra table's.
 """
 import os
 import sys
@@ -52,25 +54,38 @@ def _run(table, L, geo, F):
     return np.array([v[x] for x in outs])
 
 
-@pytest.mark.parametrize('cls', [(1, 0, 1, 0), (1, 1, 1, 0), (2, 1, 1, 0), (2, 0, 2, 0), (2, 2, 1, 0)])
-def test_pure_bra_table_matches_the_full_table(cls):
+CLASSES = [(1, 0, 1, 0), (1, 1, 1, 0), (2, 1, 1, 0), (2, 0, 2, 0), (2, 2, 1, 0), (2, 1, 2, 1)]
+
+
+@pytest.mark.parametrize('ket', [False, True], ids=['bra', 'bra_ket'])
+@pytest.mark.parametrize('cls', CLASSES)
+def test_pure_table_matches_the_full_table(cls, ket):
     LA, LB, LC, LD = cls
     L = sum(cls)
     rng = np.random.default_rng(sum(cls))
     geo = _geometry(rng)
     F = rng.uniform(0.1, 1.0, size=L + 1)
     full = _run(gen_eri.gen_optable(*cls), L, geo, F)
-    pure_table = gen_eri.gen_optable(*cls, pure_bra=True)
-    assert len(pure_table[0]) < len(gen_eri.gen_optable(*cls)[0])
+    pure_table = gen_eri.gen_optable(*cls, pure_bra=True, pure_ket=ket)
+    if ket:
+        assert gen_eri.pure_ket_gains(*cls) == (len(pure_table[0]) <
+                                                len(gen_eri.gen_optable(*cls, pure_bra=True)[0]))
+    else:
+        assert len(pure_table[0]) < len(gen_eri.gen_optable(*cls)[0])
+    assert pure_table[3] <= gen_eri.gen_optable(*cls)[3]   # fits the full table's slots
     pure = _run(pure_table, L, geo, F)
     ca, cb, cc, cd = (gen_eri.comps(x) for x in cls)
     k = 0
     for a in ca:
         for b in cb:
             top = (LA == 0 or gen_eri.tot(a) == LA) and (LB == 0 or gen_eri.tot(b) == LB)
-            for _ in cc:
-                for _ in cd:
-                    if top:
+            for c in cc:
+                for d in cd:
+                    if ket:
+                        top_k = (LC == 0 or gen_eri.tot(c) == LC) and (LD == 0 or gen_eri.tot(d) == LD)
+                    else:
+                        top_k = True
+                    if top and top_k:
                         assert pure[k] == full[k]
                     else:
                         assert pure[k] == 0.0 and pure_table[2][k] == 0
