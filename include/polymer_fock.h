@@ -130,6 +130,10 @@ int32_t pfe_context_primitive_targets(pfe_context *ctx, int32_t enable);
  * doubles) of one device buffer; pfe_batch_offsets writes off[0..n] and returns n. */
 typedef struct pfe_batch pfe_batch;
 int32_t pfe_batch_create(int32_t device, pfe_batch **out);
+/* Replaces any earlier set-up.  If one instance is refused (the status and
+ * pfe_last_error say which), every instance is freed: until a set-up succeeds,
+ * builds, screening, refresh and autotune return PFE_EINVAL, offsets and
+ * schedule report none and the census is zero. */
 int32_t pfe_batch_setup(pfe_batch *b, const pfe_args *instances, int32_t n);
 int32_t pfe_batch_offsets(pfe_batch *b, int64_t *off);
 /* pfe_context_set_screening applied to every instance. */

@@ -521,12 +521,19 @@ int32_t pfe_batch_create(int32_t device, pfe_batch** out) {
   return PFE_OK;
 }
 
-int32_t pfe_batch_destroy(pfe_batch* b) {
-  if (!b) return PFE_OK;
+// Frees the instances and the joined launches: the batch is not set up.
+static void batch_clear(pfe_batch* b) {
   cudaSetDevice(b->device);
   cudaDeviceSynchronize();
   for (pfe_context* c : b->inst) pfe_context_destroy(c);
+  b->inst.clear();
   b->release_all();
+  b->off.assign(1, 0);
+}
+
+int32_t pfe_batch_destroy(pfe_batch* b) {
+  if (!b) return PFE_OK;
+  batch_clear(b);
   delete b;
   return PFE_OK;
 }
@@ -534,25 +541,34 @@ int32_t pfe_batch_destroy(pfe_batch* b) {
 int32_t pfe_batch_setup(pfe_batch* b, const pfe_args* args, int32_t n) {
   if (!b || !args || n < 1) { set_error("pfe_batch_setup: bad argument"); return PFE_EINVAL; }
   PFE_CUDA(cudaSetDevice(b->device));
-  for (pfe_context* c : b->inst) pfe_context_destroy(c);
-  b->inst.clear();
-  b->release_all();
-  b->off.assign(1, 0);
-  for (int k = 0; k < n; ++k) {
+  batch_clear(b);
+  int rc = PFE_OK;
+  for (int k = 0; k < n && rc == PFE_OK; ++k) {
     pfe_context* c = nullptr;
-    int rc = pfe_context_create(b->device, &c);
-    if (rc != PFE_OK) return rc;
+    if ((rc = pfe_context_create(b->device, &c)) != PFE_OK) break;
     b->inst.push_back(c);
-    if ((rc = pfe_context_setup(c, &args[k])) != PFE_OK) return rc;
-    if (!c->molecular) { set_error("pfe_batch_setup: batches hold molecules only"); return PFE_EUNSUPPORTED; }
-    if (c->numprocs != 1) { set_error("pfe_batch_setup: one rank per batch (numprocs 1)"); return PFE_EUNSUPPORTED; }
-    b->off.push_back(b->off.back() + (long long)c->ncgs * c->ncgs);
+    if ((rc = pfe_context_setup(c, &args[k])) != PFE_OK) break;
+    if (!c->molecular) {
+      set_error("pfe_batch_setup: batches hold molecules only");
+      rc = PFE_EUNSUPPORTED;
+    } else if (c->numprocs != 1) {
+      set_error("pfe_batch_setup: one rank per batch (numprocs 1)");
+      rc = PFE_EUNSUPPORTED;
+    } else {
+      b->off.push_back(b->off.back() + (long long)c->ncgs * c->ncgs);
+    }
   }
-  return batch_setup(b);
+  if (rc == PFE_OK) rc = batch_setup(b);
+  if (rc != PFE_OK) {   // keep the message; leave no half-built batch behind
+    batch_clear(b);
+    return rc;
+  }
+  b->ready = true;
+  return PFE_OK;
 }
 
 int32_t pfe_batch_set_screening(pfe_batch* b, int32_t precision_mode, double mixed_cutoff, double density_tol) {
-  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!b || !b->ready) { set_error("batch is not set up"); return PFE_EINVAL; }
   for (pfe_context* c : b->inst) {
     int rc = pfe_context_set_screening(c, precision_mode, mixed_cutoff, density_tol);
     if (rc != PFE_OK) return rc;
@@ -563,7 +579,7 @@ int32_t pfe_batch_set_screening(pfe_batch* b, int32_t precision_mode, double mix
 
 int32_t pfe_batch_set_instance_screening(pfe_batch* b, int32_t k, int32_t precision_mode, double mixed_cutoff,
                                          double density_tol) {
-  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!b || !b->ready) { set_error("batch is not set up"); return PFE_EINVAL; }
   if (k < 0 || k >= (int)b->inst.size()) { set_error("no such instance in the batch"); return PFE_EINVAL; }
   pfe_context* c = b->inst[k];
   const double mc = c->mcut, dt = c->dtol;
@@ -574,7 +590,7 @@ int32_t pfe_batch_set_instance_screening(pfe_batch* b, int32_t k, int32_t precis
 }
 
 int32_t pfe_batch_refresh(pfe_batch* b, const double* d_p_c) {
-  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!b || !b->ready) { set_error("batch is not set up"); return PFE_EINVAL; }
   if (!d_p_c) { set_error("null device pointer"); return PFE_EINVAL; }
   PFE_CUDA(cudaSetDevice(b->device));
   return batch_refresh(b, d_p_c);
@@ -587,7 +603,7 @@ static int class_code(int cb, int ck) {
 }
 
 int32_t pfe_batch_autotune(pfe_batch* b, const double* d_p_c, void* stream) {
-  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!b || !b->ready) { set_error("batch is not set up"); return PFE_EINVAL; }
   if (!d_p_c) { set_error("null device pointer"); return PFE_EINVAL; }
   PFE_CUDA(cudaSetDevice(b->device));
   return batch_autotune(b, d_p_c, (cudaStream_t)stream);
@@ -617,7 +633,7 @@ int32_t pfe_batch_offsets(pfe_batch* b, int64_t* off) {
 }
 
 int32_t pfe_batch_fock_pc(pfe_batch* b, const double* d_p_c, double* d_c_c, double* d_x_c, void* stream) {
-  if (!b || b->inst.empty()) { set_error("batch is not set up"); return PFE_EINVAL; }
+  if (!b || !b->ready) { set_error("batch is not set up"); return PFE_EINVAL; }
   if (!d_p_c || !d_c_c || !d_x_c) { set_error("null device pointer"); return PFE_EINVAL; }
   PFE_CUDA(cudaSetDevice(b->device));
   return batch_fock_pc(b, d_p_c, d_c_c, d_x_c, (cudaStream_t)stream);

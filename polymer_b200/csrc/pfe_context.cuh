@@ -201,6 +201,7 @@ struct pfe_batch {
   bool ev_pending = false;
   const double* insts_for = nullptr;  // density the records point at (null: rewrite them)
   bool mixed = false;               // FP32-capable kernels (sticky once any instance asked for them)
+  bool ready = false;               // set by a pfe_batch_setup that succeeded
   std::vector<void*> owned;
   cudaError_t alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
@@ -217,6 +218,8 @@ struct pfe_batch {
     ev_pending = false;
     d_insts = nullptr;
     insts_for = nullptr;
+    nlaunch = 0;   // the launches pointed into the memory freed above
+    ready = false;
   }
 };
 

@@ -11,7 +11,9 @@ over the work of every molecule in the batch.
 * the census of a batch sums its molecules' quartets while the class launches
   do not grow with the number of molecules;
 * after the batch autotuner has timed every variant of every class, builds
-  still match the per-molecule ones.
+  still match the per-molecule ones;
+* a set-up refused for one instance leaves no half-built batch: later calls
+  answer that the batch is not set up, and the handle can be set up again.
 """
 import numpy as np
 import pytest
@@ -133,3 +135,51 @@ def test_batch_autotune_keeps_results():
     torch.cuda.synchronize()
     _check(got, ref, 'autotuned')
     b.close()
+
+
+def test_failed_setup_leaves_no_batch():
+    """A set-up refused for one instance (an f shell) frees every instance: later
+    calls on the handle answer that the batch is not set up, and a good set-up on
+    the same handle builds as the per-molecule context does."""
+    import ctypes
+    from polymer_b200 import basis, capi
+    lib = {k: list(v) for k, v in basis.load_basis_library('cc-pVDZ').items()}
+    lib['O'] = lib['O'] + [['F', 1.0, [[1.428, 1.0]]]]
+    good = _sys(geometry.water_deck(1, seed=3500))
+    def zero_onee(sysm):   # the one-electron integrals play no part in the refusal
+        z = np.zeros((sysm.ncell1, sysm.basis.npgs, sysm.basis.npgs))
+        return z, z.copy(), z.copy()
+
+    bad = system.build_system(geometry.water_deck(1, seed=3501), zero_onee, library=lib)
+    L = capi.lib()
+    h = ctypes.c_void_p()
+    capi.check(L, L.pfe_batch_create(0, ctypes.byref(h)))
+    try:
+        args = [s.pfe_args(None, None) for s in (good, bad)]
+        arr = (capi.PfeArgs * 2)(*[a for a, _ in args])
+        assert L.pfe_batch_setup(h, arr, 2) == -3                      # PFE_EUNSUPPORTED
+        n = good.basis.ncgs
+        buf = torch.zeros(4 * n * n, dtype=torch.float64, device='cuda')
+        p = ctypes.c_void_p(buf.data_ptr())
+        assert L.pfe_batch_fock_pc(h, p, p, p, None) == -1             # PFE_EINVAL
+        assert 'not set up' in capi.last_error(L)
+        off = (ctypes.c_int64 * 3)()
+        assert L.pfe_batch_offsets(h, off) == 0
+        c = capi.PfeCensus()
+        capi.check(L, L.pfe_batch_census(h, ctypes.byref(c)))
+        assert c.kernel_launches == 0 and c.quartets == 0
+        # the same handle, set up again with the good molecule alone
+        arr1 = (capi.PfeArgs * 1)(args[0][0])
+        capi.check(L, L.pfe_batch_setup(h, arr1, 1))
+        assert L.pfe_batch_offsets(h, off) == 1 and off[1] == n * n
+        pc = _pc(good, 11)
+        dp = torch.tensor(pc.T.copy(), device='cuda').reshape(-1)
+        oc, ox = torch.empty_like(dp), torch.empty_like(dp)
+        capi.check(L, L.pfe_batch_fock_pc(h, ctypes.c_void_p(dp.data_ptr()), ctypes.c_void_p(oc.data_ptr()),
+                                          ctypes.c_void_p(ox.data_ptr()), None))
+        torch.cuda.synchronize()
+        (cs, xs), = _singles([good], [pc])
+        _close(oc.reshape(n, n).T.cpu().numpy(), cs, 'reset C_C')
+        _close(ox.reshape(n, n).T.cpu().numpy(), xs, 'reset X_C')
+    finally:
+        L.pfe_batch_destroy(h)
