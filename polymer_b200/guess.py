@@ -14,6 +14,7 @@ converged densities of the GPU SCF over seeded water clusters.
 from __future__ import annotations
 
 import dataclasses
+import itertools
 import math
 import os
 from typing import Dict, List, Optional, Tuple
@@ -45,19 +46,32 @@ def _monomials(L: int):
     return [(i, j, L - i - j) for i in range(L, -1, -1) for j in range(L - i, -1, -1)]
 
 
-def monomial_transform(L: int, R: np.ndarray) -> Tuple[list, np.ndarray]:
-    """Q with m_i(R u) = sum_j Q_ij m_j(u) for the degree-L monomials (exact: fitted
-    on random points, the relation being polynomial)."""
+def monomial_transforms(L: int, Rs: np.ndarray) -> Tuple[list, np.ndarray]:
+    """Q[w] with m_i(R_w u) = sum_j Q[w]_ij m_j(u) for the degree-L monomials, for
+    a stack of rotations Rs (nw x 3 x 3): m_i(R u) is the product of the L linear
+    forms (R u)_r, one per power of monomial i, and its expansion's term
+    u_j1 ... u_jL adds prod_k R[r_k, j_k] to the monomial with those powers."""
     pws = _monomials(L)
-    rng = np.random.default_rng(12345)
-    u = rng.normal(size=(4 * len(pws) + 4, 3))
-    ru = u @ R.T
+    pos = {pw: k for k, pw in enumerate(pws)}
+    nw = Rs.shape[0]
+    # the monomial of every index tuple (j1..jL), as a 0/1 matrix (3^L x nm)
+    fold = np.zeros((3 ** L, len(pws)))
+    for t, js in enumerate(itertools.product(range(3), repeat=L)):
+        fold[t, pos[(js.count(0), js.count(1), js.count(2))]] = 1.0
+    q = np.empty((nw, len(pws), len(pws)))
+    for i, pw in enumerate(pws):
+        rows = [0] * pw[0] + [1] * pw[1] + [2] * pw[2]
+        t = np.ones((nw, 1))
+        for r in rows:   # outer product with the next linear form, j_k varying fastest last
+            t = (t[:, :, None] * Rs[:, r, None, :]).reshape(nw, -1)
+        q[:, i, :] = t @ fold
+    return pws, q
 
-    def ev(pts):
-        return np.stack([pts[:, 0] ** a * pts[:, 1] ** b * pts[:, 2] ** c for a, b, c in pws], axis=1)
 
-    q, *_ = np.linalg.lstsq(ev(u), ev(ru), rcond=None)
-    return pws, q.T
+def monomial_transform(L: int, R: np.ndarray) -> Tuple[list, np.ndarray]:
+    """Q with m_i(R u) = sum_j Q_ij m_j(u) for the degree-L monomials."""
+    pws, q = monomial_transforms(L, R[None])
+    return pws, q[0]
 
 
 @dataclasses.dataclass
@@ -69,26 +83,55 @@ class AOInfo:
     atom_funcs: List[List[int]]
 
 
+def _round10(v: np.ndarray) -> np.ndarray:
+    """Python's round(x, 10) of every element (applied once per distinct value)."""
+    u, inv = np.unique(v, return_inverse=True)
+    return np.array([round(float(x), 10) for x in u])[inv.reshape(-1)] if len(u) else v.copy()
+
+
 def ao_info(sysm: System) -> AOInfo:
+    """Per contracted function: live (a row of CC not all zero), atom and
+    Cartesian powers of its largest primitive; functions of one shell instance
+    share (atom, L, radial part), the radial part being the sorted (exponent,
+    coefficient / norm) pairs rounded to 10 digits.  Groups come in the order of
+    their first function."""
     b = sysm.basis
     n = b.ncgs
-    live = np.any(b.cc != 0.0, axis=1)
-    atom = np.zeros(n, dtype=int)
-    powers: List[tuple] = [(0, 0, 0)] * n
-    keys: Dict[tuple, List[int]] = {}
-    for i in range(n):
-        if not live[i]:
-            continue
-        ps = np.nonzero(b.cc[i])[0]
-        p0 = ps[np.argmax(np.abs(b.cc[i, ps]))]
-        pw = (int(b.pax[p0]), int(b.pay[p0]), int(b.paz[p0]))
-        powers[i] = pw
-        atom[i] = int(b.pgs_atom[p0]) - 1
-        radial = tuple(sorted((round(float(b.zt[p]), 10), round(float(b.cc[i, p]) / _norm(pw), 10)) for p in ps))
-        keys.setdefault((atom[i], sum(pw), radial), []).append(i)
-    groups = list(keys.values())
+    cc = np.asarray(b.cc)
+    live = np.any(cc != 0.0, axis=1)
+    p0 = np.argmax(np.abs(cc), axis=1)
+    pw = np.stack([np.asarray(b.pax)[p0], np.asarray(b.pay)[p0], np.asarray(b.paz)[p0]], axis=1).astype(int)
+    pw[~live] = 0
+    atom = np.where(live, np.asarray(b.pgs_atom)[p0].astype(int) - 1, 0)
+    powers: List[tuple] = list(map(tuple, pw.tolist()))
+    li = np.nonzero(live)[0]
+    groups: List[List[int]] = []
+    if len(li):
+        # _norm of every row's powers: the double factorials are exact integers
+        df = np.array([_dfact(2 * k - 1) for k in range(int(pw.max()) + 1)], dtype=float)
+        pl = pw[li]
+        norms = 1.0 / np.sqrt(df[pl[:, 0]] * df[pl[:, 1]] * df[pl[:, 2]])
+        sub = cc[li]
+        r, c = np.nonzero(sub != 0.0)
+        zr = _round10(np.asarray(b.zt, dtype=float)[c])
+        cr = _round10(sub[r, c] / norms[r])
+        o = np.lexsort((cr, zr, r))   # per row, pairs sorted by (exponent, coefficient)
+        r, zr, cr = r[o], zr[o], cr[o]
+        cnt = np.bincount(r, minlength=len(li))
+        slot = np.arange(len(r)) - (np.cumsum(cnt) - cnt)[r]
+        key = np.full((len(li), 2 + 2 * int(cnt.max())), np.inf)
+        key[:, 0] = atom[li]
+        key[:, 1] = pw[li].sum(axis=1)
+        key[r, 2 + 2 * slot] = zr
+        key[r, 3 + 2 * slot] = cr
+        _, inv = np.unique(key, axis=0, return_inverse=True)
+        inv = inv.reshape(-1)
+        first = np.full(inv.max() + 1, len(li))
+        np.minimum.at(first, inv, np.arange(len(li)))
+        for g in np.argsort(first, kind='stable'):
+            groups.append(li[inv == g].tolist())
     natom = sysm.deck.natom
-    atom_funcs = [[i for i in range(n) if live[i] and atom[i] == a] for a in range(natom)]
+    atom_funcs = [np.nonzero(live & (atom == a))[0].tolist() for a in range(natom)]
     return AOInfo(live, atom, powers, groups, atom_funcs)
 
 
@@ -115,19 +158,19 @@ def frame_transform(info: AOInfo, R: np.ndarray, funcs: List[int], qcache: Optio
 
 
 def water_frames(sysm: System) -> List[Tuple[np.ndarray, np.ndarray, List[int]]]:
-    """(origin, R, atoms) of every water: atoms come as O, H, H in the deck."""
+    """(origin, R, atoms) of every water: atoms come as O, H, H in the deck; the
+    frame's e1 bisects the two O-H bonds, e2 lies in the molecular plane."""
     d = sysm.deck
-    xyz = np.array(d.coords)
-    out = []
-    for m in range(d.natom // 3):
-        o, h1, h2 = xyz[3 * m], xyz[3 * m + 1], xyz[3 * m + 2]
-        a, c = h1 - o, h2 - o
-        e1 = (a + c) / np.linalg.norm(a + c)
-        e2 = (a - c) - np.dot(a - c, e1) * e1
-        e2 /= np.linalg.norm(e2)
-        e3 = np.cross(e1, e2)
-        out.append((o, np.stack([e1, e2, e3], axis=1), [3 * m, 3 * m + 1, 3 * m + 2]))
-    return out
+    nw = d.natom // 3
+    xyz = np.array(d.coords, dtype=float)[:3 * nw].reshape(nw, 3, 3)
+    o = xyz[:, 0]
+    a, c = xyz[:, 1] - o, xyz[:, 2] - o
+    e1 = (a + c) / np.linalg.norm(a + c, axis=1, keepdims=True)
+    e2 = (a - c) - np.sum((a - c) * e1, axis=1, keepdims=True) * e1
+    e2 /= np.linalg.norm(e2, axis=1, keepdims=True)
+    e3 = np.cross(e1, e2)
+    R = np.stack([e1, e2, e3], axis=2)
+    return [(o[m], R[m], [3 * m, 3 * m + 1, 3 * m + 2]) for m in range(nw)]
 
 
 def _type(z: int) -> np.ndarray:
@@ -225,29 +268,90 @@ def targets(sysm: System, info: AOInfo, frames, pairs, p_c: np.ndarray) -> Tuple
     return t, w
 
 
+def _layout_plan(info: AOInfo, a: int, cache: dict):
+    """Atom a's layout and its frame transform as entries per degree L: (row,
+    column, monomial row, monomial column, norm ratio) arrays, so that
+    U[row, col] = Q_L[mrow, mcol] * ratio, as frame_transform fills it."""
+    lay = _layout(info, a, cache)
+    key = ('plan', lay)
+    if key not in cache:
+        groups, pws = lay
+        plan: Dict[int, tuple] = {}
+        for g in groups:
+            L = sum(pws[g[0]])
+            pos = {pw: k for k, pw in enumerate(_monomials(L))}
+            e = plan.setdefault(L, ([], [], [], [], []))
+            for i in g:
+                for j in g:
+                    e[0].append(i)
+                    e[1].append(j)
+                    e[2].append(pos[pws[i]])
+                    e[3].append(pos[pws[j]])
+                    e[4].append(_norm(pws[i]) / _norm(pws[j]))
+        cache[key] = (len(pws), {L: tuple(np.array(x) for x in e) for L, e in plan.items()})
+    return lay, cache[key]
+
+
+def frame_inverses(info: AOInfo, frames, natom: int, cache: dict) -> dict:
+    """Per atom layout: V = U^-1 of every water's frame (nwater x nf x nf), the
+    monomial transforms of all frames computed at once per degree."""
+    Rs = np.stack([fr[1] for fr in frames]) if frames else np.zeros((0, 3, 3))
+    q: Dict[int, np.ndarray] = {}
+    out: dict = {}
+    for a in range(natom):
+        lay, (nf, plan) = _layout_plan(info, a, cache)
+        if lay in out or nf == 0:
+            continue
+        u = np.zeros((len(Rs), nf, nf))
+        for L, (ui, uj, mi, mj, ratio) in plan.items():
+            if L not in q:
+                q[L] = monomial_transforms(L, Rs)[1]
+            u[:, ui, uj] = q[L][:, mi, mj] * ratio
+        out[lay] = np.linalg.inv(u)
+    return out
+
+
 def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.ndarray:
     """Laboratory contracted density from predicted frame blocks (symmetrised:
     each block enters at (A,B) and, transposed, at (B,A); entries are averaged)."""
     n = sysm.basis.ncgs
-    acc = np.zeros((n, n))
-    cnt = np.zeros((n, n))
+    if not pairs:
+        return np.zeros((n, n))
+    natom = sysm.deck.natom
     cache: dict = {}
-    by_shape: Dict[tuple, List[int]] = {}
-    for k, (a, b, m) in enumerate(pairs):
-        by_shape.setdefault((len(info.atom_funcs[a]), len(info.atom_funcs[b])), []).append(k)
-    for (na, nb), ks in by_shape.items():
-        va = np.stack([_v_for_atom(info, frames[pairs[k][2]][1], pairs[k][0], cache) for k in ks])
-        vb = np.stack([_v_for_atom(info, frames[pairs[k][2]][1], pairs[k][1], cache) for k in ks])
+    vinv = frame_inverses(info, frames, natom, cache)
+    lays = [_layout(info, a, cache) for a in range(natom)]
+    lay_id = {lay: k for k, lay in enumerate(dict.fromkeys(lays))}
+    atom_lay = np.array([lay_id[lay] for lay in lays])
+    by_id = {k: lay for lay, k in lay_id.items()}
+    maxf = max(1, max(len(f) for f in info.atom_funcs))
+    funcs = np.zeros((natom, maxf), dtype=np.int64)
+    for a, f in enumerate(info.atom_funcs):
+        funcs[a, :len(f)] = f
+    P = np.asarray(pairs)
+    A, B, M = P[:, 0], P[:, 1], P[:, 2]
+    combo = atom_lay[A] * len(lay_id) + atom_lay[B]
+    idx, val = [], []
+    for cb in dict.fromkeys(combo.tolist()):   # first-appearance order
+        ks = np.nonzero(combo == cb)[0]
+        la, lb = by_id[cb // len(lay_id)], by_id[cb % len(lay_id)]
+        na, nb = len(la[1]), len(lb[1])
+        if na == 0 or nb == 0:
+            continue
+        va, vb = vinv[la][M[ks]], vinv[lb][M[ks]]
         blk = pred[ks].reshape(-1, MAXF, MAXF)[:, :na, :nb]
-        lab = np.einsum('kia,kab->kib', va.transpose(0, 2, 1), np.einsum('kij,kjb->kib', blk, vb))
-        rows = np.array([info.atom_funcs[pairs[k][0]] for k in ks])
-        cols = np.array([info.atom_funcs[pairs[k][1]] for k in ks])
-        r, c = rows[:, :, None], cols[:, None, :]
-        np.add.at(acc, (r, c), lab)
-        np.add.at(cnt, (r, c), 1.0)
-        np.add.at(acc, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), lab.transpose(0, 2, 1))
-        np.add.at(cnt, (c.transpose(0, 2, 1), r.transpose(0, 2, 1)), 1.0)
-    return np.where(cnt > 0, acc / np.maximum(cnt, 1.0), 0.0)
+        lab = va.transpose(0, 2, 1) @ (blk @ vb)
+        r, c = funcs[A[ks], :na], funcs[B[ks], :nb]
+        idx.append((r[:, :, None] * n + c[:, None, :]).ravel())
+        val.append(lab.ravel())
+        idx.append((c[:, None, :] * n + r[:, :, None]).ravel())   # the transpose: (B,A) gets lab[k].T
+        val.append(lab.ravel())
+    if not idx:
+        return np.zeros((n, n))
+    idx = np.concatenate(idx)
+    acc = np.bincount(idx, weights=np.concatenate(val), minlength=n * n).reshape(n, n)
+    cnt = np.bincount(idx, minlength=n * n).reshape(n, n)
+    return np.where(cnt > 0, acc / np.maximum(cnt, 1), 0.0)
 
 
 def purify(st, p_c: torch.Tensor, nocc: int, mcweeny: int = 3) -> torch.Tensor:

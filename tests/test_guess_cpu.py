@@ -1,7 +1,9 @@
 """Frame machinery of the learned guess on the CPU (oracle SCF, no network):
 the frame blocks of a converged water density do not depend on the water's
 orientation, assembling them back gives the density, and FP64 purification
-leaves a converged (idempotent) density unchanged."""
+leaves a converged (idempotent) density unchanged; the monomial transforms
+of a rotation are exact (on points and under composition), and a cluster's
+frame blocks assemble back to its density on every block the pairs cover."""
 import numpy as np
 import pytest
 import torch
@@ -29,3 +31,35 @@ def test_frame_blocks_are_orientation_independent():
     assert np.abs(back - r.p_c[0].numpy()).max() < 1e-12
     pp = guess.purify(scf.HostState(s), torch.tensor(back), s.deck.nelectrons // 2)
     assert float((pp - r.p_c[0]).abs().max()) < 1e-7
+
+
+def test_monomial_transforms_are_exact():
+    # m_i(R u) = sum_j Q_ij m_j(u) at random points, and Q(R1 R2) = Q(R1) Q(R2)
+    rng = np.random.default_rng(11)
+    R1, R2 = _random_rotation(rng), _random_rotation(rng)
+    u = rng.normal(size=(7, 3))
+    for L in range(4):
+        pws, q = guess.monomial_transforms(L, np.stack([R1, R2, R1 @ R2]))
+        ev = lambda pts: np.stack([pts[:, 0] ** a * pts[:, 1] ** b * pts[:, 2] ** c for a, b, c in pws], axis=1)
+        assert np.abs(ev(u @ R1.T) - ev(u) @ q[0].T).max() < 1e-13
+        assert np.abs(q[2] - q[0] @ q[1]).max() < 1e-13
+
+
+def test_assemble_inverts_the_frame_blocks_of_a_cluster():
+    # any symmetric density of a three-water cluster: its frame blocks, assembled
+    # back, give it on every (A, B) block the pair list covers and zero elsewhere
+    from polymer_b200 import geometry
+    s = system.build_system(geometry.water_deck(3, seed=41), oracle.onee)
+    rng = np.random.default_rng(12)
+    n = s.basis.ncgs
+    a = rng.normal(size=(n, n))
+    info, frames, pairs, x = guess.cluster_data(s)
+    p = (a + a.T) * info.live[:, None] * info.live[None, :]
+    t, w = guess.targets(s, info, frames, pairs, p)
+    back = guess.assemble(s, info, frames, pairs, t)
+    covered = np.zeros((n, n), dtype=bool)
+    for i, j, _ in pairs:
+        covered[np.ix_(info.atom_funcs[i], info.atom_funcs[j])] = True
+    assert covered.any() and not covered.all()
+    assert np.abs(back[covered] - p[covered]).max() < 1e-12 * np.abs(p).max()
+    assert not back[~covered].any()
