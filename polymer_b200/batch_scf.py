@@ -76,7 +76,7 @@ class BatchResult:
     fallback: np.ndarray        # the learned guess was rejected
     p_c: List[torch.Tensor]     # converged contracted densities, input order
     sp2_steps: int              # SP2 products over the run (per group, summed)
-    phases: Optional[dict] = None   # seconds per phase (guess, build, update) when profiled
+    phases: Optional[dict] = None   # seconds per phase when profiled (see run_batch_scf)
 
 
 def _trace(x: torch.Tensor) -> torch.Tensor:
@@ -289,7 +289,10 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     p, p_ref, c_ref, x_ref = (torch.zeros(total, **f64) for _ in range(4))
     dp, dc, dx, p_new = (torch.zeros(total, **f64) for _ in range(4))
     sp2_steps = [0]
-    phases = {'setup': 0.0, 'guess': 0.0, 'build': 0.0, 'update': 0.0, 'host': 0.0}
+    # eager iterations: host (density update), build, update (DIIS, projector);
+    # graph iterations: capture (its eager run and the capture) or replay (the
+    # host's per-molecule bookkeeping, then build and update in one replay)
+    phases = {'setup': 0.0, 'guess': 0.0, 'build': 0.0, 'update': 0.0, 'host': 0.0, 'capture': 0.0, 'replay': 0.0}
     tmark = [time.perf_counter()]
 
     def mark(name):
@@ -445,11 +448,13 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 with torch.cuda.graph(cuda_graph, stream=side):
                     device_step(True)
                 torch.cuda.synchronize(dev)
+                mark('capture')
             else:
                 fb.refresh(dp)
                 cuda_graph.replay()
                 replays += 1
                 host_stats = stats_t.cpu().numpy()
+                mark('replay')
         else:
             device_step(False)
             host_stats = stats_t.cpu().numpy()
