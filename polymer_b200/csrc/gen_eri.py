@@ -25,6 +25,7 @@ Run: python gen_eri.py <out.cuh> [lmax]  (the build does this).
 """
 import itertools
 import math
+import re
 import json
 import sys
 
@@ -327,6 +328,60 @@ def gen_class(LA, LB, LC, LD):
         body.append('    out[%d] = %s;' % (k, o))
     body.append('}')
     return '\n'.join(body), n, g.flops
+
+
+def pass_work(LA, LB, LC, LD, npass, pure_bra=False):
+    """Recursion flops per primitive quartet that the straight-line kernel of a
+    class executes when its outputs are held in `npass` register passes.
+
+    Each pass evaluates only the ops its kept outputs depend on (the rest is dead
+    code in that pass), so the work is the sum over passes of those ops.  The
+    passes split the bra pairs ab, ordered by (|a|, |b|), into slices of
+    ceil(NAB / npass); two-pass (d s| classes split at the level boundary instead
+    (k_gq's AB0/AB1).  With `pure_bra` (both bra shells pure: their lower
+    components carry no coefficient), passes whose pairs all include a lower
+    component skip their work, as k_gq's passes skip their chunks.
+    Returns (flops of one full evaluation, flops summed over the executed
+    passes, number of executed passes)."""
+    g = Gen(LA, LB, LC, LD)
+    cost = {}
+    emit = g.emit
+
+    def counting_emit(expr, flops):
+        name = emit(expr, flops)
+        cost[name] = flops
+        return name
+
+    g.emit = counting_emit
+    outs = g.build()
+    deps = {}
+    for line in g.lines:
+        lhs, rhs = line.split('=', 1)
+        deps[lhs.split()[-1]] = re.findall(r'\bt\d+\b', rhs)
+    ca, cb, cc, cd = comps(LA), comps(LB), comps(LC), comps(LD)
+    nab, ncd = len(ca) * len(cb), len(cc) * len(cd)
+    key = [tot(ca[k // len(cb)]) * 8 + tot(cb[k % len(cb)]) for k in range(nab)]
+    order = sorted(range(nab), key=lambda k: key[k])   # stable, as AbOrder
+    lower = [tot(ca[k // len(cb)]) < LA or tot(cb[k % len(cb)]) < LB for k in range(nab)]
+    nlow = sum(lower)
+    abp = -(-nab // npass)
+    split = npass == 2 and LA == 2 and LB == 0 and nlow * ncd <= 40 and (nab - nlow) * ncd <= 40
+    total, executed = 0, 0
+    for ps in range(npass):
+        a0 = (0 if ps == 0 else nlow) if split else ps * abp
+        a1 = (nlow if ps == 0 else nab) if split else min(a0 + abp, nab)
+        kept = order[a0:a1]
+        if pure_bra and (LA > 0 or LB > 0) and all(lower[k] for k in kept):
+            continue
+        need, stack = set(), [t for k in kept for i in range(ncd) for t in re.findall(r'\bt\d+\b', outs[k * ncd + i])]
+        while stack:
+            t = stack.pop()
+            if t not in need:
+                need.add(t)
+                stack.extend(deps[t])
+        total += sum(cost[t] for t in need)
+        executed += 1
+    return g.flops, total, executed
 
 
 HEADER = '''// Generated by polymer_b200/csrc/gen_eri.py -- do not edit.

@@ -91,3 +91,16 @@ def test_pure_table_matches_the_full_table(cls, ket):
                         assert pure[k] == 0.0 and pure_table[2][k] == 0
                     k += 1
     assert k == len(full)
+
+
+@pytest.mark.parametrize('cls,npass', [((1, 1, 1, 0), 2), ((2, 0, 1, 0), 2), ((2, 1, 1, 1), 14), ((2, 2, 1, 0), 10)])
+def test_pass_work_accounting(cls, npass):
+    # one pass evaluates the whole recursion once; more passes repeat the ops
+    # their outputs share, never less than one evaluation, and skipping the
+    # all-lower passes of pure bra shells only removes work
+    full, one, n1 = gen_eri.pass_work(*cls, 1)
+    assert one == full and n1 == 1
+    _, many, n = gen_eri.pass_work(*cls, npass)
+    assert n == npass and full <= many <= npass * full
+    _, pure, npure = gen_eri.pass_work(*cls, npass, pure_bra=True)
+    assert npure <= npass and pure <= many
