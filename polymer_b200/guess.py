@@ -235,39 +235,6 @@ def _layout(info: AOInfo, a: int, cache: dict):
     return cache[key]
 
 
-def _u_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
-    key = (_layout(info, a, cache), id(R))
-    if key not in cache:
-        cache[key] = frame_transform(info, R, info.atom_funcs[a], cache.setdefault(('q', id(R)), {}))
-    return cache[key]
-
-
-def _v_for_atom(info: AOInfo, R: np.ndarray, a: int, cache: dict) -> np.ndarray:
-    key = ('inv', _layout(info, a, cache), id(R))
-    if key not in cache:
-        cache[key] = np.linalg.inv(_u_for_atom(info, R, a, cache))
-    return cache[key]
-
-
-def targets(sysm: System, info: AOInfo, frames, pairs, p_c: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
-    """Frame blocks of a converged contracted density, flattened to MAXF x MAXF, and their weights."""
-    t = np.zeros((len(pairs), MAXF * MAXF))
-    w = np.zeros_like(t)
-    cache: dict = {}
-    for k, (a, b, m) in enumerate(pairs):
-        R = frames[m][1]
-        fa, fb = info.atom_funcs[a], info.atom_funcs[b]
-        ua, ub = _u_for_atom(info, R, a, cache), _u_for_atom(info, R, b, cache)
-        blk = ua.T @ p_c[np.ix_(fa, fb)] @ ub
-        full = np.zeros((MAXF, MAXF))
-        full[:len(fa), :len(fb)] = blk
-        t[k] = full.ravel()
-        wm = np.zeros((MAXF, MAXF))
-        wm[:len(fa), :len(fb)] = 1.0
-        w[k] = wm.ravel()
-    return t, w
-
-
 def _layout_plan(info: AOInfo, a: int, cache: dict):
     """Atom a's layout and its frame transform as entries per degree L: (row,
     column, monomial row, monomial column, norm ratio) arrays, so that
@@ -292,9 +259,9 @@ def _layout_plan(info: AOInfo, a: int, cache: dict):
     return lay, cache[key]
 
 
-def frame_inverses(info: AOInfo, frames, natom: int, cache: dict) -> dict:
-    """Per atom layout: V = U^-1 of every water's frame (nwater x nf x nf), the
-    monomial transforms of all frames computed at once per degree."""
+def frame_transforms(info: AOInfo, frames, natom: int, cache: dict) -> dict:
+    """Per atom layout: U of every water's frame (nwater x nf x nf), P_frame =
+    U^T P_lab U, the monomial transforms of all frames computed at once per degree."""
     Rs = np.stack([fr[1] for fr in frames]) if frames else np.zeros((0, 3, 3))
     q: Dict[int, np.ndarray] = {}
     out: dict = {}
@@ -307,19 +274,19 @@ def frame_inverses(info: AOInfo, frames, natom: int, cache: dict) -> dict:
             if L not in q:
                 q[L] = monomial_transforms(L, Rs)[1]
             u[:, ui, uj] = q[L][:, mi, mj] * ratio
-        out[lay] = np.linalg.inv(u)
+        out[lay] = u
     return out
 
 
-def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.ndarray:
-    """Laboratory contracted density from predicted frame blocks (symmetrised:
-    each block enters at (A,B) and, transposed, at (B,A); entries are averaged)."""
-    n = sysm.basis.ncgs
-    if not pairs:
-        return np.zeros((n, n))
-    natom = sysm.deck.natom
-    cache: dict = {}
-    vinv = frame_inverses(info, frames, natom, cache)
+def frame_inverses(info: AOInfo, frames, natom: int, cache: dict) -> dict:
+    """Per atom layout: V = U^-1 of every water's frame (nwater x nf x nf)."""
+    return {lay: np.linalg.inv(u) for lay, u in frame_transforms(info, frames, natom, cache).items()}
+
+
+def _pair_groups(info: AOInfo, pairs, natom: int, cache: dict):
+    """The pairs grouped by the layouts of their two atoms (first-appearance
+    order): per group the pair indices, both layouts, the owner waters and the
+    function indices of A (rows) and of B (columns)."""
     lays = [_layout(info, a, cache) for a in range(natom)]
     lay_id = {lay: k for k, lay in enumerate(dict.fromkeys(lays))}
     atom_lay = np.array([lay_id[lay] for lay in lays])
@@ -331,17 +298,42 @@ def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.
     P = np.asarray(pairs)
     A, B, M = P[:, 0], P[:, 1], P[:, 2]
     combo = atom_lay[A] * len(lay_id) + atom_lay[B]
-    idx, val = [], []
-    for cb in dict.fromkeys(combo.tolist()):   # first-appearance order
+    for cb in dict.fromkeys(combo.tolist()):
         ks = np.nonzero(combo == cb)[0]
         la, lb = by_id[cb // len(lay_id)], by_id[cb % len(lay_id)]
         na, nb = len(la[1]), len(lb[1])
         if na == 0 or nb == 0:
             continue
-        va, vb = vinv[la][M[ks]], vinv[lb][M[ks]]
-        blk = pred[ks].reshape(-1, MAXF, MAXF)[:, :na, :nb]
-        lab = va.transpose(0, 2, 1) @ (blk @ vb)
-        r, c = funcs[A[ks], :na], funcs[B[ks], :nb]
+        yield ks, la, lb, M[ks], funcs[A[ks], :na], funcs[B[ks], :nb]
+
+
+def targets(sysm: System, info: AOInfo, frames, pairs, p_c: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Frame blocks of a converged contracted density, flattened to MAXF x MAXF, and their weights."""
+    t = np.zeros((len(pairs), MAXF, MAXF))
+    w = np.zeros_like(t)
+    if pairs:
+        cache: dict = {}
+        u = frame_transforms(info, frames, sysm.deck.natom, cache)
+        for ks, la, lb, m, r, c in _pair_groups(info, pairs, sysm.deck.natom, cache):
+            blk = p_c[r[:, :, None], c[:, None, :]]
+            t[ks, :r.shape[1], :c.shape[1]] = u[la][m].transpose(0, 2, 1) @ blk @ u[lb][m]
+            w[ks, :r.shape[1], :c.shape[1]] = 1.0
+    return t.reshape(len(pairs), -1), w.reshape(len(pairs), -1)
+
+
+def assemble(sysm: System, info: AOInfo, frames, pairs, pred: np.ndarray) -> np.ndarray:
+    """Laboratory contracted density from predicted frame blocks (symmetrised:
+    each block enters at (A,B) and, transposed, at (B,A); entries are averaged)."""
+    n = sysm.basis.ncgs
+    if not pairs:
+        return np.zeros((n, n))
+    natom = sysm.deck.natom
+    cache: dict = {}
+    vinv = frame_inverses(info, frames, natom, cache)
+    idx, val = [], []
+    for ks, la, lb, m, r, c in _pair_groups(info, pairs, natom, cache):
+        blk = pred[ks].reshape(-1, MAXF, MAXF)[:, :r.shape[1], :c.shape[1]]
+        lab = vinv[la][m].transpose(0, 2, 1) @ (blk @ vinv[lb][m])
         idx.append((r[:, :, None] * n + c[:, None, :]).ravel())
         val.append(lab.ravel())
         idx.append((c[:, None, :] * n + r[:, :, None]).ravel())   # the transpose: (B,A) gets lab[k].T

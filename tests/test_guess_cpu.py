@@ -2,8 +2,9 @@
 the frame blocks of a converged water density do not depend on the water's
 orientation, assembling them back gives the density, and FP64 purification
 leaves a converged (idempotent) density unchanged; the monomial transforms
-of a rotation are exact (on points and under composition), and a cluster's
-frame blocks assemble back to its density on every block the pairs cover."""
+of a rotation are exact (on points and under composition), a cluster's frame
+blocks assemble back to its density on every block the pairs cover, and the
+frame transforms computed for all waters at once equal the per-water form."""
 import numpy as np
 import pytest
 import torch
@@ -63,3 +64,16 @@ def test_assemble_inverts_the_frame_blocks_of_a_cluster():
     assert covered.any() and not covered.all()
     assert np.abs(back[covered] - p[covered]).max() < 1e-12 * np.abs(p).max()
     assert not back[~covered].any()
+
+
+def test_batched_frame_transforms_match_the_per_water_form():
+    from polymer_b200 import geometry
+    s = system.build_system(geometry.water_deck(4, seed=43), oracle.onee)
+    info, frames, pairs, x = guess.cluster_data(s)
+    cache = {}
+    u = guess.frame_transforms(info, frames, s.deck.natom, cache)
+    for m, (_, R, atoms) in enumerate(frames):
+        for a in atoms:
+            ref = guess.frame_transform(info, R, info.atom_funcs[a])
+            got = u[guess._layout(info, a, cache)][m]
+            assert np.abs(got - ref).max() < 1e-14
