@@ -4,7 +4,9 @@ orientation, assembling them back gives the density, and FP64 purification
 leaves a converged (idempotent) density unchanged; the monomial transforms
 of a rotation are exact (on points and under composition), a cluster's frame
 blocks assemble back to its density on every block the pairs cover, and the
-frame transforms computed for all waters at once equal the per-water form."""
+frame transforms computed for all waters at once equal the per-water form;
+the basis's shell groups (6-31G** with cumulative sp shells, cc-pVDZ) are
+whole shell instances: one atom, one angular momentum, one radial part."""
 import numpy as np
 import pytest
 import torch
@@ -77,3 +79,28 @@ def test_batched_frame_transforms_match_the_per_water_form():
             ref = guess.frame_transform(info, R, info.atom_funcs[a])
             got = u[guess._layout(info, a, cache)][m]
             assert np.abs(got - ref).max() < 1e-14
+
+
+@pytest.mark.parametrize('which', ['alkane_631gss', 'water_ccpvdz'])
+def test_shell_groups_of_the_basis(which):
+    # every live contracted function sits in exactly one group; a group is one
+    # shell instance: one atom, one angular momentum, all its Cartesian
+    # components (1, 3 or 6) with the same radial part, in function order
+    from polymer_b200 import geometry
+    deck = geometry.alkane_deck(2) if which == 'alkane_631gss' else geometry.water_deck(2, seed=44)
+    s = system.build_system(deck, oracle.onee)
+    info = guess.ao_info(s)
+    members = sorted(i for g in info.groups for i in g)
+    assert members == list(np.nonzero(info.live)[0])
+    firsts = [g[0] for g in info.groups]
+    assert firsts == sorted(firsts)
+    cc = s.basis.cc
+    for g in info.groups:
+        L = {sum(info.powers[i]) for i in g}
+        assert len(L) == 1 and len(g) == {0: 1, 1: 3, 2: 6}[L.pop()]
+        assert len({int(info.atom[i]) for i in g}) == 1
+        assert len({info.powers[i] for i in g}) == len(g)
+        zs = [tuple(sorted(np.round(s.basis.zt[np.nonzero(cc[i])[0]], 10))) for i in g]
+        assert len(set(zs)) == 1
+    for a, funcs in enumerate(info.atom_funcs):
+        assert all(info.atom[i] == a and info.live[i] for i in funcs)
