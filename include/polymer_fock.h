@@ -162,7 +162,9 @@ int32_t pfe_batch_destroy(pfe_batch *b);
 /* Screened-quartet census and algorithmic FLOPs of the last setup (per Fock build). */
 typedef struct pfe_census {
   double quartets;          /* screened primitive-shell quartets computed per build   */
-  double quartets_ref;      /* the same work counted the reference's way (no symmetry) */
+  double quartets_ref;      /* lattices: the same work counted the reference's way (no
+                               symmetry); molecules: 0 (not counted; the reference's
+                               loop evaluates up to 8 orderings of each quartet)     */
   double flops;             /* FP64/FP32 recursion + digestion flops per build        */
   double quartets_fp32;     /* quartets routed to FP32 recursion (mixed mode)          */
   int64_t pairs;            /* significant primitive-shell pairs kept                 */
