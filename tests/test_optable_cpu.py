@@ -8,7 +8,10 @@ evaluated on the CPU with the op semantics the kernels use (eval_op):
   for the others -- so a chunk whose lower bra components carry no
   coefficient gets the same X from either table; the bra-and-ket table does
   the same for outputs whose bra and ket components are all top-level, and
-  drops ops beyond the pure-bra table's.
+  drops ops beyond the pure-bra table's;
+* the straight-line kernels' register passes: the work each pass executes is
+  at least one evaluation and at most npass of them, and the pass counts in
+  straight_npass, the launcher table and the large classes' dispatch agree.
 """
 import os
 import sys
@@ -104,3 +107,45 @@ def test_pass_work_accounting(cls, npass):
     assert n == npass and full <= many <= npass * full
     _, pure, npure = gen_eri.pass_work(*cls, npass, pure_bra=True)
     assert npure <= npass and pure <= many
+
+
+def test_pass_tables_agree():
+    # the pass count of each straight-line class lives in three hand-kept
+    # places: straight_npass (census, launch count), the launcher table of the
+    # smaller classes and the dispatch of the large ones (one unit per class,
+    # FP64 and batch instantiations); they must name the same classes and passes
+    import re
+    csrc = os.path.join(os.path.dirname(__file__), '..', 'polymer_b200', 'csrc')
+    kern = open(os.path.join(csrc, 'pfe_mol_kernels.cuh')).read()
+    body = kern[kern.index('static inline int straight_npass'):]
+    nums = [int(v) for v in re.findall(r'\d+', body[body.index('{{'):body.index('}};')])]
+    npass = [nums[6 * i:6 * i + 6] for i in range(6)]
+    cls = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+    seen = {}
+    table = kern[kern.index('static const LaunchFn table[6][6]'):]
+    table = table[:table.index('#undef Q')]
+    rows = re.findall(r'\{((?:Q\([^)]*\)|nullptr|[\s,])*)\}', table)
+    assert len(rows) == 6
+    for r, row in enumerate(rows):
+        entries = re.findall(r'Q\([^)]*\)|nullptr', row)
+        assert len(entries) == 6
+        for c, entry in enumerate(entries):
+            m = re.match(r'Q\((\d), (\d), (\d), (\d), (\d+)\)', entry)
+            if m:
+                seen[(r, c)] = tuple(int(v) for v in m.groups())
+    big = open(os.path.join(csrc, 'pfe_mol_big1.cu')).read()
+    for m in re.finditer(r'case (\d) \* 8 \+ (\d): return &launch_q<(\d), (\d), (\d), (\d), (\d+), false, BATCH>', big):
+        key = (int(m.group(1)), int(m.group(2)))
+        assert key not in seen
+        seen[key] = tuple(int(v) for v in m.groups()[2:])
+        inst = 'template void launch_q<%s, %s, %s, %s, %s, false, %%s>' % m.groups()[2:]
+        units = ''.join(open(os.path.join(csrc, 'pfe_mol_big%d.cu' % k)).read() for k in range(1, 9))
+        for batch in ('false', 'true'):
+            assert any(line.startswith(inst % batch) for line in units.splitlines()), inst % batch
+    assert len(seen) == sum(1 for row in npass for v in row if v) == 19
+    for cb in range(6):
+        for ck in range(6):
+            if npass[cb][ck] == 0:
+                assert (cb, ck) not in seen
+            else:
+                assert seen[(cb, ck)] == cls[cb] + cls[ck] + (npass[cb][ck],)
