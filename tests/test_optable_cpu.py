@@ -11,7 +11,9 @@ evaluated on the CPU with the op semantics the kernels use (eval_op):
   drops ops beyond the pure-bra table's;
 * the straight-line kernels' register passes: the work each pass executes is
   at least one evaluation and at most npass of them, and the pass counts in
-  straight_npass, the launcher table and the large classes' dispatch agree.
+  straight_npass, the launcher table and the large classes' dispatch agree;
+* the hand-kept op-table lookups and interpreter dispatch return each class's
+  own tables and kernels, for exactly the classes the generator serves.
 """
 import os
 import sys
@@ -149,3 +151,39 @@ def test_pass_tables_agree():
                 assert (cb, ck) not in seen
             else:
                 assert seen[(cb, ck)] == cls[cb] + cls[ck] + (npass[cb][ck],)
+
+
+def test_table_lookups_match_the_generator():
+    # host_optable*, hand-kept: each case returns the table of its own class,
+    # the full tables cover every class, the pure-bra ones every bra class with
+    # a p or d shell, and the bra-and-ket ones exactly the classes the
+    # generator emits them for
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), '..', 'polymer_b200', 'csrc', 'pfe_eri.cu')).read()
+    cls = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
+
+    def cases(fn, suffix):
+        body = src[src.index('const OpTableHost* %s(int cb, int ck) {' % fn):]
+        body = body[:body.index('\n}\n')]
+        got = set()
+        for m in re.finditer(r'case (?:(\d) \* 8 \+ (\d)|0): return &op_(\d{4})%s;' % suffix, body):
+            cb, ck = (int(m.group(1)), int(m.group(2))) if m.group(1) else (0, 0)
+            assert m.group(3) == '%d%d%d%d' % (cls[cb] + cls[ck]), m.group(0)
+            got.add((cb, ck))
+        return got
+
+    every = {(cb, ck) for cb in range(6) for ck in range(cb + 1)}
+    assert cases('host_optable', '') == every
+    assert cases('host_optable_pure', '_pure') == {(b, k) for b, k in every if cls[b][0] >= 1}
+    assert cases('host_optable_pure2', '_pure2') == {
+        (b, k) for b, k in every if cls[b][0] >= 1 and cls[k][0] >= 1 and gen_eri.pure_ket_gains(*(cls[b] + cls[k]))}
+    # the interpreters' template dispatch (variants() of pfe_mol.cu), likewise
+    mol = open(os.path.join(os.path.dirname(__file__), '..', 'polymer_b200', 'csrc', 'pfe_mol.cu')).read()
+    body = mol[mol.index('static Variants variants(int cb, int ck) {'):]
+    body = body[:body.index('\n}\n')]
+    got = set()
+    for m in re.finditer(r'case (\d+): return V\((\d), (\d), (\d), (\d)\);', body):
+        cb, ck = divmod(int(m.group(1)), 8)
+        assert tuple(int(v) for v in m.groups()[1:]) == cls[cb] + cls[ck], m.group(0)
+        got.add((cb, ck))
+    assert got == every
