@@ -41,7 +41,7 @@ def test_library_exports_every_symbol():
 
 
 @pytest.mark.parametrize('cname,pyt', [('pfe_args', capi.PfeArgs), ('pfe_onee_args', capi.PfeOneeArgs),
-                                       ('pfe_census', capi.PfeCensus)])
+                                       ('pfe_census', capi.PfeCensus), ('pfe_kernel_stat', capi.PfeKernelStat)])
 def test_struct_layout_matches_header(cname, pyt):
     fields = [f[0] for f in pyt._fields_]
     src = ['#include <stdio.h>', '#include <stddef.h>', '#include "%s"' % HEADER, 'int main(void){',
