@@ -58,3 +58,29 @@ def test_struct_layout_matches_header(cname, pyt):
     assert vals[0] == ctypes.sizeof(pyt)
     for f, off in zip(fields, vals[1:]):
         assert getattr(pyt, f).offset == off, f
+
+
+def test_ctypes_signatures_match_the_headers():
+    # every prototype of include/*.h against the argtypes/restype capi.py sets:
+    # argument count, pointer or not, and the scalar type of the rest
+    root = os.path.join(os.path.dirname(__file__), '..', 'include')
+    hdr = ''.join(open(os.path.join(root, f)).read() for f in sorted(os.listdir(root)) if f.endswith('.h'))
+    hdr = re.sub(r'/\*.*?\*/', '', hdr, flags=re.S)
+    protos = {m.group(2): (m.group(1), m.group(3))
+              for m in re.finditer(r'\b(int32_t|void|double)\s+(pfe_\w+)\s*\(([^)]*)\)\s*;', hdr)}
+    assert len(protos) >= len(capi.EXPORTS)
+    scalar = {'int32_t': ctypes.c_int32, 'int64_t': ctypes.c_int64, 'double': ctypes.c_double,
+              'float': ctypes.c_float}
+    L = capi.lib()
+    for name, (ret, args) in protos.items():
+        fn = getattr(L, name)
+        params = [a.strip() for a in args.split(',')] if args.strip() not in ('', 'void') else []
+        assert fn.argtypes is not None and len(fn.argtypes) == len(params), name
+        for p, t in zip(params, fn.argtypes):
+            if '*' in p:
+                assert t is ctypes.c_void_p or t is ctypes.c_char_p or issubclass(t, ctypes._Pointer), (name, p)
+            else:
+                ctype = p.replace('const', '').split()[0]
+                assert t is scalar[ctype], (name, p, t)
+        if ret != 'void':
+            assert fn.restype is scalar[ret], (name, ret)
