@@ -2,8 +2,13 @@
 
 * every entry point include/polymer_fock.h declares is exported by the built
   libpolymer_fock.so (no compute call is made);
-* the ctypes mirrors of pfe_args / pfe_onee_args / pfe_census have exactly the
-  C layout (offsets measured by compiling a probe against the header).
+* the ctypes mirrors of pfe_args / pfe_onee_args / pfe_census /
+  pfe_kernel_stat have exactly the C layout (offsets measured by compiling a
+  probe against the header);
+* the ctypes signature of every prototype in include/*.h matches it (count,
+  pointers, scalar and return types);
+* the Fortran shim's BIND(C) type in the integration notes has pfe_args'
+  members in order, with the same kinds and array lengths.
 """
 import ctypes
 import os
@@ -84,3 +89,29 @@ def test_ctypes_signatures_match_the_headers():
                 assert t is scalar[ctype], (name, p, t)
         if ret != 'void':
             assert fn.restype is scalar[ret], (name, ret)
+
+
+def test_fortran_shim_type_matches_pfe_args():
+    # the BIND(C) type of the Fortran shim given in the integration notes (no
+    # Fortran compiler here to check it): same members, order, kinds and array
+    # lengths as pfe_args, whose ctypes mirror the layout test pins to the header
+    doc = open(os.path.join(os.path.dirname(__file__), '..', 'INTEGRATION.md')).read()
+    body = doc[doc.index('TYPE, BIND(C) :: PFE_ARGS'):doc.index('END TYPE')]
+    kinds = {'INTEGER(C_INT32_T)': ctypes.c_int32, 'REAL(C_DOUBLE)': ctypes.c_double, 'TYPE(C_PTR)': None}
+    fortran = []
+    for line in body.splitlines()[1:]:
+        if not line.strip():
+            continue
+        m = re.match(r'\s*(INTEGER\(C_INT32_T\)|REAL\(C_DOUBLE\)|TYPE\(C_PTR\))\s*::\s*(.*)', line)
+        assert m, line
+        for name, n in re.findall(r'(\w+)(?:\((\d+)\))?', m.group(2)):
+            fortran.append((name.lower(), kinds[m.group(1)], int(n) if n else 1))
+    c = []
+    for name, t in capi.PfeArgs._fields_:
+        if issubclass(t, ctypes.Array):
+            c.append((name, t._type_, t._length_))
+        elif issubclass(t, ctypes._Pointer) or t is ctypes.c_void_p:
+            c.append((name, None, 1))
+        else:
+            c.append((name, t, 1))
+    assert fortran == c
