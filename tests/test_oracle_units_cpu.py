@@ -1,0 +1,64 @@
+"""Unit checks of the oracle against closed forms, independent of the
+reference's recorded outputs (which pin it end to end through SCF energies):
+
+* the Boys table IGAMMA(i, m) = F_m(i/20) of FMT_PRELIMINARY, from the oracle
+  and from the host mirror, against F_m(T) = Gamma(m+1/2) P(m+1/2, T) /
+  (2 T^(m+1/2)) (P the regularised lower incomplete gamma), F_m(0) = 1/(2m+1);
+* C_C and X_C of an s-only basis (four centres, two uncontracted s primitives
+  each, no screening) against J and K assembled from the closed-form primitive
+  integrals (ab|cd) = 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) K_ab K_cd
+  F_0(rho |P-Q|^2), contracted with CC as FOURINDEX_ERI does.
+"""
+import numpy as np
+from scipy.special import erf, gamma, gammainc
+
+import oracle
+from polymer_b200 import inputdeck, system
+
+
+def _boys(m, t):
+    t = np.asarray(t, dtype=float)
+    out = np.full(t.shape, 1.0 / (2 * m + 1))
+    pos = t > 0.0
+    out[pos] = gamma(m + 0.5) * gammainc(m + 0.5, t[pos]) / (2.0 * t[pos] ** (m + 0.5))
+    return out
+
+
+def test_boys_table_matches_the_closed_form():
+    t = np.arange(1701) / 20.0
+    for tab in (oracle.fmt_table(), system.fmt_table()):
+        tab = np.asarray(tab)
+        assert tab.shape == (1701, 28)
+        for m in range(28):
+            ref = _boys(m, t)
+            assert np.all(np.abs(tab[:, m] - ref) <= 1e-12 * ref), m
+
+
+def test_s_only_fock_matches_closed_form_integrals():
+    lib = {'H': [['S', 1.0, [[1.3, 1.0]]], ['S', 1.0, [[0.35, 1.0]]]]}
+    xyz = [[0.0, 0.0, 0.0], [1.4, 0.2, 0.0], [0.3, 1.7, 0.5], [-1.1, 0.6, 1.2]]   # bohr
+    deck = inputdeck.make_deck([1, 1, 1, 1], xyz, 'STO-3G', inttol=0.0)
+    s = system.build_system(deck, oracle.onee, library=lib)
+    b = s.basis
+    assert not (np.any(b.pax) or np.any(b.pay) or np.any(b.paz))
+    cc = b.cc
+    rng = np.random.default_rng(7)
+    a = rng.normal(size=(b.ncgs, b.ncgs))
+    pp = cc.T @ (a + a.T) @ cc               # a decontracted density, as the reference's P_P
+    c_c, x_c = oracle.fourindex_eri(s, pp[None])
+
+    pos, z = b.pgs, b.zt
+    zeta = z[:, None] + z[None, :]
+    centre = (z[:, None, None] * pos[:, None, :] + z[None, :, None] * pos[None, :, :]) / zeta[..., None]
+    kab = np.exp(-z[:, None] * z[None, :] / zeta * ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    zz = zeta[:, :, None, None] + zeta[None, None, :, :]
+    rho = zeta[:, :, None, None] * zeta[None, None, :, :] / zz
+    t = rho * ((centre[:, :, None, None, :] - centre[None, None, :, :, :]) ** 2).sum(-1)
+    f0 = np.where(t > 1e-14, 0.5 * np.sqrt(np.pi / np.maximum(t, 1e-300)) * erf(np.sqrt(t)), 1.0 - t / 3.0)
+    eri = (2.0 * np.pi ** 2.5 / (zeta[:, :, None, None] * zeta[None, None, :, :] * np.sqrt(zz))
+           * kab[:, :, None, None] * kab[None, None, :, :] * f0)
+    j_p = np.einsum('pqrs,rs->pq', eri, pp)          # C_P(i,j) += P_P(k,l) (ij|kl)
+    k_p = np.einsum('pqrs,rq->ps', eri, pp)          # X_P(i,l) += P_P(k,j) (ij|kl)
+    j_c, k_c = cc @ j_p @ cc.T, cc @ k_p @ cc.T
+    assert np.abs(c_c[0] - j_c).max() <= 1e-12 * np.abs(j_c).max()
+    assert np.abs(x_c[0] - k_c).max() <= 1e-12 * np.abs(k_c).max()
