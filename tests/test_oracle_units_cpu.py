@@ -7,7 +7,10 @@ reference's recorded outputs (which pin it end to end through SCF energies):
 * C_C and X_C of an s-only basis (four centres, two uncontracted s primitives
   each, no screening) against J and K assembled from the closed-form primitive
   integrals (ab|cd) = 2 pi^(5/2) / (zeta eta sqrt(zeta+eta)) K_ab K_cd
-  F_0(rho |P-Q|^2), contracted with CC as FOURINDEX_ERI does.
+  F_0(rho |P-Q|^2), contracted with CC as FOURINDEX_ERI does;
+* the (p, s) blocks of C_C and X_C of a basis with a p shell, for a density
+  on the s primitives, against the same closed form differentiated in the p
+  primitive's centre (a complex step: exact to rounding).
 """
 import numpy as np
 from scipy.special import erf, gamma, gammainc
@@ -54,7 +57,7 @@ def test_s_only_fock_matches_closed_form_integrals():
     zz = zeta[:, :, None, None] + zeta[None, None, :, :]
     rho = zeta[:, :, None, None] * zeta[None, None, :, :] / zz
     t = rho * ((centre[:, :, None, None, :] - centre[None, None, :, :, :]) ** 2).sum(-1)
-    f0 = np.where(t > 1e-14, 0.5 * np.sqrt(np.pi / np.maximum(t, 1e-300)) * erf(np.sqrt(t)), 1.0 - t / 3.0)
+    f0 = _f0(t)
     eri = (2.0 * np.pi ** 2.5 / (zeta[:, :, None, None] * zeta[None, None, :, :] * np.sqrt(zz))
            * kab[:, :, None, None] * kab[None, None, :, :] * f0)
     j_p = np.einsum('pqrs,rs->pq', eri, pp)          # C_P(i,j) += P_P(k,l) (ij|kl)
@@ -62,3 +65,65 @@ def test_s_only_fock_matches_closed_form_integrals():
     j_c, k_c = cc @ j_p @ cc.T, cc @ k_p @ cc.T
     assert np.abs(c_c[0] - j_c).max() <= 1e-12 * np.abs(j_c).max()
     assert np.abs(x_c[0] - k_c).max() <= 1e-12 * np.abs(k_c).max()
+
+
+def _f0(t):
+    """F_0(t) = sqrt(pi) erf(sqrt t) / (2 sqrt t), also for complex t: the ratio
+    is even in sqrt(t), so it does not depend on the branch of the root."""
+    r = np.sqrt(t)
+    with np.errstate(divide='ignore', invalid='ignore'):
+        f = 0.5 * np.sqrt(np.pi) * erf(r) / r
+    return np.where(t == 0, 1.0, f)
+
+
+def _ss_rows(pos, z, p):
+    """(p q|r s) of s primitives for one bra primitive p and all q, r, s; pos may
+    be complex (the closed form is analytic in the centres)."""
+    zeta = z[:, None] + z[None, :]
+    centre = (z[:, None, None] * pos[:, None, :] + z[None, :, None] * pos[None, :, :]) / zeta[..., None]
+    kab = np.exp(-z[:, None] * z[None, :] / zeta * ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1))
+    zz = zeta[p][:, None, None] + zeta[None, :, :]
+    rho = zeta[p][:, None, None] * zeta[None, :, :] / zz
+    t = rho * ((centre[p][:, None, None, :] - centre[None, :, :, :]) ** 2).sum(-1)
+    f0 = _f0(t)
+    return 2.0 * np.pi ** 2.5 / (zeta[p][:, None, None] * zeta[None] * np.sqrt(zz)) * kab[p][:, None, None] * kab[None] * f0
+
+
+def test_p_s_blocks_match_the_derivative_of_the_closed_form():
+    # a p primitive (x - A_x) e^{-a|r-A|^2} is (1/2a) d/dA_x of the s primitive,
+    # so with the density on s primitives only, the (p, s) blocks of J and K are
+    # (1/2a) d/dA of s-only sums: taken by a complex step (exact to rounding)
+    lib = {'H': [['S', 1.0, [[1.3, 1.0]]], ['S', 1.0, [[0.35, 1.0]]]],
+           'He': [['S', 1.0, [[2.1, 1.0]]], ['P', 1.0, [[0.8, 1.0]]]]}
+    xyz = [[0.0, 0.0, 0.0], [1.4, 0.2, 0.3], [0.3, 1.7, -0.5]]   # bohr
+    s = system.build_system(inputdeck.make_deck([2, 1, 1], xyz, 'STO-3G', inttol=0.0), oracle.onee, library=lib)
+    b = s.basis
+    cc = b.cc
+    lsum = b.pax + b.pay + b.paz
+    live = np.any(cc != 0.0, axis=0)
+    s_prim = np.nonzero(live & (lsum == 0))[0]
+    p_prim = np.nonzero(live & (lsum == 1))[0]
+    assert len(p_prim) == 3 and np.all(np.count_nonzero(cc[:, live], axis=0) == 1)
+    rng = np.random.default_rng(9)
+    pp = np.zeros((b.npgs, b.npgs))
+    a = rng.normal(size=(len(s_prim), len(s_prim)))
+    pp[np.ix_(s_prim, s_prim)] = a + a.T
+    c_c, x_c = oracle.fourindex_eri(s, pp[None])
+
+    zs = b.zt[s_prim]
+    h = 1e-30
+    for p in p_prim:
+        axis = int(np.argmax([b.pax[p], b.pay[p], b.paz[p]]))
+        pos = np.vstack([b.pgs[p], b.pgs[s_prim]]).astype(complex)   # row 0: the p primitive's centre
+        pos[0, axis] += 1j * h
+        z = np.concatenate([[b.zt[p]], zs])
+        d = _ss_rows(pos, z, 0)[1:, 1:, 1:].imag / h / (2.0 * b.zt[p])   # (p q|r s), q, r, s over s_prim
+        ps = pp[np.ix_(s_prim, s_prim)]
+        j_p = np.einsum('qrs,rs->q', d, ps)           # C_P(p, q)
+        k_p = np.einsum('qrs,rq->s', d, ps)           # X_P(p, l)
+        i = int(np.nonzero(cc[:, p])[0][0])
+        for q_k, q in enumerate(s_prim):
+            jq = int(np.nonzero(cc[:, q])[0][0])
+            scale = cc[i, p] * cc[jq, q]
+            assert abs(c_c[0][i, jq] - scale * j_p[q_k]) <= 1e-12 * np.abs(c_c[0]).max()
+            assert abs(x_c[0][i, jq] - scale * k_p[q_k]) <= 1e-12 * np.abs(x_c[0]).max()
