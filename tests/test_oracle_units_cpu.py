@@ -10,7 +10,9 @@ reference's recorded outputs (which pin it end to end through SCF energies):
   F_0(rho |P-Q|^2), contracted with CC as FOURINDEX_ERI does;
 * the (p, s) blocks of C_C and X_C of a basis with a p shell, for a density
   on the s primitives, against the same closed form differentiated in the p
-  primitive's centre (a complex step: exact to rounding).
+  primitive's centre (a complex step: exact to rounding);
+* the (d, s) blocks likewise, from second derivatives of the closed form in
+  the d primitive's centre (torch autograd in FP64).
 """
 import numpy as np
 from scipy.special import erf, gamma, gammainc
@@ -127,3 +129,73 @@ def test_p_s_blocks_match_the_derivative_of_the_closed_form():
             scale = cc[i, p] * cc[jq, q]
             assert abs(c_c[0][i, jq] - scale * j_p[q_k]) <= 1e-12 * np.abs(c_c[0]).max()
             assert abs(x_c[0][i, jq] - scale * k_p[q_k]) <= 1e-12 * np.abs(x_c[0]).max()
+
+
+def test_d_s_blocks_match_second_derivatives_of_the_closed_form():
+    # a Cartesian d primitive is a second derivative of the s primitive in its
+    # centre: (x-A_x)^2 e = (d2/dA_x2 + 2a) e / (4a^2), (x-A_x)(y-A_y) e =
+    # d2/dA_x dA_y e / (4a^2); torch autograd (FP64) differentiates the closed
+    # form; with the density on s primitives the (d, s) blocks of C_C and X_C
+    # follow, through CC (whichever contracted functions the d shell makes)
+    import torch
+    lib = {'H': [['S', 1.0, [[1.3, 1.0]]], ['S', 1.0, [[0.35, 1.0]]]],
+           'He': [['S', 1.0, [[2.1, 1.0]]], ['D', 1.0, [[0.9, 1.0]]]]}
+    xyz = [[0.0, 0.0, 0.0], [1.4, 0.2, 0.3], [0.3, 1.7, -0.5]]   # bohr
+    s = system.build_system(inputdeck.make_deck([2, 1, 1], xyz, 'STO-3G', inttol=0.0), oracle.onee, library=lib)
+    b = s.basis
+    cc = b.cc
+    pw = np.stack([b.pax, b.pay, b.paz], axis=1).astype(int)
+    live = np.any(cc != 0.0, axis=0)
+    s_prim = np.nonzero(live & (pw.sum(1) == 0))[0]
+    d_prim = np.nonzero(live & (pw.sum(1) == 2))[0]
+    assert len(d_prim) == 6
+    rng = np.random.default_rng(10)
+    pp = np.zeros((b.npgs, b.npgs))
+    a = rng.normal(size=(len(s_prim), len(s_prim)))
+    pp[np.ix_(s_prim, s_prim)] = a + a.T
+    c_c, x_c = oracle.fourindex_eri(s, pp[None])
+
+    t64 = dict(dtype=torch.float64)
+    zs = torch.tensor(b.zt[s_prim], **t64)
+    ps = torch.tensor(pp[np.ix_(s_prim, s_prim)], **t64)
+    cs = torch.tensor(b.pgs[s_prim], **t64)
+
+    def sums(centre, za):
+        # (a q|r s) over s primitives q, r, s for an s primitive a at `centre`,
+        # contracted with the density: J row (q) and K row (l)
+        zq = za + zs
+        pq = (za * centre + zs[:, None] * cs) / zq[:, None]
+        kq = torch.exp(-za * zs / zq * ((centre - cs) ** 2).sum(1))
+        zrs = zs[:, None] + zs[None, :]
+        prs = (zs[:, None, None] * cs[:, None, :] + zs[None, :, None] * cs[None, :, :]) / zrs[..., None]
+        krs = torch.exp(-zs[:, None] * zs[None, :] / zrs * ((cs[:, None, :] - cs[None, :, :]) ** 2).sum(-1))
+        zz = zq[:, None, None] + zrs[None]
+        rho = zq[:, None, None] * zrs[None] / zz
+        t = rho * ((pq[:, None, None, :] - prs[None]) ** 2).sum(-1)
+        f0 = torch.where(t > 1e-12, 0.5 * np.sqrt(np.pi) * torch.erf(torch.sqrt(t.clamp_min(1e-12))) /
+                         torch.sqrt(t.clamp_min(1e-12)), 1.0 - t / 3.0 + t * t / 10.0)
+        eri = 2.0 * np.pi ** 2.5 / (zq[:, None, None] * zrs[None] * torch.sqrt(zz)) * kq[:, None, None] * krs[None] * f0
+        return torch.cat([torch.einsum('qrs,rs->q', eri, ps), torch.einsum('qrs,rq->s', eri, ps)])
+
+    n_s = len(s_prim)
+    c_p = np.zeros((b.npgs, b.npgs))
+    x_p = np.zeros((b.npgs, b.npgs))
+    for p in d_prim:
+        za = float(b.zt[p])
+        centre = torch.tensor(b.pgs[p], **t64)
+        jac2 = torch.autograd.functional.jacobian(
+            lambda c: torch.autograd.functional.jacobian(lambda c2: sums(c2, za), c, create_graph=True), centre)
+        axes = [ax for ax in range(3) for _ in range(pw[p][ax])]
+        val = jac2[:, axes[0], axes[1]]
+        if axes[0] == axes[1]:
+            val = val + 2.0 * za * sums(centre, za)
+        val = (val / (4.0 * za * za)).detach().numpy()
+        c_p[p, s_prim], x_p[p, s_prim] = val[:n_s], val[n_s:]
+    rows = np.nonzero(np.any(cc[:, d_prim] != 0.0, axis=1))[0]
+    assert len(rows) and not np.any(cc[np.ix_(rows, s_prim)])
+    cols = np.nonzero(np.any(cc[:, s_prim] != 0.0, axis=1))[0]
+    want_c = (cc @ c_p @ cc.T)[np.ix_(rows, cols)]
+    want_x = (cc @ x_p @ cc.T)[np.ix_(rows, cols)]
+    assert np.abs(c_c[0][np.ix_(rows, cols)] - want_c).max() <= 1e-12 * np.abs(c_c[0]).max()
+    assert np.abs(x_c[0][np.ix_(rows, cols)] - want_x).max() <= 1e-12 * np.abs(x_c[0]).max()
+    assert np.abs(want_c).max() > 1e-3 * np.abs(c_c[0]).max()
