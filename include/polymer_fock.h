@@ -235,8 +235,12 @@ int32_t pfe_nuclear_attraction(const pfe_onee_args *a, double *n_p);
  * 2*npgs*npgs*cells1 results must fit there (a 976-primitive molecule does);
  * larger inputs return PFE_EINVAL with the size needed.  The first call on a
  * device does the set-up (module load and symbol lookup on that device) and
- * should come before any stream capture.  Calls share the one buffer per
- * device, so they are serialised by a lock; host buffers as pfe_overlap_kinetic. */
+ * should come before any stream capture; the address found then is kept for
+ * the life of the process, so a cudaDeviceReset between calls is not
+ * supported.  Calls share the one buffer per device, so they are serialised
+ * by a lock; host buffers as pfe_overlap_kinetic.  P_SHELL entries of every
+ * component a shell reaches must name primitives 1..npgs (else PFE_EINVAL,
+ * checked before any device work). */
 int32_t pfe_overlap_kinetic_noalloc(const pfe_onee_args *a, double *s_p, double *t_p);
 
 /* Library version string. */

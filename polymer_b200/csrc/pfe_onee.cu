@@ -267,13 +267,47 @@ static int upload(std::vector<void*>& owned, const T* h, size_t n, T** d) {
   return PFE_OK;
 }
 
-static int onee_run(const pfe_onee_args* a, double* s_p, double* t_p, double* n_p) {
-  if (!a || a->npgs <= 0 || a->npshell <= 0 || a->natom <= 0) { set_error("invalid one-electron arguments"); return PFE_EINVAL; }
-  for (int s = 0; s < a->npshell; ++s)
-    if (a->p_shell_ang[s] > LMAX_SUPPORTED) {
-      set_error("f shells are not implemented by the one-electron kernels");
-      return PFE_EUNSUPPORTED;
+// Host-side checks shared by the one-electron entry points, made before any
+// device work: the kernels index S_P/T_P/N_P by P_SHELL of every component a
+// shell reaches (i1+i2+i3 <= P_SHELL_ANG) and by the shell head P_SHELL(s,0,0,0),
+// so each of those entries must name a primitive 1..NPGS.  `need_atoms`: the
+// allocating entry point uploads the atom list and the Boys table as well.
+static int onee_validate(const pfe_onee_args* a, bool need_atoms) {
+  if (!a || a->npgs <= 0 || a->npshell <= 0 || (need_atoms && a->natom <= 0)) {
+    set_error("invalid one-electron arguments");
+    return PFE_EINVAL;
+  }
+  if (!a->p_shell || !a->p_shell_ang || !a->pgsx || !a->pgsy || !a->pgsz || !a->zt ||
+      (need_atoms && (!a->iatom || !a->atomx || !a->atomy || !a->atomz || !a->igamma))) {
+    set_error("a required one-electron array pointer is null");
+    return PFE_EINVAL;
+  }
+  for (int k = 0; k < 3; ++k)
+    if (a->cel1[k] < 0 || a->cel2[k] < 0) { set_error("negative cutoff"); return PFE_EINVAL; }
+  for (int s = 0; s < a->npshell; ++s) {
+    const int L = a->p_shell_ang[s];
+    if (L < 0 || L > LMAX_SUPPORTED) {
+      set_error("P_SHELL_ANG outside the one-electron kernels (s, p, d)");
+      return L < 0 ? PFE_EINVAL : PFE_EUNSUPPORTED;
     }
+    for (int i1 = 0; i1 <= L; ++i1)
+      for (int i2 = 0; i2 <= L - i1; ++i2)
+        for (int i3 = 0; i3 <= L - i1 - i2; ++i3) {
+          const int p = a->p_shell[(size_t)s + (size_t)a->npshell * (i1 + NPOW * (i2 + NPOW * i3))];
+          if (p < 1 || p > a->npgs) {
+            char msg[160];
+            std::snprintf(msg, sizeof msg, "P_SHELL(%d,%d,%d,%d) = %d is not a primitive 1..NPGS (%d)", s + 1, i1, i2,
+                          i3, p, a->npgs);
+            set_error(msg);
+            return PFE_EINVAL;
+          }
+        }
+  }
+  return PFE_OK;
+}
+
+static int onee_run(const pfe_onee_args* a, double* s_p, double* t_p, double* n_p) {
+  if (const int v = onee_validate(a, true)) return v;
   std::vector<void*> owned;
   OneeDev d{};
   int rc = PFE_OK;
@@ -377,9 +411,8 @@ static int noalloc_scratch(void** out) {
 }
 
 static int onee_noalloc(const pfe_onee_args* a, double* s_p, double* t_p) {
-  if (!a || !s_p || !t_p || a->npgs <= 0 || a->npshell <= 0) { set_error("invalid one-electron arguments"); return PFE_EINVAL; }
-  for (int k = 0; k < 3; ++k)
-    if (a->cel1[k] < 0 || a->cel2[k] < 0) { set_error("negative cutoff"); return PFE_EINVAL; }
+  if (!s_p || !t_p) { set_error("invalid one-electron arguments"); return PFE_EINVAL; }
+  if (const int v = onee_validate(a, false)) return v;
   const long long n1 = (long long)(2 * a->cel1[0] + 1) * (2 * a->cel1[1] + 1) * (2 * a->cel1[2] + 1);
   const size_t out_n = (size_t)a->npgs * a->npgs * n1;
   const size_t psz = (size_t)a->npshell * NPOW * NPOW * NPOW;
@@ -396,13 +429,6 @@ static int onee_noalloc(const pfe_onee_args* a, double* s_p, double* t_p) {
     set_error(msg);
     return PFE_EINVAL;
   }
-  for (int s = 0; s < a->npshell; ++s)
-    if (a->p_shell_ang[s] < 0 || a->p_shell_ang[s] > LMAX_SUPPORTED) {
-      set_error("P_SHELL_ANG outside the one-electron kernels (s, p, d)");
-      return a->p_shell_ang[s] < 0 ? PFE_EINVAL : PFE_EUNSUPPORTED;
-    }
-  for (size_t i = 0; i < psz; ++i)
-    if (a->p_shell[i] > a->npgs) { set_error("P_SHELL entry beyond NPGS"); return PFE_EINVAL; }
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   void* base = nullptr;
   int rc = noalloc_scratch(&base);

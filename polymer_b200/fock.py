@@ -23,9 +23,9 @@ from .capi import PfeCensus, PfeOneeArgs, check, lib
 from .system import System, from_fortran, to_fortran
 
 
-def onee(sysm: System):
-    """(S_P, T_P, N_P) cell-major from the device kernels (OVERLAP_KINETIC / NUCLEAR_ATTRACTION)."""
-    L = lib()
+def onee_args(sysm: System):
+    """The pfe_onee_args block of a system, and the arrays it points into (keep
+    them alive for as long as the block is used)."""
     b, d = sysm.basis, sysm.deck
     keep = dict(p_shell=np.asfortranarray(b.p_shell.astype(np.int32)),
                 ang=np.ascontiguousarray(b.p_shell_ang.astype(np.int32)),
@@ -48,6 +48,14 @@ def onee(sysm: System):
         a.cel1[k], a.cel2[k], a.period[k] = d.cel1[k], d.cel2[k], d.period[k]
     a.helix = d.helix
     a.igamma = capi.dptr(keep['ig'])
+    return a, keep
+
+
+def onee(sysm: System):
+    """(S_P, T_P, N_P) cell-major from the device kernels (OVERLAP_KINETIC / NUCLEAR_ATTRACTION)."""
+    L = lib()
+    b = sysm.basis
+    a, keep = onee_args(sysm)
     nc = sysm.ncell1
     n = b.npgs * b.npgs * nc
     s, t, v = np.zeros(n), np.zeros(n), np.zeros(n)

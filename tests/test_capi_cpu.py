@@ -7,8 +7,11 @@
   probe against the header);
 * the ctypes signature of every prototype in include/*.h matches it (count,
   pointers, scalar and return types);
-* the Fortran shim's BIND(C) type in the integration notes has pfe_args'
-  members in order, with the same kinds and array lengths.
+* the Fortran shim's BIND(C) type (fortran/pfourindexdirect_gpu.f90) has
+  pfe_args' members in order, with the same kinds and array lengths;
+* the one-electron entry points refuse a P_SHELL entry outside 1..NPGS for a
+  component a shell reaches with PFE_EINVAL, before any device work (so the
+  call returns the same on a machine without a GPU).
 """
 import ctypes
 import os
@@ -92,11 +95,11 @@ def test_ctypes_signatures_match_the_headers():
 
 
 def test_fortran_shim_type_matches_pfe_args():
-    # the BIND(C) type of the Fortran shim given in the integration notes (no
+    # the BIND(C) type of the Fortran shim fortran/pfourindexdirect_gpu.f90 (no
     # Fortran compiler here to check it): same members, order, kinds and array
     # lengths as pfe_args, whose ctypes mirror the layout test pins to the header
-    doc = open(os.path.join(os.path.dirname(__file__), '..', 'INTEGRATION.md')).read()
-    body = doc[doc.index('TYPE, BIND(C) :: PFE_ARGS'):doc.index('END TYPE')]
+    src = open(os.path.join(ROOT, 'fortran', 'pfourindexdirect_gpu.f90')).read()
+    body = src[src.index('TYPE, BIND(C) :: PFE_ARGS'):src.index('END TYPE')]
     kinds = {'INTEGER(C_INT32_T)': ctypes.c_int32, 'REAL(C_DOUBLE)': ctypes.c_double, 'TYPE(C_PTR)': None}
     fortran = []
     for line in body.splitlines()[1:]:
@@ -115,3 +118,30 @@ def test_fortran_shim_type_matches_pfe_args():
         else:
             c.append((name, t, 1))
     assert fortran == c
+
+
+@pytest.mark.parametrize('bad', [0, -1, 10 ** 6])
+@pytest.mark.parametrize('entry', ['pfe_overlap_kinetic', 'pfe_overlap_kinetic_noalloc', 'pfe_nuclear_attraction'])
+def test_onee_entry_points_refuse_a_malformed_p_shell(entry, bad):
+    import numpy as np
+
+    import oracle
+    from polymer_b200 import fock, geometry, system
+    sysm = system.build_system(geometry.water_deck(1, seed=2001), oracle.onee)
+    b = sysm.basis
+    # a component the p shell reaches (its x component) points nowhere
+    s = int(np.nonzero(b.p_shell_ang == 1)[0][0])
+    a, keep = fock.onee_args(sysm)
+    keep['p_shell'][s, 1, 0, 0] = bad
+    a.p_shell = capi.iptr(keep['p_shell'])
+    n = b.npgs ** 2 * sysm.ncell1
+    out1, out2 = np.zeros(n), np.zeros(n)
+    L = capi.lib()
+    fn = getattr(L, entry)
+    if entry == 'pfe_nuclear_attraction':
+        rc = fn(ctypes.byref(a), capi.dptr(out1))
+    else:
+        rc = fn(ctypes.byref(a), capi.dptr(out1), capi.dptr(out2))
+    assert rc == -1, (entry, bad, rc)   # PFE_EINVAL
+    assert 'P_SHELL' in capi.last_error(L)
+    assert not out1.any() and not out2.any()

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import oracle
-from polymer_b200 import capi, geometry, system
+from polymer_b200 import capi, fock, geometry, system
 
 pytestmark = pytest.mark.gpu
 
@@ -21,29 +21,7 @@ RTOL = 1e-14
 
 
 def _args(sysm):
-    b, d = sysm.basis, sysm.deck
-    keep = dict(p_shell=np.asfortranarray(b.p_shell.astype(np.int32)),
-                ang=np.ascontiguousarray(b.p_shell_ang.astype(np.int32)),
-                atom=np.ascontiguousarray(b.pgs_atom.astype(np.int32)),
-                x=np.ascontiguousarray(b.pgs[:, 0]), y=np.ascontiguousarray(b.pgs[:, 1]),
-                z=np.ascontiguousarray(b.pgs[:, 2]), zt=np.ascontiguousarray(b.zt),
-                iatom=np.array(d.atoms, dtype=np.int32),
-                ax=np.array([c[0] for c in d.coords]), ay=np.array([c[1] for c in d.coords]),
-                az=np.array([c[2] for c in d.coords]), ig=np.asfortranarray(sysm.igamma))
-    a = capi.PfeOneeArgs()
-    a.npgs, a.npshell, a.natom = b.npgs, b.npshell, d.natom
-    a.p_shell = capi.iptr(keep['p_shell'])
-    a.p_shell_ang = capi.iptr(keep['ang'])
-    a.pgs_atom = capi.iptr(keep['atom'])
-    a.pgsx, a.pgsy, a.pgsz = capi.dptr(keep['x']), capi.dptr(keep['y']), capi.dptr(keep['z'])
-    a.zt = capi.dptr(keep['zt'])
-    a.iatom = capi.iptr(keep['iatom'])
-    a.atomx, a.atomy, a.atomz = capi.dptr(keep['ax']), capi.dptr(keep['ay']), capi.dptr(keep['az'])
-    for k in range(3):
-        a.cel1[k], a.cel2[k], a.period[k] = d.cel1[k], d.cel2[k], d.period[k]
-    a.helix = d.helix
-    a.igamma = capi.dptr(keep['ig'])
-    return a, keep
+    return fock.onee_args(sysm)
 
 
 def _run(fn, a, n):
@@ -71,6 +49,25 @@ def test_noalloc_matches_allocating_entry_point(name):
         s, t = _run(L.pfe_overlap_kinetic_noalloc, a, n)
         assert np.abs(s - s_ref).max() <= RTOL * np.abs(s_ref).max()
         assert np.abs(t - t_ref).max() <= RTOL * np.abs(t_ref).max()
+
+
+def test_noalloc_matches_the_oracle_in_every_cell():
+    """The shared kernel itself against the oracle's OVERLAP_KINETIC on a helical
+    chain: S_P and T_P of every lattice cell (the helical image of the second
+    centre included), not only the home cell."""
+    from polymer_b200.system import from_fortran
+    sysm = system.build_system(CASES['helix_pe_631g'](), oracle.onee)
+    assert sysm.ncell1 > 1
+    a, keep = _args(sysm)
+    npgs, nc = sysm.basis.npgs, sysm.ncell1
+    s_o, t_o, _ = oracle.onee_overlap(sysm)
+    L = capi.lib()
+    for _ in range(2):
+        s, t = _run(L.pfe_overlap_kinetic_noalloc, a, npgs * npgs * nc)
+        s, t = from_fortran(s, (nc,), npgs), from_fortran(t, (nc,), npgs)
+        for c in range(nc):
+            assert np.abs(s[c] - s_o[c]).max() <= 1e-13 * np.abs(s_o).max() + 1e-15, c
+            assert np.abs(t[c] - t_o[c]).max() <= 1e-13 * np.abs(t_o).max() + 1e-15, c
 
 
 def test_noalloc_refuses_inputs_beyond_its_scratch():
