@@ -109,6 +109,16 @@ def water_cluster(k: int, seed: int) -> Tuple[List[int], np.ndarray]:
     return atoms, np.array(xyz)
 
 
+def water_single_point_deck(**opts) -> Deck:
+    """The water single point: O (0, 0, 0.1173) A, H (0, +-0.7572, -0.4692) A,
+    cc-pVDZ with spherical d, a molecule (no lattice), INTTOL 1e-12, SCFCONV 1e-8."""
+    xyz = np.array([[0.0, 0.0, 0.1173], [0.0, 0.7572, -0.4692], [0.0, -0.7572, -0.4692]])
+    opts.setdefault('inttol', 1.0e-12)
+    opts.setdefault('scfconv', 1.0e-8)
+    opts.setdefault('spherical', True)
+    return make_deck([8, 1, 1], xyz / ANG_BOHR, 'cc-pVDZ', **opts)
+
+
 def water_deck(k: int, seed: int, basis: str = 'cc-pVDZ', **opts) -> Deck:
     atoms, xyz = water_cluster(k, seed)
     opts.setdefault('inttol', 1.0e-10)

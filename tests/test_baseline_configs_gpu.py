@@ -1,0 +1,111 @@
+"""GPU against the oracle on the benchmark configurations at their full sizes.
+
+The other parity tests use small systems so the oracle finishes in seconds on
+one core.  These run the configurations the throughput and time-to-solution
+numbers are quoted on, with the oracle spread over the host's cores
+(tests/oracle_pool.py splits J/K into bra-shell or cell-pair-ticket pieces
+that sum exactly to the whole build):
+
+* the all-trans alkanes C10H22 and C20H42 in 6-31G** at INTTOL 1e-10 (C20H42
+  is the Fock-build benchmark), FP64, and the mixed FP32/FP64 path at the
+  Schwarz x density cutoff 1e-6 with its max|dJ|, |dK| against the oracle;
+* the water single point (O (0,0,0.1173) A, cc-pVDZ spherical, INTTOL 1e-12,
+  SCFCONV 1e-8): the SCF with the CUDA Fock build against the SCF with the
+  oracle's, energies within 1e-8 Eh;
+* a 16-water cluster in cc-pVDZ (1072 primitives: beyond the reference's
+  1024-primitive cap, so only the oracle can check it);
+* the helical polyethylene chain in 6-31G at CUTOFF1/CUTOFF2 = 5/10 (121
+  cell-pair tickets, Q3 over 21 cells), full build.
+
+FP64 tolerance as the other parity tests: |dC_C|, |dX_C| <= 1e-11 max|C_C| +
+1e-13 Hartree.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+import oracle_pool
+from polymer_b200 import fock, geometry, scf, system
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+RTOL = 1e-11
+# mixed FP32/FP64 recursion: quartets whose Schwarz bound times max|P| is below
+# 1e-6 run in FP32; their error is ~1e-7 of values below 1e-6 per quartet
+MIXED_TOL = 1e-8
+
+
+def _onee_s(sysm):
+    """S_P and T_P from the oracle; the Fock build reads no N_P (zeros)."""
+    s_p, t_p, _ = oracle.onee_overlap(sysm)
+    return s_p, t_p, np.zeros_like(t_p)
+
+
+def _close(got, ref, what, rtol=RTOL):
+    scale = np.abs(ref).max()
+    err = np.abs(got - ref).max()
+    assert err <= rtol * scale + 1e-13, '%s: max|diff| %.3e (scale %.3e)' % (what, err, scale)
+    return err
+
+
+def _mol_density(sysm, seed):
+    rng = np.random.default_rng(seed)
+    n = sysm.basis.ncgs
+    a = rng.normal(size=(n, n)) * 0.3
+    return np.einsum('ai,cab,bj->cij', sysm.basis.cc, (a + a.T)[None], sysm.basis.cc)
+
+
+@pytest.mark.parametrize('n', [10, 20])
+def test_alkane_at_full_size_matches_oracle(n):
+    s = system.build_system(geometry.alkane_deck(n, inttol=1e-10), _onee_s)
+    pp = _mol_density(s, seed=100 + n)
+    c_ref, x_ref = oracle_pool.fourindex_eri(s, pp)
+    c_gpu, x_gpu = fock.fourindex_eri(s, pp)
+    _close(c_gpu, c_ref, 'C_C')
+    _close(x_gpu, x_ref, 'X_C')
+    c_mx, x_mx = fock.fourindex_eri(s, pp, precision=1, mixed_cutoff=1e-6)
+    dj = _close(c_mx, c_ref, 'mixed C_C', MIXED_TOL)
+    dk = _close(x_mx, x_ref, 'mixed X_C', MIXED_TOL)
+    print('C%dH%d mixed FP32/FP64 at 1e-6: max|dJ| %.2e, max|dK| %.2e (max|J| %.2e)'
+          % (n, 2 * n + 2, dj, dk, np.abs(c_ref).max()))
+
+
+def test_water_single_point_scf_matches_oracle_scf():
+    d = geometry.water_single_point_deck()
+    s = system.build_system(d, oracle.onee)
+    ref = scf.run_scf(s, oracle.fock_builder(s), device='cpu')
+    gpu = scf.run_scf(s, fock.DeviceFock(s), device='cuda')
+    assert ref.converged and gpu.converged
+    assert abs(gpu.energy - ref.energy) <= 1e-8, (gpu.energy, ref.energy)
+    assert len(gpu.iterations) == len(ref.iterations)
+
+
+def test_water16_cluster_matches_oracle():
+    s = system.build_system(geometry.water_deck(16, seed=2001), _onee_s)
+    assert s.basis.npgs == 1072
+    pp = _mol_density(s, seed=16)
+    c_ref, x_ref = oracle_pool.fourindex_eri(s, pp)
+    c_gpu, x_gpu = fock.fourindex_eri(s, pp)
+    _close(c_gpu, c_ref, 'C_C')
+    _close(x_gpu, x_ref, 'X_C')
+
+
+def test_helical_chain_at_cutoff_5_10_matches_oracle():
+    s = system.build_system(geometry.polyethylene_deck('6-31G', cutoff1=5, cutoff2=10, kpoints=16), oracle.onee)
+    assert tuple(s.reduced_cel1) == (5, 0, 0)
+    rng = np.random.default_rng(3)
+    n = s.basis.ncgs
+    pc = rng.normal(size=(s.ncell1, n, n)) * 0.1
+    for c, q in enumerate(s.cells):          # P(-q) = P(q)^T, P(0) symmetric
+        cm = s.cell_index(-q[0], -q[1], -q[2])
+        if cm == c:
+            pc[c] = 0.5 * (pc[c] + pc[c].T)
+        elif cm < c:
+            pc[c] = pc[cm].T
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc)
+    ph = scf.rotate(scf.HostState(s), torch.tensor(pp)).numpy()
+    c_ref, x_ref = oracle_pool.fourindex_eri(s, pp, ph)
+    c_gpu, x_gpu = fock.fourindex_eri(s, pp, ph)
+    _close(c_gpu, c_ref, 'C_C')
+    _close(x_gpu, x_ref, 'X_C')
