@@ -451,7 +451,7 @@ def main():
     if dom:
         ach = dom['flops'] / (dom['ms'] * 1e-3) / 1e12
         traffic = ncu_traffic_per_launch()
-        kname = ['k_gq', 'k_gq_warp', 'k_gq_block'][dom['variant']]
+        kname = ['k_gq', 'k_gq_warp', 'k_gq_block', 'k_gq_wide'][dom['variant']]
         roof = {'bound': 'fp64', 'kernel': '%s<%s>' % (kname, dom['cls']), 'achieved': ach, 'peak': peak,
                 'unit': 'TFLOP/s', 'frac': ach / peak if peak else None,
                 'peak_source': 'measured in this run: DFMA loop over all SMs (pfe_measure_fp64_peak); '

@@ -183,9 +183,10 @@ int32_t pfe_batch_census(pfe_batch *b, pfe_census *out);
 int32_t pfe_context_profile(pfe_context *ctx, int32_t enable);
 typedef struct pfe_kernel_stat {
   int32_t cls;
-  int32_t variant;    /* 0 straight-line thread/quartet, 1 warp/quartet, 2 block/quartet */
+  int32_t variant;    /* 0 straight-line thread/quartet, 1 warp/quartet, 2 block/quartet,
+                         3 warp/quartet with per-lane Boys and geometry, kept outputs only */
   float ms;
-  float tuned_ms[3];  /* autotuner timing of each variant, 0 where not run */
+  float tuned_ms[4];  /* autotuner timing of each variant, 0 where not run */
   double quartets;
   double flops;
   int32_t grid_mult;  /* straight-line variant: blocks per SM of its persistent grid */
@@ -201,7 +202,7 @@ int32_t pfe_batch_schedule(pfe_batch *b, pfe_kernel_stat *out, int32_t cap);
  * host entry point pfe_fourindex_eri runs it on its first call after a set-up. */
 int32_t pfe_context_autotune(pfe_context *ctx, const double *d_p_p, const double *d_p_p_helix, void *stream);
 
-/* Force execution variant v (0/1/2 as in pfe_kernel_stat) on every quartet
+/* Force execution variant v (0..3 as in pfe_kernel_stat) on every quartet
  * class that has it; the others keep theirs (diagnostics and tests). */
 int32_t pfe_context_force_variant(pfe_context *ctx, int32_t variant);
 

@@ -2,8 +2,9 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this package.  It wraps oracle/oracle.c, a plain-C restatement of the
-reference's FOURINDEX_ERI, OVERLAP_KINETIC, NUCLEAR_ATTRACTION and
-FMT_PRELIMINARY (see that file's header for the file:line map), through the
+reference's FOURINDEX_ERI, OVERLAP_KINETIC, NUCLEAR_ATTRACTION,
+FMT_PRELIMINARY, the primitive half of FORM_C2H and the P_P_HELIX part of
+ROTATE_DENSITYMATRIX (see that file's header for the file:line map), through the
 same pfe_args C-ABI block the product takes.
 
 Pinned against the reference's recorded outputs in tests/test_oracle_golden.py
@@ -60,6 +61,10 @@ def lib():
         L.oracle_overlap_kinetic.restype = ctypes.c_int32
         L.oracle_nuclear_attraction.argtypes = [ctypes.POINTER(OneeArgs), _dp]
         L.oracle_nuclear_attraction.restype = ctypes.c_int32
+        L.oracle_form_p2h.argtypes = [ctypes.c_int32, _ip, _ip, _ip, _ip, ctypes.c_double, ctypes.c_int32, _dp]
+        L.oracle_form_p2h.restype = None
+        L.oracle_rotate_density.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _dp, _dp, _dp]
+        L.oracle_rotate_density.restype = None
         _L = L
     return _L
 
@@ -156,3 +161,39 @@ def fock_builder(sysm):
         return (torch.tensor(c, dtype=torch.float64, device=p_p.device),
                 torch.tensor(x, dtype=torch.float64, device=p_p.device))
     return f
+
+
+def form_p2h(sysm) -> np.ndarray:
+    """P2H cell-major [q + NH] (NH = CEL2X + CEL1X), each (npgs, npgs), from the
+    oracle's FORM_C2H restatement."""
+    from polymer_b200.basis import p2c_map
+    b, d = sysm.basis, sysm.deck
+    nh = d.cel2[0] + d.cel1[0]
+    pax, pay, paz = (np.ascontiguousarray(x.astype(np.int32)) for x in (b.pax, b.pay, b.paz))
+    p2c = np.ascontiguousarray(p2c_map(b, ghost_value=-1).astype(np.int32))
+    out = np.zeros(b.npgs * b.npgs * (2 * nh + 1))
+    lib().oracle_form_p2h(b.npgs, pax.ctypes.data_as(_ip), pay.ctypes.data_as(_ip), paz.ctypes.data_as(_ip),
+                          p2c.ctypes.data_as(_ip), float(d.helix), nh, out.ctypes.data_as(_dp))
+    from polymer_b200.system import from_fortran
+    return from_fortran(out, (2 * nh + 1,), b.npgs).copy()
+
+
+def rotate_density(sysm, p_p: np.ndarray, p2h: np.ndarray = None) -> np.ndarray:
+    """P_P_HELIX [q1 + NH, q2 + CEL2X] (the layout of scf.rotate) from the
+    oracle's ROTATE_DENSITYMATRIX restatement; p_p is cell-major over the x
+    cells -CEL1X..CEL1X of a chain, p2h as form_p2h returns it (default: that)."""
+    d = sysm.deck
+    n = sysm.basis.npgs
+    c1, c2 = d.cel1[0], d.cel2[0]
+    nh = c1 + c2
+    if p2h is None:
+        p2h = form_p2h(sysm)
+    cells = [sysm.cell_index(q, 0, 0) for q in range(-c1, c1 + 1)]
+    pp_f = np.ascontiguousarray(np.swapaxes(np.asarray(p_p)[cells], -1, -2)).reshape(-1)
+    p2h_f = np.ascontiguousarray(np.swapaxes(p2h, -1, -2)).reshape(-1)
+    out = np.zeros(n * n * (2 * c2 + 1) * (2 * nh + 1))
+    lib().oracle_rotate_density(n, c1, c2, p2h_f.ctypes.data_as(_dp), pp_f.ctypes.data_as(_dp),
+                                out.ctypes.data_as(_dp))
+    # column-major (n, n, q2, q1) -> [q1][q2][i][j]
+    o = out.reshape(2 * nh + 1, 2 * c2 + 1, n, n)
+    return np.swapaxes(o, -1, -2).copy()

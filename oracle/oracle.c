@@ -9,6 +9,8 @@
  *   oracle_overlap_kinetic      OVERLAP_KINETIC(0)     src/ponee.f90:1-160 (S_P, T_P per cell)
  *   oracle_nuclear_attraction   NUCLEAR_ATTRACTION(0)  src/ponee.f90:418-603 (N_P per cell)
  *   oracle_fourindex_eri        FOURINDEX_ERI          src/pfourindexdirect.f90:1-814
+ *   oracle_form_p2h             FORM_C2H (P2H part)    src/pbasis.f90:134-413 (p and d)
+ *   oracle_rotate_density       ROTATE_DENSITYMATRIX   src/pdensitymatrix.f90:516-563 (P_P_HELIX)
  *
  * oracle_fourindex_eri follows the reference's loop order and formulas: the
  * Obara-Saika index tables (:101-221), the (Q1,Q2) cell-pair ticket split
@@ -763,4 +765,92 @@ int32_t oracle_nuclear_attraction(const oracle_onee_args *a, double *n_p) {
   }
 #undef N1I
   return PFE_OK;
+}
+
+/* ------------------------------------------------------- helical density rotation
+ *
+ * oracle_form_p2h: the primitive half of FORM_C2H (src/pbasis.f90:134-413):
+ * P2H(:,:,J) for J = -NH..NH is the identity, except that every p triple
+ * (x,y,z starting at a primitive with PAX=1,PAY=0,PAZ=0 that has a contracted
+ * function, src/pbasis.f90:196-218) and every d sextet (PAX=2, :220-253) is
+ * rotated by HELIX*J about the x axis.  p2c[i] is the contracted row of
+ * primitive i (0-based) or -1 (P2C of :165-180).  Output column-major
+ * P2H(npgs,npgs,2*NH+1).  f functions are not restated (the kernels take s, p, d).
+ */
+void oracle_form_p2h(int32_t npgs, const int32_t *pax, const int32_t *pay, const int32_t *paz, const int32_t *p2c,
+                     double helix, int32_t nh, double *p2h) {
+  const size_t nn = (size_t)npgs * npgs;
+  memset(p2h, 0, sizeof(double) * nn * (size_t)(2 * nh + 1));
+  for (int32_t j = -nh; j <= nh; ++j) {
+    double *P = p2h + nn * (size_t)(j + nh);
+#define P2H(a, b) P[(size_t)(a) + (size_t)npgs * (size_t)(b)]
+    for (int32_t i = 0; i < npgs; ++i) P2H(i, i) = 1.0;
+    if (helix == 0.0) continue;
+    const double ang = helix * (double)j, c = cos(ang), s = sin(ang);
+    for (int32_t i = 0; i < npgs; ++i) {   /* P ORBITALS */
+      if (!(pax[i] == 1 && pay[i] == 0 && paz[i] == 0) || p2c[i] == -1) continue;
+      P2H(i, i) = 1.0;
+      P2H(i + 1, i + 1) = c;
+      P2H(i + 2, i + 2) = c;
+      P2H(i + 1, i + 2) = s;
+      P2H(i + 2, i + 1) = -s;
+    }
+    for (int32_t i = 0; i < npgs; ++i) {   /* D ORBITALS */
+      if (!(pax[i] == 2 && pay[i] == 0 && paz[i] == 0) || p2c[i] == -1) continue;
+      P2H(i, i) = 1.0;
+      P2H(i + 1, i + 1) = c * c;
+      P2H(i + 1, i + 2) = s * s;
+      P2H(i + 1, i + 4) = 2.0 * c * s;
+      P2H(i + 2, i + 1) = s * s;
+      P2H(i + 2, i + 2) = c * c;
+      P2H(i + 2, i + 4) = -2.0 * c * s;
+      P2H(i + 3, i + 3) = c;
+      P2H(i + 3, i + 5) = s;
+      P2H(i + 4, i + 1) = -c * s;
+      P2H(i + 4, i + 2) = c * s;
+      P2H(i + 4, i + 4) = c * c - s * s;
+      P2H(i + 5, i + 3) = -s;
+      P2H(i + 5, i + 5) = c;
+    }
+#undef P2H
+  }
+}
+
+/*
+ * oracle_rotate_density: the P_P_HELIX part of ROTATE_DENSITYMATRIX
+ * (src/pdensitymatrix.f90:516-563), in the reference's loop order:
+ *   TMP1(I,J) = sum_II P2H(II,I,Q2X) P_P(II,J,Q1X-Q2X)
+ *   P_P_HELIX(I,J,Q2X,Q1X) = sum_JJ P2H(JJ,J,Q1X) TMP1(I,JJ)
+ * for Q2X in [-CEL2X,CEL2X], Q1X in [-CEL2X-CEL1X, CEL2X+CEL1X] with
+ * |Q1X-Q2X| <= CEL1X; every other block is zero.  Layouts (column-major):
+ * P_P(npgs,npgs,-cel1x:cel1x) (the x cells of a 1-D chain), P2H(npgs,npgs,
+ * -(cel2x+cel1x):+), P_P_HELIX(npgs,npgs,-cel2x:cel2x,-(cel2x+cel1x):+).
+ */
+void oracle_rotate_density(int32_t npgs, int32_t cel1x, int32_t cel2x, const double *p2h, const double *p_p,
+                           double *p_p_helix) {
+  const size_t nn = (size_t)npgs * npgs;
+  const int32_t h3 = cel1x + cel2x, n2 = 2 * cel2x + 1;
+  double *tmp1 = malloc(sizeof(double) * nn);
+  memset(p_p_helix, 0, sizeof(double) * nn * (size_t)n2 * (size_t)(2 * h3 + 1));
+  for (int32_t q2 = -cel2x; q2 <= cel2x; ++q2)
+    for (int32_t q1 = -h3; q1 <= h3; ++q1) {
+      if (q1 - q2 < -cel1x || q1 - q2 > cel1x) continue;
+      const double *A = p2h + nn * (size_t)(q2 + h3);
+      const double *B = p2h + nn * (size_t)(q1 + h3);
+      const double *Pq = p_p + nn * (size_t)(q1 - q2 + cel1x);
+      double *O = p_p_helix + nn * ((size_t)(q2 + cel2x) + (size_t)n2 * (size_t)(q1 + h3));
+      for (int32_t i = 0; i < npgs; ++i)
+        for (int32_t j = 0; j < npgs; ++j) {
+          double t = 0.0;
+          for (int32_t ii = 0; ii < npgs; ++ii) t += A[ii + (size_t)npgs * i] * Pq[ii + (size_t)npgs * j];
+          tmp1[i + (size_t)npgs * j] = t;
+        }
+      for (int32_t i = 0; i < npgs; ++i)
+        for (int32_t j = 0; j < npgs; ++j) {
+          double t = 0.0;
+          for (int32_t jj = 0; jj < npgs; ++jj) t += B[jj + (size_t)npgs * j] * tmp1[i + (size_t)npgs * jj];
+          O[i + (size_t)npgs * j] = t;
+        }
+    }
+  free(tmp1);
 }

@@ -61,7 +61,7 @@ class PfeCensus(ctypes.Structure):
 
 class PfeKernelStat(ctypes.Structure):
     _fields_ = [('cls', ctypes.c_int32), ('variant', ctypes.c_int32), ('ms', ctypes.c_float),
-                ('tuned_ms', ctypes.c_float * 3), ('quartets', ctypes.c_double), ('flops', ctypes.c_double),
+                ('tuned_ms', ctypes.c_float * 4), ('quartets', ctypes.c_double), ('flops', ctypes.c_double),
                 ('grid_mult', ctypes.c_int32), ('pad_', ctypes.c_int32)]
 
 

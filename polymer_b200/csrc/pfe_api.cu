@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -345,6 +346,19 @@ static int setup_impl(pfe_context* ctx, const pfe_args* a, const HostShells& hs,
           scoef[(size_t)sh * MAXCOMP + c] = tcoef[p];
           stidx[(size_t)sh * MAXCOMP + c] = tidx[p];
         }
+      for (int L = 0; L < 3; ++L) { ctx->kept_max[L] = 0; ctx->lower_kept[L] = false; }
+      for (int sh = 0; sh < a->npshell; ++sh) {
+        const int L = hs.L[sh];
+        int kept = 0, c = 0;
+        for (int i1 = 0; i1 <= L; ++i1)   // the components in P_SHELL order, with their total power
+          for (int i2 = 0; i2 <= L - i1; ++i2)
+            for (int i3 = 0; i3 <= L - i1 - i2; ++i3, ++c)
+              if (stidx[(size_t)sh * MAXCOMP + c] >= 0) {
+                ++kept;
+                if (i1 + i2 + i3 < L) ctx->lower_kept[L] = true;
+              }
+        ctx->kept_max[L] = std::max(ctx->kept_max[L], kept);
+      }
       PFE_CUDA(ctx->alloc((void**)&ctx->d_scoef, sizeof(double) * scoef.size()));
       PFE_CUDA(ctx->alloc((void**)&ctx->d_stidx, sizeof(int) * stidx.size()));
       PFE_CUDA(cudaMemcpy(ctx->d_scoef, scoef.data(), sizeof(double) * scoef.size(), cudaMemcpyHostToDevice));
@@ -616,7 +630,7 @@ int32_t pfe_batch_schedule(pfe_batch* b, pfe_kernel_stat* out, int32_t cap) {
     const ClassLaunch& cl = b->launches[i];
     out[n].cls = class_code(cl.cb, cl.ck);
     out[n].variant = cl.variant;
-    for (int v = 0; v < 3; ++v) out[n].tuned_ms[v] = cl.tuned_ms[v];
+    for (int v = 0; v < 4; ++v) out[n].tuned_ms[v] = cl.tuned_ms[v];
     out[n].ms = 0.f;
     out[n].quartets = cl.quartets;
     out[n].flops = cl.quartets * class_flops(cl.cb, cl.ck);
@@ -712,7 +726,7 @@ int32_t pfe_context_kernel_stats(pfe_context* ctx, pfe_kernel_stat* out, int32_t
     PFE_CUDA(cudaEventElapsedTime(&ms, ctx->ev[i], ctx->ev[i + 1]));
     out[n].cls = ctx->ev_cls[i];
     out[n].variant = ctx->ev_variant[i];
-    for (int v = 0; v < 3; ++v) out[n].tuned_ms[v] = ctx->ev_tuned[i][v];
+    for (int v = 0; v < 4; ++v) out[n].tuned_ms[v] = ctx->ev_tuned[i][v];
     out[n].ms = ms;
     out[n].quartets = ctx->ev_quartets[i];
     out[n].flops = ctx->ev_flops[i];
@@ -733,12 +747,13 @@ int32_t pfe_context_autotune(pfe_context* ctx, const double* d_p_p, const double
 
 int32_t pfe_context_force_variant(pfe_context* ctx, int32_t variant) {
   if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
-  if (variant < 0 || variant > 2) { set_error("variant must be 0, 1 or 2"); return PFE_EINVAL; }
+  if (variant < 0 || variant > 3) { set_error("variant must be 0, 1, 2 or 3"); return PFE_EINVAL; }
   for (int i = 0; i < ctx->nlaunch; ++i) {
     ClassLaunch& cl = ctx->launches[i];
     if (variant == 0 && cl.has_straight) cl.variant = 0;
     if (variant == 1 && cl.has_table && sizeof(double) * (size_t)cl.per_warp <= 200 * 1024) cl.variant = 1;
     if (variant == 2 && cl.has_table) cl.variant = 2;
+    if (variant == 3 && cl.has_wide) cl.variant = 3;
   }
   ctx->tuned = true;
   return PFE_OK;

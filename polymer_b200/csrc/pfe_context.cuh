@@ -43,7 +43,9 @@ struct ClassLaunch {
   int4* chunks;  // (bra pair, first ket, end ket, 0)
   double quartets;
   // execution variant: 0 = straight-line thread per quartet, 1 = warp per
-  // quartet on the op table, 2 = block per quartet on the op table
+  // quartet on the op table, 2 = block per quartet on the op table, 3 = warp
+  // per quartet on the op table with per-lane Boys/geometry and only the
+  // outputs that carry a coefficient (pfe_mol_wide.cu)
   int variant;
   bool has_straight, has_table;
   const unsigned short* ops;
@@ -60,8 +62,14 @@ struct ClassLaunch {
   int nlevels_p2;
   int wpb, per_warp;         // warps per block and doubles per warp (variant 1)
   size_t smem_big, smem_warp;
-  float tuned_ms[3];         // autotuner timings per variant (0 = not run)
+  float tuned_ms[4];         // autotuner timings per variant (0 = not run)
   double* xg;                // block variant: per-block X scratch in global memory, or null
+  int nslots_p, nslots_p2;   // slots of the pure-bra and bra-and-ket tables (0: none)
+  // variant 3 (warp per primitive quartet, kept outputs only): per-warp shared
+  // memory in doubles, of which wide_vmax op-table slots and wide_xmax outputs
+  bool has_wide;
+  int wide_wpb, wide_per_warp, wide_vmax, wide_xmax;
+  size_t smem_wide;
   int npass;                 // launches of the straight-line variant
   int gmul = 32;             // straight-line variant: persistent grid of up to gmul blocks per SM
 };
@@ -104,6 +112,11 @@ struct pfe_context {
   double* d_scoef = nullptr; // shell x component -> coefficient of its primitive (tcoef)
   int* d_stidx = nullptr;    // shell x component -> target row of its primitive (tidx)
   int* d_blk = nullptr;      // shell -> contracted block id
+  // per angular momentum L of a shell: the most components with a target row
+  // one shell of that L has, and whether some shell of that L has a target on
+  // a component below L (a cumulative sp/spd shell, not a pure p/d one)
+  int kept_max[3] = {1, 4, 10};
+  bool lower_kept[3] = {false, true, true};
   int nblk = 0;
   bool force_primitive = false;  // set before set-up: primitive targets even when CC allows contracted ones
   int* d_rep = nullptr;      // target -> representative primitive (largest |coefficient|)
@@ -150,7 +163,7 @@ struct pfe_context {
   int nev = 0;
   int ev_cls[64] = {0};
   int ev_variant[64] = {0};
-  float ev_tuned[64][3] = {};
+  float ev_tuned[64][4] = {};
   double ev_quartets[64] = {0}, ev_flops[64] = {0};
   int ev_gmul[64] = {0};
   int nprof = 0;

@@ -44,6 +44,7 @@
 #include "pfe_interp.cuh"
 #include "generated/eri_classes.cuh"
 #include "pfe_mol_kernels.cuh"
+#include "pfe_mol_wide.cuh"
 
 namespace pfe {
 
@@ -156,7 +157,8 @@ __global__ void k_pack_pairs(PairArrays pr, PairRec* __restrict__ rec, long long
   r.schwarz = pr.schwarz[t];
   r.si = pr.si[t];
   r.sj = pr.sj[t];
-  r.pad[0] = r.pad[1] = r.pad[2] = 0.0;
+  r.oz = 0.5 / r.zeta;
+  r.pad[0] = r.pad[1] = 0.0;
   rec[t] = r;
 }
 
@@ -673,6 +675,40 @@ static int exclusive_sum(pfe_context* ctx, const int* in, int* out, int n, cudaS
   return PFE_OK;
 }
 
+// Shared memory of the wide variant (pfe_mol_wide.cu) for this molecule's
+// shells: the slots of the largest op table one of its group quartets can take
+// (the pure-bra or bra-and-ket table when no shell of the bra or ket kind has a
+// target on a lower component) and the kept outputs of its largest group
+// quartet; warps per block chosen for the most resident warps per SM.
+static int size_wide(ClassLaunch& cl, const int kept_max[3], const bool lower_kept[3]) {
+  cl.has_wide = false;
+  const WideVariant wv = wide_variant(cl.cb, cl.ck);
+  if (!wv.launch || !cl.has_table) return PFE_OK;
+  const int la = kCL[cl.cb][0], lb = kCL[cl.cb][1], lc = kCL[cl.ck][0], ld = kCL[cl.ck][1];
+  const bool bra_full = !cl.ops_p || lower_kept[la] || lower_kept[lb];
+  const bool ket_full = lower_kept[lc] || lower_kept[ld] || !cl.ops_p2;
+  const int vmax = bra_full ? cl.nslots : (ket_full ? cl.nslots_p : cl.nslots_p2);
+  auto km = [&](int L) { return std::max(kept_max[L], 1); };
+  const int xmax = km(la) * km(lb) * km(lc) * km(ld);
+  const size_t pw = sizeof(double) * (size_t)wv.doubles(vmax, xmax);
+  const size_t cap = 227 * 1024;
+  int best = 0, best_w = 0;
+  for (int w = 1; w <= 8; ++w) {
+    if (w * pw > cap) break;
+    const int resident = w * (int)((228 * 1024) / (w * pw + 1024));
+    if (resident > best_w) { best_w = resident; best = w; }
+  }
+  if (best == 0) return PFE_OK;   // does not fit: the class keeps its other variants
+  cl.wide_vmax = vmax;
+  cl.wide_xmax = xmax;
+  cl.wide_per_warp = (int)(pw / sizeof(double));
+  cl.wide_wpb = best;
+  cl.smem_wide = pw * best;
+  PFE_CUDA(wv.allow(cl.smem_wide));
+  cl.has_wide = true;
+  return PFE_OK;
+}
+
 int molecular_setup(pfe_context* ctx, const pfe_args* a) {
   (void)a;
   cudaStream_t s = ctx->stream;
@@ -862,11 +898,13 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
         cl.ops = d.ops; cl.levels = d.levels; cl.out = d.out;
         cl.nlevels = d.nlevels; cl.nout = d.nout; cl.nslots = d.nslots;
         cl.ops_p = nullptr; cl.levels_p = nullptr; cl.out_p = nullptr; cl.nlevels_p = 0;
+        cl.nslots_p = cl.nslots_p2 = 0;
         if (const OpTableHost* hp = host_optable_pure(cb, ck)) {
           OpTableDev dp{};
           if ((rc = upload_optable(ctx, hp, &dp)) != PFE_OK) return rc;
           if (dp.nslots <= d.nslots) {   // runs inside the full table's shared-memory layout
             cl.ops_p = dp.ops; cl.levels_p = dp.levels; cl.out_p = dp.out; cl.nlevels_p = dp.nlevels;
+            cl.nslots_p = dp.nslots;
           }
         }
         cl.ops_p2 = nullptr; cl.levels_p2 = nullptr; cl.out_p2 = nullptr; cl.nlevels_p2 = 0;
@@ -875,6 +913,7 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
           if ((rc = upload_optable(ctx, hp, &dp)) != PFE_OK) return rc;
           if (dp.nslots <= d.nslots && cl.ops_p) {   // taken only where the pure-bra table is
             cl.ops_p2 = dp.ops; cl.levels_p2 = dp.levels; cl.out_p2 = dp.out; cl.nlevels_p2 = dp.nlevels;
+            cl.nslots_p2 = dp.nslots;
           }
         }
         cl.per_warp = vv.doubles(h->nslots, true);
@@ -899,15 +938,17 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
           PFE_CUDA(ctx->alloc((void**)&cl.xg, sizeof(double) * (size_t)h->nout * 2 * ctx->num_sms));
         }
         PFE_CUDA(vv.allow(cl.smem_big, std::min<size_t>(cl.smem_warp, 220 * 1024)));
-        // default schedule (measured on B200): straight-line code where a class has it, one
-        // primitive quartet per warp up to 640 integrals, per block beyond
-        cl.variant = cl.has_straight ? 0 : ((h->nout <= 640 && cl.smem_warp <= 200 * 1024) ? 1 : 2);
+        if ((rc = size_wide(cl, ctx->kept_max, ctx->lower_kept)) != PFE_OK) return rc;
+        // default schedule (measured on B200): straight-line code where a class has it, else
+        // the wide warp variant where the working set fits, else one primitive quartet per
+        // warp up to 640 integrals, per block beyond
+        cl.variant = cl.has_straight ? 0 : (cl.has_wide ? 3 : ((h->nout <= 640 && cl.smem_warp <= 200 * 1024) ? 1 : 2));
       }
       if (!cl.has_straight && !cl.has_table) {
         set_error("no kernel for a quartet class");
         return PFE_EUNSUPPORTED;
       }
-      for (int v = 0; v < 3; ++v) cl.tuned_ms[v] = 0.f;
+      for (int v = 0; v < 4; ++v) cl.tuned_ms[v] = 0.f;
       ctx->launches[ctx->nlaunch++] = cl;
       ctx->census_quartets += (double)nq;
       ctx->census_flops += (double)nq * class_flops(cb, ck);
@@ -964,6 +1005,13 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
   }
   OpTableDev t{cl.ops,   cl.levels,   cl.out,     cl.nlevels,   cl.nout,   cl.nslots,     cl.ops_p,
                cl.levels_p, cl.out_p, cl.nlevels_p, cl.ops_p2, cl.levels_p2, cl.out_p2, cl.nlevels_p2};
+  if (variant == 3 && cl.has_wide) {
+    const int per_sm = std::max(1, (int)((228 * 1024) / (cl.smem_wide + 1024)));   // resident blocks per SM
+    const int grid = std::min((work + cl.wide_wpb - 1) / cl.wide_wpb, ctx->num_sms * per_sm);
+    wide_variant(cl.cb, cl.ck).launch(ql, t, std::max(grid, 1), cl.wide_wpb, cl.wide_per_warp, cl.wide_vmax,
+                                      cl.wide_xmax, cl.smem_wide, s);
+    return;
+  }
   if (variant == 1) {
     const int grid = std::min((work + cl.wpb - 1) / cl.wpb, ctx->num_sms * 8);
     variants(cl.cb, cl.ck).warp(ql, t, std::max(grid, 1), cl.wpb, cl.per_warp, cl.smem_warp, s);
@@ -991,6 +1039,7 @@ static const double* target_density(pfe_context* ctx, const double* d_pp, cudaSt
 static bool variant_ok(const ClassLaunch& cl, int v) {
   if (v == 0) return cl.has_straight;
   if (v == 1) return cl.has_table && cl.smem_warp <= 200 * 1024;
+  if (v == 3) return cl.has_wide;
   return cl.has_table;
 }
 
@@ -1001,7 +1050,7 @@ static int tune_class(pfe_context* ctx, ClassLaunch& cl, const MolLaunch& ql, cu
                       cudaEvent_t e0, cudaEvent_t e1) {
   float best = 1e30f;
   int bestv = cl.variant, bestg = cl.gmul;
-  for (int v = 0; v < 3; ++v) {
+  for (int v = 0; v < 4; ++v) {
     if (!variant_ok(cl, v)) continue;
     static const int kGmul[4] = {4, 8, 16, 32};
     const int ng = v == 0 ? 4 : 1;
@@ -1087,7 +1136,7 @@ static int run_build(pfe_context* ctx, const double* d_dt, double* d_cc, double*
       ctx->ev_flops[i] = cl.quartets * class_flops(cl.cb, cl.ck);
       ctx->ev_gmul[i] = cl.gmul;
       ctx->ev_variant[i] = cl.variant;
-      for (int v = 0; v < 3; ++v) ctx->ev_tuned[i][v] = cl.tuned_ms[v];
+      for (int v = 0; v < 4; ++v) ctx->ev_tuned[i][v] = cl.tuned_ms[v];
     }
   }
   if (ctx->contracted) {
@@ -1170,6 +1219,15 @@ int batch_setup(pfe_batch* b) {
       if (!tmpl || total == 0) continue;
       if (total >= (1LL << 31)) { set_error("batch: too many chunks in one quartet class"); return PFE_EINVAL; }
       ClassLaunch cl = *tmpl;
+      if (cl.has_wide) {   // the wide variant's working set must cover every instance
+        int km[3] = {1, 1, 1};
+        bool lk[3] = {false, false, false};
+        for (pfe_context* c : b->inst)
+          for (int L = 0; L < 3; ++L) { km[L] = std::max(km[L], c->kept_max[L]); lk[L] = lk[L] || c->lower_kept[L]; }
+        const int rc = size_wide(cl, km, lk);
+        if (rc != PFE_OK) return rc;
+        if (!cl.has_wide && cl.variant == 3) cl.variant = cl.has_straight ? 0 : 2;
+      }
       cl.nchunks_host = (int)total;
       cl.quartets = 0.0;
       PFE_CUDA(b->alloc((void**)&cl.chunks, sizeof(int4) * total));

@@ -11,17 +11,19 @@
 namespace pfe {
 
 // One shell pair as the quartet kernels read it, 128 bytes (seven 16-byte
-// loads): P[3], PA[3], AB[3], zeta, S, Schwarz bound, (si, sj), padding.
+// loads): P[3], PA[3], AB[3], zeta, S, Schwarz bound, (si, sj), 1/(2 zeta),
+// padding.
 struct __align__(16) PairRec {
   double P[3], PA[3], AB[3];
   double zeta, S, schwarz;
   int si, sj;
-  double pad[3];
+  double oz;
+  double pad[2];
 };
 static_assert(sizeof(PairRec) == 128, "PairRec layout");
 
 struct PairView {
-  double P[3], PA[3], AB[3], zeta, S;
+  double P[3], PA[3], AB[3], zeta, S, oz;
   int si, sj;
 };
 
@@ -36,6 +38,7 @@ __device__ __forceinline__ PairView load_pair(const PairRec* __restrict__ rec, i
   v.AB[0] = d.x; v.AB[1] = d.y; v.AB[2] = e.x;
   v.zeta = e.y; v.S = f.x;
   v.si = __double2loint(g.x); v.sj = __double2hiint(g.x);
+  v.oz = g.y;
   return v;
 }
 
@@ -299,7 +302,9 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
         const double zb = bp.zeta;
         const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];
         const double zz = zb + ze;
-        const double rho = zb * ze / zz;
+        // one reciprocal per primitive quartet; 1/(2 zeta) of either pair comes with its record
+        const double rzz = 1.0 / zz;
+        const double rho = zb * ze * rzz;
         const double dx = Px - Qx, dy = Py - Qy, dz = Pz - Qz;
         const double T = rho * (dx * dx + dy * dy + dz * dz);
         const double pref = c2pi * bp.S * Sq * sqrt(rho);
@@ -314,14 +319,14 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
           out[0] = F[0];
         } else {
           EriGeom<double> g;
-          const double Wx = (zb * Px + ze * Qx) / zz, Wy = (zb * Py + ze * Qy) / zz, Wz = (zb * Pz + ze * Qz) / zz;
+          const double Wx = (zb * Px + ze * Qx) * rzz, Wy = (zb * Py + ze * Qy) * rzz, Wz = (zb * Pz + ze * Qz) * rzz;
           g.PA[0] = bp.PA[0]; g.PA[1] = bp.PA[1]; g.PA[2] = bp.PA[2];
           g.QC[0] = kq.PA[0]; g.QC[1] = kq.PA[1]; g.QC[2] = kq.PA[2];
           g.AB[0] = bp.AB[0]; g.AB[1] = bp.AB[1]; g.AB[2] = bp.AB[2];
           g.CD[0] = kq.AB[0]; g.CD[1] = kq.AB[1]; g.CD[2] = kq.AB[2];
           g.WP[0] = Wx - Px; g.WP[1] = Wy - Py; g.WP[2] = Wz - Pz;
           g.WQ[0] = Wx - Qx; g.WQ[1] = Wy - Qy; g.WQ[2] = Wz - Qz;
-          g.oz = 0.5 / zb; g.oe = 0.5 / ze; g.oze = 0.5 / zz; g.roz = rho / zb; g.roe = rho / ze;
+          g.oz = bp.oz; g.oe = kq.oz; g.oze = 0.5 * rzz; g.roz = ze * rzz; g.roe = zb * rzz;
           if constexpr (MIXED) {
             if (f32) eri_prec<float, LA, LB, LC, LD>(F, pref, g, out);
             else eri_prec<double, LA, LB, LC, LD>(F, pref, g, out);

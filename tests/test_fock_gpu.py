@@ -70,7 +70,7 @@ def test_alkane_screened_matches_oracle(n, inttol):
     _assert_close(x_gpu, x_ref, 'X_C')
 
 
-@pytest.mark.parametrize('variant', [0, 1, 2])
+@pytest.mark.parametrize('variant', [0, 1, 2, 3])
 @pytest.mark.parametrize('mol', ['alkane', 'water'])
 def test_every_execution_variant_matches_oracle(variant, mol, reference_runs):
     """Straight-line, warp-per-quartet and block-per-quartet schedules all agree:

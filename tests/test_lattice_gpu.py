@@ -89,3 +89,15 @@ def test_molecular_rank_shares_sum_to_the_full_build():
     parts = [fock.fourindex_eri(s, pp, myid=r, numprocs=2) for r in range(2)]
     _close(parts[0][0] + parts[1][0], c_full, 'sum C_C')
     _close(parts[0][1] + parts[1][1], x_full, 'sum X_C')
+
+
+def test_rotate_on_the_gpu_matches_oracle():
+    """ROTATE_DENSITYMATRIX (P_P_HELIX) as the SCF runs it on the device, against
+    the oracle's restatement (src/pdensitymatrix.f90:516-563)."""
+    s = system.build_system(geometry.polyethylene_deck('6-31G', cutoff1=5, cutoff2=10, kpoints=16), oracle.onee)
+    rng = np.random.default_rng(9)
+    n = s.basis.ncgs
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, rng.normal(size=(s.ncell1, n, n)) * 0.1, s.basis.cc)
+    ref = oracle.rotate_density(s, pp)
+    got = scf.rotate(scf.HostState(s, 'cuda'), torch.tensor(pp, device='cuda')).cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
