@@ -119,7 +119,7 @@ def build_problem(device: int):
     p_out, _, _, _ = scf.fock_build(st, st.t_c + st.n_c + c_c - 0.5 * x_c)
     p_p = scf.decontract(st, p_out)
     df0.close()
-    return sysm, p_p
+    return sysm, p_p, p_out
 
 
 def measure_fp64_peak(device: int) -> float:
@@ -245,6 +245,82 @@ def run_reference(args):
     return 0
 
 
+def build_rate(sysm, device: int, p_p, p_ph=None, steps: int = 3, warmup: int = 1, **kw):
+    """Fock builds/s of one system with device-resident densities (CUDA events,
+    L2 flushed before each build), with its census rates; also returns the
+    last build's (C_C, X_C) in the Fortran layout."""
+    import torch
+    from polymer_b200 import fock
+    dev = torch.device('cuda', device)
+    t0 = time.perf_counter()
+    df = fock.DeviceFock(sysm, device, **kw)
+    torch.cuda.synchronize(dev)
+    t_setup = time.perf_counter() - t0
+    pp = p_p.transpose(-1, -2).contiguous()
+    ph = p_ph.transpose(-1, -2).contiguous() if p_ph is not None else None
+    nc, n = sysm.ncell1, sysm.basis.ncgs
+    out_c = torch.empty((nc, n, n), dtype=torch.float64, device=dev)
+    out_x = torch.empty_like(out_c)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    for _ in range(warmup):
+        df.run_fortran(pp, ph, out_c, out_x)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    stream = torch.cuda.current_stream(dev)
+    for k in range(steps):
+        flush.fill_(float(k))
+        evs[k][0].record(stream)
+        df.run_fortran(pp, ph, out_c, out_x)
+        evs[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+    cen = df.census()
+    df.close()
+    return ({'build_ms': ms, 'builds_per_s': 1000.0 / ms, 'setup_s': t_setup, 'npgs': sysm.basis.npgs,
+             'ncgs': sysm.basis.ncgs, 'quartets_per_build': cen['quartets'],
+             'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
+             'quartets_fp32': cen['quartets_fp32'], 'launches_per_build': int(cen['kernel_launches'])},
+            (out_c, out_x))
+
+
+def extra_legs(device: int, peak: float):
+    """The other Fock-build configurations at their own sizes: C40H82 6-31G**
+    (1936 primitives, beyond the reference's 1024-primitive cap) and the helical
+    polyethylene chain in 6-31G at CUTOFF1/CUTOFF2 = 5/10 (translation-indexed
+    quartets, FP64).  Densities: one SCF iteration from the nuclear-charge guess
+    (C40H82), the nuclear-charge guess rotated into P_P_HELIX (the chain)."""
+    import torch
+    from polymer_b200 import fock, geometry, scf, system
+    dev = torch.device('cuda', device)
+    out = {}
+    s40 = system.build_system(geometry.alkane_deck(40, inttol=INTTOL), fock.onee)
+    st = scf.HostState(s40, dev)
+    p_p = scf.decontract(st, torch.tensor(scf.guess_density(s40), dtype=torch.float64, device=dev))
+    r, _ = build_rate(s40, device, p_p)
+    r['workload'] = workload_name(40)
+    r['frac_fp64_peak'] = r['tflops'] / peak if peak else None
+    out['c40h82'] = r
+    sh = system.build_system(geometry.polyethylene_deck('6-31G', cutoff1=5, cutoff2=10, kpoints=16), fock.onee)
+    st = scf.HostState(sh, dev)
+    p_p = scf.decontract(st, torch.tensor(scf.guess_density(sh), dtype=torch.float64, device=dev))
+    p_ph = scf.rotate(st, p_p)
+    r, (c64, x64) = build_rate(sh, device, p_p, p_ph)
+    r['workload'] = ('helical polyethylene 6-31G (C2H4 cell, period 2.55 A, 180 deg screw, seeded jitter 0.01 A), '
+                     'CUTOFF1/CUTOFF2 = 5/10, INTTOL 1e-10, FP64')
+    r['frac_fp64_peak'] = r['tflops'] / peak if peak else None
+    # far cells (ket images outside the CUTOFF1 box) in FP32, near cells in FP64
+    c64, x64 = c64.clone(), x64.clone()
+    rm, (cm, xm) = build_rate(sh, device, p_p, p_ph, precision=1, mixed_cutoff=1e-6)
+    dj, dk = cm - c64, xm - x64
+    r['mixed_far_cells_fp32'] = {'build_ms': rm['build_ms'], 'builds_per_s': rm['builds_per_s'],
+                                 'quartets_fp32_fraction': rm['quartets_fp32'] / max(rm['quartets_per_build'], 1.0),
+                                 'max_abs_dF': float((dj - 0.5 * dk).abs().max()),
+                                 'max_abs_dJ': float(dj.abs().max()), 'max_abs_dK': float(dk.abs().max()),
+                                 'against': 'the FP64 build of the same density (pinned to the oracle at this '
+                                            'configuration by the full-size parity tests)'}
+    out['helix_pe_631g_5_10'] = r
+    return out
+
+
 def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: bool = False, scf_runs: bool = True):
     """Uneven water clusters (cc-pVDZ, k ~ U{1..16} as geometry.water_batch_decks
     draws them) as one batch: batched full FP64 Fock builds per second, and the
@@ -365,6 +441,8 @@ def main():
                     help='water clusters in the batched leg (0: skip it)')
     ap.add_argument('--no-batch-scf', action='store_true',
                     help='batched leg: the batched builds only, no SCF of the set')
+    ap.add_argument('--no-extra', action='store_true',
+                    help='skip the C40H82 and helical-chain build rates')
     ap.add_argument('--autotune', action='store_true',
                     help='time every kernel variant per quartet class and keep the fastest '
                          '(default: the library\'s measured schedule table)')
@@ -380,7 +458,7 @@ def main():
     import numpy as np
     import torch
     import torch.distributed as dist
-    from polymer_b200 import capi, fock, system
+    from polymer_b200 import capi, fock, scf, system
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -391,7 +469,7 @@ def main():
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
     dev = torch.device('cuda', local)
 
-    sysm, p_p = build_problem(local)
+    sysm, p_p, p_c = build_problem(local)
     df = fock.DeviceFock(sysm, local, myid=rank, numprocs=world)
     cen = df.census()
     nc, n = sysm.ncell1, sysm.basis.ncgs
@@ -461,6 +539,35 @@ def main():
         all_flops = sum(k['flops'] for k in kern)
         roof['build_achieved'] = all_flops / (tot_ms * 1e-3) / 1e12
 
+    # ---- the mixed FP32/FP64 recursion (Schwarz x density cutoff 1e-6) on the same
+    # density, against the FP64 build (itself checked against the oracle on this
+    # workload by tests/test_baseline_configs_gpu.py): max|dF| (F = J - K/2) and
+    # dE = tr(P dJ)/2 - tr(P dK)/4 of this density
+    mixed = None
+    if world == 1:
+        dfm = fock.DeviceFock(sysm, local, precision=capi.PFE_PREC_MIXED, mixed_cutoff=1e-6)
+        c64, x64 = df(p_p)
+        cmx, xmx = dfm(p_p)
+        for _ in range(args.warmup):
+            dfm(p_p)
+        evm = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evm[k][0].record(stream)
+            dfm.run_fortran(pp_f, None, out_c, out_x)
+            evm[k][1].record(stream)
+        torch.cuda.synchronize()
+        cmm = dfm.census()
+        dj, dk = cmx - c64, xmx - x64
+        mixed = {'mixed_cutoff': 1e-6, 'build_ms': sum(a.elapsed_time(b) for a, b in evm) / args.steps,
+                 'quartets_fp32_fraction': cmm['quartets_fp32'] / max(cmm['quartets'], 1.0),
+                 'max_abs_dF': float((dj - 0.5 * dk).abs().max()),
+                 'max_abs_dJ': float(dj.abs().max()), 'max_abs_dK': float(dk.abs().max()),
+                 'dE': float(0.5 * (p_c[0] * dj[0]).sum() - 0.25 * (p_c[0] * dk[0]).sum()),
+                 'against': 'the FP64 build of the same density (pinned to the oracle at this workload by the '
+                            'full-size parity tests)'}
+        dfm.close()
+
     # ---- end to end through the host C ABI (pinned host buffers)
     e2e = None
     if world == 1:
@@ -519,6 +626,11 @@ def main():
 
     legs['scf_leg_s'] = time.perf_counter() - t_leg
     t_leg = time.perf_counter()
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        extra = extra_legs(local, peak)
+    legs['extra_leg_s'] = time.perf_counter() - t_leg
+    t_leg = time.perf_counter()
     batch = None
     if rank == 0 and world == 1 and args.batch > 0:
         batch = batch_leg(args.batch, local, args.steps, args.warmup, args.autotune, not args.no_batch_scf)
@@ -543,8 +655,8 @@ def main():
                            if world > 1 else 'single GPU'},
                 'quartets_per_build': cen['quartets'], 'quartets_per_s': cen['quartets'] * value,
                 'gpu_launches': args.steps * int(cen['kernel_launches']),
-                'roofline': roof, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'scf': scf_line,
-                'batch': batch, 'cpu_baseline': cpu, 'wall_clock_s': legs}
+                'roofline': roof, 'mixed': mixed, 'kernels': kern, 'clocks': clk.summary(), 'e2e': e2e, 'scf': scf_line,
+                'other_configs': extra, 'batch': batch, 'cpu_baseline': cpu, 'wall_clock_s': legs}
         print(json.dumps(line))
     df.close()
     if world > 1:

@@ -33,7 +33,8 @@ extern "C" {
 #define PFE_ENAN (-7)        /* non-finite density on input */
 
 #define PFE_PREC_FP64 0      /* every quartet in FP64 (parity path) */
-#define PFE_PREC_MIXED 1     /* quartets with Schwarz*|P|max below mixed_cutoff recur in FP32 */
+#define PFE_PREC_MIXED 1     /* molecules: quartets with Schwarz*|P|max below mixed_cutoff recur in FP32;
+                                lattices: quartets whose ket image lies outside the CUTOFF1 box */
 
 typedef struct pfe_args {
   int32_t npgs, ncgs, npshell;       /* NPGS, NCGS, NPSHELL (module BASISSET)            */
@@ -111,8 +112,12 @@ int32_t pfe_context_fock_pc(pfe_context *ctx, const double *d_p_c, double *d_c_c
  * Schwarz(ij)*Schwarz(kl)*M < density_tol are skipped (0 = off), and with
  * PFE_PREC_MIXED those with Schwarz(ij)*Schwarz(kl)*M < mixed_cutoff run the
  * recursion in FP32 (Boys function, geometry, contraction and J/K in FP64).
- * Meant for incremental builds from density differences.  Lattices: FP64 and
- * no density screening only (PFE_EUNSUPPORTED otherwise). */
+ * Meant for incremental builds from density differences.  Lattices and
+ * helices: no density screening (PFE_EUNSUPPORTED); PFE_PREC_MIXED (with any
+ * positive mixed_cutoff) runs the recursion of every quartet whose ket image
+ * Q3 lies outside the CUTOFF1 box (the far cells) in FP32 and the near cells
+ * in FP64 (Boys function, geometry and J/K accumulation stay FP64).  The same
+ * holds for precision_mode/mixed_cutoff in pfe_args. */
 int32_t pfe_context_set_screening(pfe_context *ctx, int32_t precision_mode, double mixed_cutoff,
                                   double density_tol);
 

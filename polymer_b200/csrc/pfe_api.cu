@@ -515,9 +515,13 @@ int32_t pfe_context_set_screening(pfe_context* ctx, int32_t precision_mode, doub
     return PFE_EINVAL;
   }
   if (!(mixed_cutoff >= 0.0) || !(density_tol >= 0.0)) { set_error("cutoffs must be >= 0"); return PFE_EINVAL; }
-  if (!ctx->molecular && (precision_mode != PFE_PREC_FP64 || density_tol != 0.0)) {
-    set_error("mixed precision and density screening are implemented for molecules only");
+  if (!ctx->molecular && density_tol != 0.0) {
+    set_error("density screening is implemented for molecules only");
     return PFE_EUNSUPPORTED;
+  }
+  if (!ctx->molecular && precision_mode == PFE_PREC_MIXED && !(mixed_cutoff > 0.0)) {
+    set_error("lattices: PFE_PREC_MIXED needs a positive mixed_cutoff (it switches the far cells to FP32)");
+    return PFE_EINVAL;
   }
   ctx->mcut = precision_mode == PFE_PREC_MIXED ? mixed_cutoff : 0.0;
   ctx->dtol = density_tol;
@@ -690,7 +694,7 @@ int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
   out->quartets_ref = ctx->census_ref;
   out->flops = ctx->census_flops;
   out->quartets_fp32 = 0.0;
-  if (ctx->molecular && ctx->d_n32) {
+  if (ctx->d_n32) {
     unsigned long long n32 = 0;
     PFE_CUDA(cudaMemcpy(&n32, ctx->d_n32, sizeof(n32), cudaMemcpyDeviceToHost));
     out->quartets_fp32 = (double)n32;

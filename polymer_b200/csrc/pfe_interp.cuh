@@ -48,6 +48,36 @@ __device__ __forceinline__ double eval_op(const unsigned short* __restrict__ ops
   return val;
 }
 
+// The same op in FP32 (the mixed-precision lattice path): slots hold F_m/pref
+// and the recursion's geometry rounded to float.
+struct OpGeomF {
+  float G1[4][3], G2[4][3];
+  float X[4], Y[4], Z;
+};
+
+__device__ __forceinline__ float eval_op_f(const unsigned short* __restrict__ ops, int o, const float* v,
+                                           const OpGeomF& geo) {
+  const uint4 r = __ldg(reinterpret_cast<const uint4*>(ops) + o);
+  const int h = r.x & 0xffff;
+  const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
+  float val = geo.G1[kind][ax] * v[r.x >> 16] + geo.G2[kind][ax] * v[r.y & 0xffff];
+  if (cA) val += (float)cA * geo.X[kind] * (v[r.y >> 16] - geo.Y[kind] * v[r.z & 0xffff]);
+  if (cB) val += (float)cB * geo.Z * v[r.z >> 16];
+  return val;
+}
+
+__device__ __forceinline__ void geom_to_float(const OpGeom& g, OpGeomF& f) {
+  for (int k = 0; k < 4; ++k) {
+    for (int a = 0; a < 3; ++a) {
+      f.G1[k][a] = (float)g.G1[k][a];
+      f.G2[k][a] = (float)g.G2[k][a];
+    }
+    f.X[k] = (float)g.X[k];
+    f.Y[k] = (float)g.Y[k];
+  }
+  f.Z = (float)g.Z;
+}
+
 __device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restrict__ v, const OpGeom& geo,
                                             int base) {
   for (int l = 0; l < t.nlevels; ++l) {

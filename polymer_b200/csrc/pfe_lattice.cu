@@ -233,6 +233,10 @@ struct LatticeRun {
   const int* qcell;
   LatGeom g;
   int npgs;
+  // mixed precision: ket images Q3 outside the CUTOFF1 box (the far cells) run
+  // the recursion in FP32, the rest in FP64; n32 counts the FP32 quartets
+  int far32;
+  unsigned long long* n32;
 };
 
 // (LA LB|LC LD) is the evaluated canonical class; SWAP: its first pair is the ket.
@@ -246,12 +250,16 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
   constexpr int NBRA = N1 * N2;
   extern __shared__ double smem[];
   __shared__ OpGeom s_geo[8];
+  __shared__ OpGeomF s_geof[8];
   __shared__ int s_prm[8][N1 + N2 + M1 + M2];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   double* v = smem + (size_t)wid * per_warp;
   double* DJ = v + tab.nslots;      // D(k,l), [c][d] over ket canonical comps
   double* DK = DJ + M1 * M2;        // D(k,j), [ket comp of K][bra comp of J]
   OpGeom& geo = s_geo[wid];
+  OpGeomF& geof = s_geof[wid];
+  float* vf = reinterpret_cast<float*>(v);   // the slots as floats on the FP32 path
+  unsigned long long n32 = 0;
   int* b1 = s_prm[wid];             // bra first centre prims
   int* b2 = b1 + N1;
   int* k1 = b2 + N2;
@@ -292,6 +300,9 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
                (q1[k] - q3[k] <= g.c1[k]);
       const double ang = q3x * g.helix, cs = cos(ang), sn = sin(ang);
       const double tr[3] = {q3x * g.period[0], q3y * g.period[1], q3z * g.period[2]};
+      // warp-uniform: the whole chunk's kets are images in the same cell Q3
+      const bool f32 = R.far32 && LT > 0 &&
+                       (abs(q3x) > g.c1[0] || abs(q3y) > g.c1[1] || abs(q3z) > g.c1[2]);
       for (int qq = ch.y; qq < ch.z; ++qq) {
         const bool swk = R.swp[qq] != 0;
         const double ze = pr.zeta[qq];
@@ -305,11 +316,19 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
                                 (Pb[2] - Q[2]) * (Pb[2] - Q[2]));
         const double pref = c2pi * pr.S[p] * pr.S[qq] * sqrt(rho);
         if (lane == 0) {
+          // FP32: the recursion runs on F_m/pref (values of order one); the
+          // outputs are scaled back by pref in FP64
           double F[LT + 1];
-          boys_tab<LT>(T, pref, R.boys, F);
-          v[0] = 0.0;
+          boys_tab<LT>(T, f32 ? 1.0 : pref, R.boys, F);
+          if (f32) {
+            vf[0] = 0.0f;
 #pragma unroll
-          for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
+            for (int m = 0; m <= LT; ++m) vf[1 + m] = (float)F[m];
+          } else {
+            v[0] = 0.0;
+#pragma unroll
+            for (int m = 0; m <= LT; ++m) v[1 + m] = F[m];
+          }
         } else if (lane == 1) {
           double WP[3], WQ[3];
           for (int k = 0; k < 3; ++k) {
@@ -321,6 +340,7 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
             set_geom(geo, PAb, WP, QC, WQ, ABb, CD, 0.5 / zb, 0.5 / ze, 0.5 / zz, rho / zb, rho / ze);
           else
             set_geom(geo, QC, WQ, PAb, WP, CD, ABb, 0.5 / ze, 0.5 / zb, 0.5 / zz, rho / ze, rho / zb);
+          if (f32) geom_to_float(geo, geof);
         }
         for (int x = lane; x < M1; x += 32) k1[x] = R.prim[pr.si[qq] * MAXCOMP + x];
         for (int x = lane; x < M2; x += 32) k2[x] = R.prim[pr.sj[qq] * MAXCOMP + x];
@@ -348,17 +368,24 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
             DK[t] = val;
           }
         }
-        for (int l = 0; l < tab.nlevels; ++l) {
-          const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-          for (int o = o0 + lane; o < o1; o += 32) {
-            v[base + o] = eval_op(tab.ops, o, v, geo);
+        if (f32) {
+          ++n32;
+          for (int l = 0; l < tab.nlevels; ++l) {
+            const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
+            for (int o = o0 + lane; o < o1; o += 32) vf[base + o] = eval_op_f(tab.ops, o, vf, geof);
+            __syncwarp();
           }
-          __syncwarp();
+        } else {
+          for (int l = 0; l < tab.nlevels; ++l) {
+            const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
+            for (int o = o0 + lane; o < o1; o += 32) v[base + o] = eval_op(tab.ops, o, v, geo);
+            __syncwarp();
+          }
         }
         // integral of bra comps (a over first, b over second) and ket comps (c, d)
         auto E = [&](int a, int b, int cc, int d) -> double {
           const int idx = SWAP ? ((cc * M2 + d) * N1 + a) * N2 + b : ((a * N2 + b) * M1 + cc) * M2 + d;
-          return v[tab.out[idx]];
+          return f32 ? pref * (double)vf[tab.out[idx]] : v[tab.out[idx]];
         };
         // J: C(i,j,Q1) += sum_kl DJ(k,l) (ij|kl), accumulated over the whole chunk
 #pragma unroll
@@ -393,6 +420,8 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
       }
     }
     // flush J of this chunk
+    if (lane == 0 && n32) atomicAdd(R.n32, n32);
+    n32 = 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const int t = lane + 32 * r;
@@ -548,6 +577,10 @@ int lattice_setup(pfe_context* ctx, const pfe_args* a) {
   cudaStream_t s = ctx->stream;
   LatticeState* L = new LatticeState();
   ctx->lattice = L;
+  if (!ctx->d_n32) {   // FP32 quartet counter of the mixed-precision path
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_n32, sizeof(unsigned long long)));
+    PFE_CUDA(cudaMemset(ctx->d_n32, 0, sizeof(unsigned long long)));
+  }
   const LatGeom g = make_geom(ctx);
   const int n = ctx->npshell;
   // cells of the REDUCED_CEL1 box, x fastest within the list index
@@ -766,6 +799,9 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
   R.qcell = L->d_qcell;
   R.g = make_geom(ctx);
   R.npgs = ctx->npgs;
+  R.far32 = ctx->mcut > 0.0 ? 1 : 0;
+  R.n32 = ctx->d_n32;
+  PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
   for (int i = 0; i < L->nlaunch; ++i) {
     const LatticeLaunch& ll = L->launches[i];
     R.chunks = ll.chunks;

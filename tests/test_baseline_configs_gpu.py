@@ -15,7 +15,8 @@ that sum exactly to the whole build):
 * a 16-water cluster in cc-pVDZ (1072 primitives: beyond the reference's
   1024-primitive cap, so only the oracle can check it);
 * the helical polyethylene chain in 6-31G at CUTOFF1/CUTOFF2 = 5/10 (121
-  cell-pair tickets, Q3 over 21 cells), full build.
+  cell-pair tickets, Q3 over 21 cells), full build, FP64 and with the far
+  cells (Q3 outside the CUTOFF1 box) in FP32.
 
 FP64 tolerance as the other parity tests: |dC_C|, |dX_C| <= 1e-11 max|C_C| +
 1e-13 Hartree.
@@ -34,6 +35,9 @@ RTOL = 1e-11
 # mixed FP32/FP64 recursion: quartets whose Schwarz bound times max|P| is below
 # 1e-6 run in FP32; their error is ~1e-7 of values below 1e-6 per quartet
 MIXED_TOL = 1e-8
+# lattices: every quartet of a far cell runs in FP32, whatever its size; the
+# far cells' share of J is a sum of many Coulomb tails, each good to ~1e-7
+LATTICE_MIXED_TOL = 1e-6
 
 
 def _onee_s(sysm):
@@ -109,3 +113,9 @@ def test_helical_chain_at_cutoff_5_10_matches_oracle():
     c_gpu, x_gpu = fock.fourindex_eri(s, pp, ph)
     _close(c_gpu, c_ref, 'C_C')
     _close(x_gpu, x_ref, 'X_C')
+    # far cells (ket images outside the CUTOFF1 box) in FP32, near cells FP64
+    c_mx, x_mx = fock.fourindex_eri(s, pp, ph, precision=1, mixed_cutoff=1e-6)
+    dj = _close(c_mx, c_ref, 'mixed C_C', LATTICE_MIXED_TOL)
+    dk = _close(x_mx, x_ref, 'mixed X_C', LATTICE_MIXED_TOL)
+    assert dj > 0.0   # the far cells did run in FP32
+    print('helix 5/10 far cells FP32: max|dJ| %.2e, max|dK| %.2e (max|J| %.2e)' % (dj, dk, np.abs(c_ref).max()))
