@@ -4,7 +4,9 @@ The other parity tests use small systems so the oracle finishes in seconds on
 one core.  These run the configurations the throughput and time-to-solution
 numbers are quoted on, with the oracle spread over the host's cores
 (tests/oracle_pool.py splits J/K into bra-shell or cell-pair-ticket pieces
-that sum exactly to the whole build):
+that sum exactly to the whole build), or, for the two largest cases, against
+projections of the oracle's J and K made the same way and committed as
+fixtures (tests/golden/make_fullsize.py):
 
 * the all-trans alkanes C10H22 and C20H42 in 6-31G** at INTTOL 1e-10 (C20H42
   is the Fock-build benchmark), FP64, and the mixed FP32/FP64 path at the
@@ -21,12 +23,16 @@ that sum exactly to the whole build):
 FP64 tolerance as the other parity tests: |dC_C|, |dX_C| <= 1e-11 max|C_C| +
 1e-13 Hartree.
 """
+import os
+
 import numpy as np
 import pytest
 import torch
 
 import oracle
 import oracle_pool
+from conftest import GOLDEN
+from golden import make_fullsize
 from polymer_b200 import fock, geometry, scf, system
 
 pytestmark = [pytest.mark.gpu, pytest.mark.slow]
@@ -60,10 +66,9 @@ def _mol_density(sysm, seed):
     return np.einsum('ai,cab,bj->cij', sysm.basis.cc, (a + a.T)[None], sysm.basis.cc)
 
 
-@pytest.mark.parametrize('n', [10, 20])
-def test_alkane_at_full_size_matches_oracle(n):
-    s = system.build_system(geometry.alkane_deck(n, inttol=1e-10), _onee_s)
-    pp = _mol_density(s, seed=100 + n)
+def test_c10h22_at_full_size_matches_oracle():
+    s = system.build_system(geometry.alkane_deck(10, inttol=1e-10), _onee_s)
+    pp = _mol_density(s, seed=110)
     c_ref, x_ref = oracle_pool.fourindex_eri(s, pp)
     c_gpu, x_gpu = fock.fourindex_eri(s, pp)
     _close(c_gpu, c_ref, 'C_C')
@@ -71,8 +76,36 @@ def test_alkane_at_full_size_matches_oracle(n):
     c_mx, x_mx = fock.fourindex_eri(s, pp, precision=1, mixed_cutoff=1e-6)
     dj = _close(c_mx, c_ref, 'mixed C_C', MIXED_TOL)
     dk = _close(x_mx, x_ref, 'mixed X_C', MIXED_TOL)
-    print('C%dH%d mixed FP32/FP64 at 1e-6: max|dJ| %.2e, max|dK| %.2e (max|J| %.2e)'
-          % (n, 2 * n + 2, dj, dk, np.abs(c_ref).max()))
+    print('C10H22 mixed FP32/FP64 at 1e-6: max|dJ| %.2e, max|dK| %.2e (max|J| %.2e)'
+          % (dj, dk, np.abs(c_ref).max()))
+
+
+def _check_projected(name, c, x, rtol):
+    """(C_C, X_C) against the oracle's projections in tests/golden/fullsize_<name>.npz
+    (made by tests/golden/make_fullsize.py): an element-wise agreement to
+    rtol*max|C_C| bounds every projection by that times ||R[:, k]||_1."""
+    g = np.load(os.path.join(GOLDEN, 'fullsize_%s.npz' % name))
+    r = make_fullsize.projector(c.shape[0])
+    w = np.abs(r).sum(axis=0)
+    for got, ref, m, what in ((c @ r, g['cr'], float(g['cmax']), 'C_C'), (x @ r, g['xr'], float(g['xmax']), 'X_C')):
+        err = np.abs(got - ref).max(axis=0)
+        assert np.all(err <= (rtol * m + 1e-13) * w), '%s %s: projected |diff| %s vs bound %s' % (
+            name, what, err, (rtol * m + 1e-13) * w)
+    assert abs(np.abs(c).max() - float(g['cmax'])) <= rtol * float(g['cmax']) + 1e-13
+    assert abs(np.abs(x).max() - float(g['xmax'])) <= rtol * float(g['xmax']) + 1e-13
+
+
+def test_c20h42_benchmark_workload_matches_oracle():
+    """The Fock-build benchmark itself (C20H42 6-31G**, INTTOL 1e-10): FP64 and
+    the mixed path against the oracle's J and K (projected fixtures)."""
+    s = system.build_system(geometry.alkane_deck(20, inttol=1e-10), _onee_s)
+    pc, pp = make_fullsize.density(s, 120)
+    c_gpu, x_gpu = fock.fourindex_eri(s, pp)
+    _check_projected('c20h42', c_gpu[0], x_gpu[0], RTOL)
+    c_mx, x_mx = fock.fourindex_eri(s, pp, precision=1, mixed_cutoff=1e-6)
+    _check_projected('c20h42', c_mx[0], x_mx[0], MIXED_TOL)
+    print('C20H42 mixed FP32/FP64 at 1e-6 against FP64: max|dJ| %.2e, max|dK| %.2e'
+          % (np.abs(c_mx - c_gpu).max(), np.abs(x_mx - x_gpu).max()))
 
 
 def test_water_single_point_scf_matches_oracle_scf():
@@ -88,11 +121,9 @@ def test_water_single_point_scf_matches_oracle_scf():
 def test_water16_cluster_matches_oracle():
     s = system.build_system(geometry.water_deck(16, seed=2001), _onee_s)
     assert s.basis.npgs == 1072
-    pp = _mol_density(s, seed=16)
-    c_ref, x_ref = oracle_pool.fourindex_eri(s, pp)
+    pc, pp = make_fullsize.density(s, 16)
     c_gpu, x_gpu = fock.fourindex_eri(s, pp)
-    _close(c_gpu, c_ref, 'C_C')
-    _close(x_gpu, x_ref, 'X_C')
+    _check_projected('water16', c_gpu[0], x_gpu[0], RTOL)
 
 
 def test_helical_chain_at_cutoff_5_10_matches_oracle():

@@ -38,3 +38,17 @@ def test_lattice_tickets_sum_to_the_whole_build():
     c2, x2 = oracle_pool.fourindex_eri(s, pp, ph, nproc=2)
     assert np.abs(c1 - c2).max() <= 1e-12 * np.abs(c1).max()
     assert np.abs(x1 - x2).max() <= 1e-12 * np.abs(x1).max()
+
+
+def test_fullsize_fixtures_describe_the_test_systems():
+    """The projected oracle fixtures of the full-size parity tests belong to the
+    systems and seeded densities the GPU test builds (sizes and seeds)."""
+    import os
+    from conftest import GOLDEN
+    from golden import make_fullsize
+    for name, make in make_fullsize.cases().items():
+        g = np.load(os.path.join(GOLDEN, 'fullsize_%s.npz' % name))
+        s, seed = make()
+        assert int(g['npgs']) == s.basis.npgs and int(g['ncgs']) == s.basis.ncgs and int(g['seed']) == seed
+        assert g['cr'].shape == (s.basis.ncgs, 4) and g['xr'].shape == (s.basis.ncgs, 4)
+        assert float(g['cmax']) > 0.0 and float(g['xmax']) > 0.0
