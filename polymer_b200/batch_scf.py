@@ -32,6 +32,7 @@ from typing import Callable, List, Optional, Sequence
 
 import numpy as np
 import torch
+from torch.cuda import nvtx
 
 from . import fock as fock_mod
 from .scf import SCFError, guess_density, incremental_tol
@@ -365,8 +366,11 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             pv.copy_(upd)
             g.view(dp).copy_((pv - g.view(p_ref) * incr_t[sl][:, None, None]) * live_t[sl][:, None, None])
         mark('host')
+        nvtx.range_push('batched Fock build')
         fb.run_packed(dp, dc, dx)
+        nvtx.range_pop()
         mark('build')
+        nvtx.range_push('Fock assembly, DIIS, SP2 projector')
         for g in groups:
             sl = g.sl
             im = incr_t[sl][:, None, None]
@@ -394,6 +398,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             dchg = torch.sqrt(((pn - pv) ** 2).sum((1, 2)) / float(g.n * g.n))
             stats_t[sl] = torch.stack([e, fe, dchg, defect], 1)
         slot_t.add_(1).remainder_(D)
+        nvtx.range_pop()
 
     state = np.full(nmol, _FULL)
     nbuild = np.zeros(nmol, dtype=int)
@@ -414,6 +419,9 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
     cuda_graph = None
     replays = 0
     for it in range(1, ncycles + 1):
+        if it > 1:
+            nvtx.range_pop()
+        nvtx.range_push('batched SCF iteration %d' % it)
         # ---- per-molecule build mode and screening
         for kk in range(nmol):
             if done[kk]:
@@ -500,6 +508,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
                 float(host[~done, 2].max()) if nd < nmol else 0.0, '  (graph)' if cuda_graph is not None else ''))
         if done.all():
             break
+    nvtx.range_pop()   # the last iteration's range
     # apply the last outcome (molecules that did not converge keep their newest density)
     for g in groups:
         tk = torch.from_numpy(take[g.sl]).to(dev)

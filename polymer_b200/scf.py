@@ -104,6 +104,14 @@ def _eigh(a: torch.Tensor):
         return e.to(a.device), v.to(a.device)
 
 
+def _nvtx_iteration(iscf: int) -> None:
+    """NVTX range of one SCF iteration (closes the previous one): the phases a
+    profiler timeline shows around the Fock builds."""
+    if iscf > 1:
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.nvtx.range_push('SCF iteration %d' % iscf)
+
+
 def guess_density(sysm: System) -> np.ndarray:
     """Nuclear-charge diagonal guess (GUESS_DENSITYMATRIX, src/pdensitymatrix.f90:83-127)."""
     b, d = sysm.basis, sysm.deck
@@ -394,6 +402,7 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
     eps = None
     mu = 0.0
     for iscf in range(1, ncycles + 1):
+        _nvtx_iteration(iscf)
         ti = time.perf_counter()
         tf = time.perf_counter()
         if fast is None:
@@ -460,6 +469,7 @@ def run_scf(sysm: System, fock: FockBuilder, *, device='cpu', p_c0: Optional[np.
             break
         final_pending = False
         e_old = e
+    torch.cuda.nvtx.range_pop()   # the last iteration's range
     if not converged and raise_on_fail:
         raise SCFError('SCF CONVERGENCE NOT MET')
     e, comp = energy(st, p_c, c_c, x_c, d.hfexchange, sysm.e_nuc, d.temphf, eps, mu, nelec)
@@ -523,6 +533,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
     eps = None
     last_change = math.inf
     for iscf in range(1, ncycles + 1):
+        _nvtx_iteration(iscf)
         ti = time.perf_counter()
         full = final_pending or ref is None or not opts.incremental or nbuild % max(1, opts.reset_every) == 0
         tf = time.perf_counter()
@@ -597,6 +608,7 @@ def run_scf_fast(sysm: System, fock, *, opts: Optional[FastOptions] = None, devi
             break
         final_pending = dchg < conv
         p_c = p_new
+    torch.cuda.nvtx.range_pop()   # the last iteration's range
     if not converged and raise_on_fail:
         raise SCFError('SCF CONVERGENCE NOT MET')
     comp = {'total': e, 'guess_fallback': fallback, 'first_error': iters[0].asymmetry if iters else None}
