@@ -752,6 +752,10 @@ int32_t pfe_context_autotune(pfe_context* ctx, const double* d_p_p, const double
 int32_t pfe_context_force_variant(pfe_context* ctx, int32_t variant) {
   if (!ctx || !ctx->ready) { set_error("context is not set up"); return PFE_EINVAL; }
   if (variant < 0 || variant > 3) { set_error("variant must be 0, 1, 2 or 3"); return PFE_EINVAL; }
+  if (!ctx->molecular) {   // lattices: straight-line kernels where a class has them (0) or the interpreter
+    lattice_force_interpreter(ctx, variant != 0);
+    return PFE_OK;
+  }
   for (int i = 0; i < ctx->nlaunch; ++i) {
     ClassLaunch& cl = ctx->launches[i];
     if (variant == 0 && cl.has_straight) cl.variant = 0;

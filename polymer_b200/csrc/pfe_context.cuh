@@ -70,6 +70,8 @@ struct ClassLaunch {
   bool has_wide;
   int wide_wpb, wide_per_warp, wide_vmax, wide_xmax;
   size_t smem_wide;
+  int* queue;                // device work queue: one chunk counter per launch (pass), zeroed before each
+  unsigned int* cost;        // screened primitive quartets per chunk (chunks are sorted by it, descending)
   int npass;                 // launches of the straight-line variant
   int gmul = 32;             // straight-line variant: persistent grid of up to gmul blocks per SM
 };
@@ -144,6 +146,7 @@ struct pfe_context {
   int class_off[8] = {0}, class_n[8] = {0};
   pfe::ClassLaunch launches[64];
   int nlaunch = 0;
+  int* d_queue = nullptr;    // 64 chunk counters per class launch (the work queues of launches[])
   double census_quartets = 0.0, census_flops = 0.0, census_ref = 0.0, census_fp32 = 0.0;
 
   // host-path staging (pfe_fourindex_eri)
@@ -207,6 +210,7 @@ struct pfe_batch {
   std::vector<long long> off;       // packed offsets (doubles) of the ncgs x ncgs matrices, n+1
   pfe::ClassLaunch launches[64];    // joined chunk lists; ops/tables of the first instance with the class
   int nlaunch = 0;
+  int* d_queue = nullptr;           // the joined launches' work queues (64 counters each)
   void* d_insts = nullptr;          // the instances' launch records (MolLaunch) on the device
   void* h_insts = nullptr;          // ... and their pinned host copy, uploaded by every build (so a
                                     // captured graph re-reads it at each replay)
@@ -273,6 +277,7 @@ int lattice_setup(pfe_context* ctx, const pfe_args* a);
 int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, double* d_cc, double* d_xc,
                  cudaStream_t s);
 void lattice_release(pfe_context* ctx);
+void lattice_force_interpreter(pfe_context* ctx, bool on);
 const char* last_error_cstr();
 int measure_fp64_peak(int device, double* tflops);
 }  // namespace pfe

@@ -34,18 +34,48 @@ struct OpGeom {
   double X[4], Y[4], Z;
 };
 
-// Value of op o of a table: each op is one 16-byte record of eight uint16,
+// Value of an op of a table: each op is one 16-byte record of eight uint16,
 // (kind<<12 | axis<<10 | cA<<5 | cB, s1, s2, s3, s4, s5, 0, 0), read with one
 // vector load:  G1*v[s1] + G2*v[s2] + cA*X*(v[s3] - Y*v[s4]) + cB*Z*v[s5].
-__device__ __forceinline__ double eval_op(const unsigned short* __restrict__ ops, int o, const double* v,
-                                          const OpGeom& geo) {
-  const uint4 r = __ldg(reinterpret_cast<const uint4*>(ops) + o);
+__device__ __forceinline__ double eval_rec(const uint4 r, const double* v, const OpGeom& geo) {
   const int h = r.x & 0xffff;
   const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
   double val = geo.G1[kind][ax] * v[r.x >> 16] + geo.G2[kind][ax] * v[r.y & 0xffff];
   if (cA) val += (double)cA * geo.X[kind] * (v[r.y >> 16] - geo.Y[kind] * v[r.z & 0xffff]);
   if (cB) val += (double)cB * geo.Z * v[r.z >> 16];
   return val;
+}
+
+__device__ __forceinline__ double eval_op(const unsigned short* __restrict__ ops, int o, const double* v,
+                                          const OpGeom& geo) {
+  return eval_rec(__ldg(reinterpret_cast<const uint4*>(ops) + o), v, geo);
+}
+
+struct EvalD {
+  __device__ __forceinline__ double operator()(const uint4 r, const double* v, const OpGeom& g) const {
+    return eval_rec(r, v, g);
+  }
+};
+
+// One level [o0, o1) of a table by a team of `team` threads (this one is tid):
+// the ops of a level only read lower levels, so each thread loads four op
+// records before evaluating any of them (four record loads in flight instead
+// of one load-use chain per op).
+template <typename T, typename Geo, typename Eval>
+__device__ __forceinline__ void run_level(const unsigned short* __restrict__ ops, int o0, int o1, T* v, int base,
+                                          const Geo& geo, int tid, int team, Eval eval) {
+  const uint4* rec = reinterpret_cast<const uint4*>(ops);
+  int o = o0 + tid;
+  for (; o + 3 * team < o1; o += 4 * team) {
+    const uint4 r0 = __ldg(rec + o), r1 = __ldg(rec + o + team), r2 = __ldg(rec + o + 2 * team),
+                r3 = __ldg(rec + o + 3 * team);
+    const T a0 = eval(r0, v, geo), a1 = eval(r1, v, geo), a2 = eval(r2, v, geo), a3 = eval(r3, v, geo);
+    v[base + o] = a0;
+    v[base + o + team] = a1;
+    v[base + o + 2 * team] = a2;
+    v[base + o + 3 * team] = a3;
+  }
+  for (; o < o1; o += team) v[base + o] = eval(__ldg(rec + o), v, geo);
 }
 
 // The same op in FP32 (the mixed-precision lattice path): slots hold F_m/pref
@@ -55,9 +85,7 @@ struct OpGeomF {
   float X[4], Y[4], Z;
 };
 
-__device__ __forceinline__ float eval_op_f(const unsigned short* __restrict__ ops, int o, const float* v,
-                                           const OpGeomF& geo) {
-  const uint4 r = __ldg(reinterpret_cast<const uint4*>(ops) + o);
+__device__ __forceinline__ float eval_rec_f(const uint4 r, const float* v, const OpGeomF& geo) {
   const int h = r.x & 0xffff;
   const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
   float val = geo.G1[kind][ax] * v[r.x >> 16] + geo.G2[kind][ax] * v[r.y & 0xffff];
@@ -65,6 +93,12 @@ __device__ __forceinline__ float eval_op_f(const unsigned short* __restrict__ op
   if (cB) val += (float)cB * geo.Z * v[r.z >> 16];
   return val;
 }
+
+struct EvalF {
+  __device__ __forceinline__ float operator()(const uint4 r, const float* v, const OpGeomF& g) const {
+    return eval_rec_f(r, v, g);
+  }
+};
 
 __device__ __forceinline__ void geom_to_float(const OpGeom& g, OpGeomF& f) {
   for (int k = 0; k < 4; ++k) {
@@ -82,7 +116,7 @@ __device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restr
                                             int base) {
   for (int l = 0; l < t.nlevels; ++l) {
     const int o0 = t.levels[l], o1 = t.levels[l + 1];
-    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) v[base + o] = eval_op(t.ops, o, v, geo);
+    run_level(t.ops, o0, o1, v, base, geo, (int)threadIdx.x, (int)blockDim.x, EvalD{});
     __syncthreads();
   }
 }

@@ -32,6 +32,7 @@
 #include "pfe_common.cuh"
 #include "pfe_context.cuh"
 #include "pfe_interp.cuh"
+#include "pfe_lattice.cuh"
 
 namespace pfe {
 
@@ -60,17 +61,12 @@ struct LatticeState {
   double* d_quirk = nullptr;   // ntk * npl bra bounds (sorted order of the Q1 list)
   LatticeLaunch launches[36];
   int nlaunch = 0;
+  int* d_queue = nullptr;      // one chunk counter per launch (straight-line kernels)
+  bool interpret_only = false; // every class on the op-table interpreter (tests)
   double quartets = 0.0, flops = 0.0;
 };
 
 // ---------------------------------------------------------------- set-up kernels
-
-struct LatGeom {
-  int c1[3], c2[3];
-  int n1[3];
-  double period[3];
-  double helix;
-};
 
 __device__ __forceinline__ void screw(const LatGeom& g, double x, double y, double z, int qx, int qy, int qz,
                                       double* o) {
@@ -79,10 +75,6 @@ __device__ __forceinline__ void screw(const LatGeom& g, double x, double y, doub
   o[0] = x + qx * g.period[0];
   o[1] = y * c - z * s + qy * g.period[1];
   o[2] = y * s + z * c + qz * g.period[2];
-}
-
-__device__ __forceinline__ int cell1_index(const LatGeom& g, int qx, int qy, int qz) {
-  return (qx + g.c1[0]) + g.n1[0] * ((qy + g.c1[1]) + g.n1[1] * (qz + g.c1[2]));
 }
 
 // Fill pair record t for shells (I at cell A, J at cell B) with overlap S.
@@ -218,27 +210,6 @@ __global__ void k_lat_fill(const int* __restrict__ nvalid, const int* __restrict
 
 // ---------------------------------------------------------------- build kernel
 
-struct LatticeRun {
-  PairArrays pairs;
-  const unsigned char* swp;
-  const int* prim;
-  const double* boys;
-  const double* pp;    // P_P (npgs,npgs,cells1)
-  const double* pph;   // P_P_HELIX or null
-  double* cp;          // C_P (npgs,npgs,cells1)
-  double* xp;
-  const int4* chunks;
-  const int* nchunks;
-  const int4* tickets;
-  const int* qcell;
-  LatGeom g;
-  int npgs;
-  // mixed precision: ket images Q3 outside the CUTOFF1 box (the far cells) run
-  // the recursion in FP32, the rest in FP64; n32 counts the FP32 quartets
-  int far32;
-  unsigned long long* n32;
-};
-
 // (LA LB|LC LD) is the evaluated canonical class; SWAP: its first pair is the ket.
 template <int LA, int LB, int LC, int LD, bool SWAP>
 __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, int per_warp) {
@@ -372,13 +343,13 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
           ++n32;
           for (int l = 0; l < tab.nlevels; ++l) {
             const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-            for (int o = o0 + lane; o < o1; o += 32) vf[base + o] = eval_op_f(tab.ops, o, vf, geof);
+            run_level(tab.ops, o0, o1, vf, base, geof, lane, 32, EvalF{});
             __syncwarp();
           }
         } else {
           for (int l = 0; l < tab.nlevels; ++l) {
             const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-            for (int o = o0 + lane; o < o1; o += 32) v[base + o] = eval_op(tab.ops, o, v, geo);
+            run_level(tab.ops, o0, o1, v, base, geo, lane, 32, EvalD{});
             __syncwarp();
           }
         }
@@ -577,6 +548,7 @@ int lattice_setup(pfe_context* ctx, const pfe_args* a) {
   cudaStream_t s = ctx->stream;
   LatticeState* L = new LatticeState();
   ctx->lattice = L;
+  PFE_CUDA(ctx->alloc((void**)&L->d_queue, sizeof(int) * 64));
   if (!ctx->d_n32) {   // FP32 quartet counter of the mixed-precision path
     PFE_CUDA(ctx->alloc((void**)&ctx->d_n32, sizeof(unsigned long long)));
     PFE_CUDA(cudaMemset(ctx->d_n32, 0, sizeof(unsigned long long)));
@@ -802,13 +774,21 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
   R.far32 = ctx->mcut > 0.0 ? 1 : 0;
   R.n32 = ctx->d_n32;
   PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
+  PFE_CUDA(cudaMemsetAsync(L->d_queue, 0, sizeof(int) * 64, s));
   for (int i = 0; i < L->nlaunch; ++i) {
     const LatticeLaunch& ll = L->launches[i];
     R.chunks = ll.chunks;
     R.nchunks = ll.d_nchunks;
+    R.queue = L->d_queue + i;
     const int e1 = std::max(ll.cb, ll.ck), e2 = std::min(ll.cb, ll.ck);
-    int grid = std::min((ll.ncells_chunks + ll.wpb - 1) / ll.wpb, ctx->num_sms * 8);
-    lat_variant(e1, e2, ll.cb < ll.ck).fn(R, ll.tab, std::max(grid, 1), ll.wpb, ll.per_warp, ll.smem, s);
+    if (LatSlFn f = L->interpret_only ? nullptr : lattice_sl_launcher(e1, e2, ll.cb < ll.ck)) {
+      // straight-line: one chunk per warp from the queue, a persistent grid of 16 blocks per SM
+      const int grid = std::min((ll.ncells_chunks + 3) / 4, ctx->num_sms * 16);
+      f(R, std::max(grid, 1), s);
+    } else {
+      int grid = std::min((ll.ncells_chunks + ll.wpb - 1) / ll.wpb, ctx->num_sms * 8);
+      lat_variant(e1, e2, ll.cb < ll.ck).fn(R, ll.tab, std::max(grid, 1), ll.wpb, ll.per_warp, ll.smem, s);
+    }
     PFE_CUDA(cudaGetLastError());
   }
   int rc = contract_outputs(ctx, ctx->d_jp, ctx->d_kp, d_cc, d_xc, /*symmetrize=*/false, ctx->ncell1, s);
@@ -830,6 +810,10 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
     }
   }
   return PFE_OK;
+}
+
+void lattice_force_interpreter(pfe_context* ctx, bool on) {
+  if (ctx->lattice) ((LatticeState*)ctx->lattice)->interpret_only = on;
 }
 
 void lattice_release(pfe_context* ctx) {

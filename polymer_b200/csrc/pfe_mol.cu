@@ -248,9 +248,12 @@ __global__ void k_chunk_fill(const double* __restrict__ gr_max, const int* __res
 
 // Primitive quartets of every chunk that pass the screen (the census): lane per
 // ket group, binary search over each ket group's bound-sorted pairs.
+// Screened primitive quartets of every chunk (its cost, also the sort key of
+// the work queue) and their total.
 __global__ void k_chunk_census(const int4* __restrict__ chunks, int nchunks, const int* __restrict__ bk_list,
                                const int* __restrict__ gr_start, const int* __restrict__ gr_n,
-                               const double* __restrict__ sch, double inttol, unsigned long long* __restrict__ total) {
+                               const double* __restrict__ sch, double inttol, unsigned long long* __restrict__ total,
+                               unsigned int* __restrict__ cost) {
   const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= nchunks) return;
@@ -272,7 +275,10 @@ __global__ void k_chunk_census(const int4* __restrict__ chunks, int nchunks, con
     }
   }
   for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-  if (lane == 0 && n) atomicAdd(total, n);
+  if (lane == 0) {
+    if (n) atomicAdd(total, n);
+    cost[c] = (unsigned int)min(n, 0xffffffffull);
+  }
 }
 
 // ------------------------------------------------------------------ density in target space
@@ -515,9 +521,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
         sync();
         for (int l = 0; l < t_nlevels; ++l) {
           const int o0 = t_levels[l], o1 = t_levels[l + 1];
-          for (int o = o0 + tid; o < o1; o += team) {
-            v[base + o] = eval_op(t_ops, o, v, geo);
-          }
+          run_level(t_ops, o0, o1, v, base, geo, tid, team, EvalD{});
           sync();
         }
         const double w = sw[0];
@@ -846,6 +850,8 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
   // chunk lists for every class pair cb >= ck
   ctx->nlaunch = 0;
   ctx->census_quartets = ctx->census_flops = ctx->census_ref = 0.0;
+  PFE_CUDA(ctx->alloc((void**)&ctx->d_queue, sizeof(int) * 64 * 64));
+  PFE_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int) * 64 * 64, s));
   int maxg = 1;
   for (int c = 0; c < 6; ++c) maxg = std::max(maxg, cgn[c]);
   int *nchunk = nullptr, *offs = nullptr;
@@ -878,9 +884,26 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
       k_chunk_fill<<<(nbg + 127) / 128, 128, 0, s>>>(ctx->d_gr_max, ctx->d_bk_list, cg0[cb], nbg, seg[ck], cb == ck,
                                                      ctx->inttol, offs, cl.chunks);
       PFE_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
+      unsigned int *cost = nullptr, *cost_sorted = nullptr;
+      int4* sorted = nullptr;
+      PFE_CUDA(ctx->alloc((void**)&cost, sizeof(unsigned int) * total));
+      PFE_CUDA(ctx->alloc((void**)&cost_sorted, sizeof(unsigned int) * total));
+      PFE_CUDA(ctx->alloc((void**)&sorted, sizeof(int4) * total));
       k_chunk_census<<<(total + 3) / 4, 128, 0, s>>>(cl.chunks, total, ctx->d_bk_list, ctx->d_gr_start, ctx->d_gr_n,
-                                                     ctx->pairs.schwarz, ctx->inttol, d_total);
+                                                     ctx->pairs.schwarz, ctx->inttol, d_total, cost);
       PFE_CUDA(cudaGetLastError());
+      {  // the work queue hands out the costliest chunks first (stable: equal costs keep their order)
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, cost, cost_sorted, cl.chunks, sorted, total, 0, 32, s);
+        void* tmp = nullptr;
+        PFE_CUDA(ctx->alloc(&tmp, tb + 16));
+        PFE_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, cost, cost_sorted, cl.chunks, sorted, total, 0, 32,
+                                                           s));
+        PFE_CUDA(cudaMemcpyAsync(cl.chunks, sorted, sizeof(int4) * total, cudaMemcpyDeviceToDevice, s));
+        PFE_CUDA(cudaStreamSynchronize(s));
+        for (void* p : {(void*)tmp, (void*)cost, (void*)sorted}) ctx->free_now(p);
+        cl.cost = cost_sorted;   // kept: a batch sorts its joined chunk list by it
+      }
       unsigned long long nq = 0;
       PFE_CUDA(cudaMemcpyAsync(&nq, d_total, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
       PFE_CUDA(cudaStreamSynchronize(s));
@@ -949,6 +972,7 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
         return PFE_EUNSUPPORTED;
       }
       for (int v = 0; v < 4; ++v) cl.tuned_ms[v] = 0.f;
+      cl.queue = ctx->d_queue + 64 * ctx->nlaunch;
       ctx->launches[ctx->nlaunch++] = cl;
       ctx->census_quartets += (double)nq;
       ctx->census_flops += (double)nq * class_flops(cb, ck);
@@ -997,6 +1021,8 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
                          bool mixed) {
   ql.chunks = cl.chunks;
   ql.nchunks = cl.d_nchunks;
+  ql.queue = cl.queue;
+  cudaMemsetAsync(cl.queue, 0, sizeof(int) * 64, s);   // every launch (pass) of the class starts its queue at 0
   const int work = (cl.nchunks_host + ctx->numprocs - 1) / ctx->numprocs;
   if ((variant == 0 && cl.has_straight) || !cl.has_table) {
     const int grid = std::min((work + 3) / 4, ctx->num_sms * cl.gmul);
@@ -1200,6 +1226,7 @@ __global__ void k_tag_chunks(int4* __restrict__ chunks, int n, int instance) {
 // tags queued on one stream, one synchronisation at the end.
 int batch_setup(pfe_batch* b) {
   b->nlaunch = 0;
+  PFE_CUDA(b->alloc((void**)&b->d_queue, sizeof(int) * 64 * 64));
   cudaStream_t st = nullptr;
   PFE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   struct StreamGuard {
@@ -1230,8 +1257,11 @@ int batch_setup(pfe_batch* b) {
       }
       cl.nchunks_host = (int)total;
       cl.quartets = 0.0;
+      cl.queue = b->d_queue + 64 * b->nlaunch;
       PFE_CUDA(b->alloc((void**)&cl.chunks, sizeof(int4) * total));
       PFE_CUDA(b->alloc((void**)&cl.d_nchunks, sizeof(int)));
+      unsigned int* jcost = nullptr;
+      PFE_CUDA(b->alloc((void**)&jcost, sizeof(unsigned int) * total));
       PFE_CUDA(cudaMemcpy(cl.d_nchunks, &cl.nchunks_host, sizeof(int), cudaMemcpyHostToDevice));   // pageable: synchronous
       long long o = 0;
       for (size_t k = 0; k < b->inst.size(); ++k) {
@@ -1241,11 +1271,26 @@ int batch_setup(pfe_batch* b) {
           if (li.cb != cb || li.ck != ck) continue;
           PFE_CUDA(cudaMemcpyAsync(cl.chunks + o, li.chunks, sizeof(int4) * li.nchunks_host, cudaMemcpyDeviceToDevice,
                                    st));
+          PFE_CUDA(cudaMemcpyAsync(jcost + o, li.cost, sizeof(unsigned int) * li.nchunks_host,
+                                   cudaMemcpyDeviceToDevice, st));
           k_tag_chunks<<<(li.nchunks_host + 255) / 256, 256, 0, st>>>(cl.chunks + o, li.nchunks_host, (int)k);
           PFE_CUDA(cudaGetLastError());
           o += li.nchunks_host;
           cl.quartets += li.quartets;
         }
+      }
+      {  // one queue over the whole batch, costliest chunks first
+        unsigned int* ks = nullptr;
+        int4* vs = nullptr;
+        PFE_CUDA(b->alloc((void**)&ks, sizeof(unsigned int) * total));
+        PFE_CUDA(b->alloc((void**)&vs, sizeof(int4) * total));
+        size_t tb = 0;
+        cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, jcost, ks, cl.chunks, vs, (int)total, 0, 32, st);
+        void* tmp = nullptr;
+        PFE_CUDA(b->alloc(&tmp, tb + 16));
+        PFE_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp, tb, jcost, ks, cl.chunks, vs, (int)total, 0, 32, st));
+        PFE_CUDA(cudaMemcpyAsync(cl.chunks, vs, sizeof(int4) * total, cudaMemcpyDeviceToDevice, st));
+        cl.cost = ks;
       }
       b->launches[b->nlaunch++] = cl;
     }

@@ -66,8 +66,9 @@ struct MolLaunch {
   double dtol;            // skip quartets with bound * max|P| < dtol (0: the reference's screen only)
   double mcut;            // FP32 recursion where bound * max|P| < mcut (0: FP64 only)
   unsigned long long* n32;  // quartets run in FP32
-  const int4* chunks;     // (bra group, first list entry, end list entry, 0)
+  const int4* chunks;     // (bra group, first list entry, end list entry, 0), costliest first
   const int* nchunks;
+  int* queue;             // chunk counters (one per pass), zero at launch: warps take chunks in order
   double inttol;
   int nt;
   int myid, numprocs;
@@ -217,11 +218,16 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   auto in_pass = [&](int a, int b) { const int k = ORD.pos[a * NB + b]; return k >= AB0 && k < AB1; };
   auto xi = [&](int a, int b, int cc, int d) { return (ORD.pos[a * NB + b] - AB0) * NCD + cc * ND + d; };
   const int lane = threadIdx.x & 31;
-  const int wpb = blockDim.x >> 5;
   const int nchunks = *lq.nchunks;
-  const int stride = gridDim.x * wpb * lq.numprocs;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  for (int c = (blockIdx.x * wpb + (threadIdx.x >> 5)) * lq.numprocs + lq.myid; c < nchunks; c += stride) {
+  // the warp takes the next chunk of this rank's share (every numprocs-th,
+  // starting at myid) from the pass's work queue: chunks are sorted costliest
+  // first, so the launch ends with the cheap ones
+  for (;;) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(lq.queue + PASS, 1);
+    const int c = __shfl_sync(0xffffffffu, t, 0) * lq.numprocs + lq.myid;
+    if (c >= nchunks) break;
     const int4 ch = lq.chunks[c];
     // this chunk's instance: batches read its launch record from global memory
     const MolLaunch& ql = [&]() -> const MolLaunch& {

@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
   constexpr int LT = LA + LB + LC + LD;
   using W = WideLayout<NA, NB, NC, ND>;
   extern __shared__ double smem[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   double* v = smem + (size_t)wid * per_warp;
   double* X = v + vmax;
   int* xs = reinterpret_cast<int*>(X + xmax);
@@ -94,8 +94,11 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
   const int base = LT + 2;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const int nchunks = *lq.nchunks;
-  const int stride = gridDim.x * wpb * lq.numprocs;
-  for (int c = (blockIdx.x * wpb + wid) * lq.numprocs + lq.myid; c < nchunks; c += stride) {
+  for (;;) {   // chunks from the launch's work queue, costliest first
+    int tk = 0;
+    if (lane == 0) tk = atomicAdd(lq.queue, 1);
+    const int c = __shfl_sync(0xffffffffu, tk, 0) * lq.numprocs + lq.myid;
+    if (c >= nchunks) break;
     const int4 ch = lq.chunks[c];
     const MolLaunch& ql = lq.insts ? lq.insts[ch.w] : lq;
     const PairRec* __restrict__ rec = ql.rec;
@@ -213,7 +216,7 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
           __syncwarp();
           for (int l = 0; l < nlev; ++l) {
             const int o1 = levels[l + 1];
-            for (int o = levels[l] + lane; o < o1; o += 32) v[base + o] = eval_op(ops, o, v, geo);
+            run_level(ops, levels[l], o1, v, base, geo, lane, 32, EvalD{});
             __syncwarp();
           }
           for (int i = lane; i < nx; i += 32) {

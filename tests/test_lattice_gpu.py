@@ -101,3 +101,30 @@ def test_rotate_on_the_gpu_matches_oracle():
     ref = oracle.rotate_density(s, pp)
     got = scf.rotate(scf.HostState(s, 'cuda'), torch.tensor(pp, device='cuda')).cpu().numpy()
     assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize('variant', [0, 1])
+@pytest.mark.parametrize('name', ['helix_631g', 'chain_631gss', 'box_sto3g'])
+def test_straight_line_and_interpreter_match_oracle(name, variant):
+    """Both lattice executions against the oracle: the straight-line kernels
+    (one ket per lane, classes up to 64 integrals; variant 0) and the op-table
+    interpreter for every class (variant 1), FP64 and with the far cells in FP32."""
+    s = system.build_system(CASES[name], oracle.onee)
+    pp, ph = _density(s, seed=5)
+    c_ref, x_ref = oracle.fourindex_eri(s, pp, ph)
+    df = fock.DeviceFock(s)
+    df.force_variant(variant)
+    dev = torch.device('cuda')
+    c_d, x_d = df(torch.tensor(pp, device=dev), torch.tensor(ph, device=dev) if ph is not None else None)
+    torch.cuda.synchronize()
+    _close(c_d.cpu().numpy(), c_ref, 'C_C variant %d' % variant)
+    _close(x_d.cpu().numpy(), x_ref, 'X_C variant %d' % variant)
+    df.close()
+    dm = fock.DeviceFock(s, precision=1, mixed_cutoff=1e-6)
+    dm.force_variant(variant)
+    c_m, x_m = dm(torch.tensor(pp, device=dev), torch.tensor(ph, device=dev) if ph is not None else None)
+    torch.cuda.synchronize()
+    scale = np.abs(c_ref).max()
+    assert np.abs(c_m.cpu().numpy() - c_ref).max() <= 1e-6 * scale
+    assert np.abs(x_m.cpu().numpy() - x_ref).max() <= 1e-6 * scale
+    dm.close()
