@@ -16,9 +16,15 @@ One step = one direct J/K build (FOURINDEX_ERI) of all-trans C20H42 in
   bounded sample of bra shells, extrapolated to one full build, one core.
 * scf: time to a converged SCF of the same molecule, the reference's loop with
   full FP64 builds against the time-to-solution path (batch_scf / scf.run_scf_fast).
-* batch (--batch N, default 32; 0 skips it): N uneven water clusters in cc-pVDZ
-  as one batch -- batched Fock builds/s, and the time to converged SCF of the
-  whole set, one plain FP64 GPU SCF per molecule against the batched SCF.
+* batch (--batch N, default 256; 0 skips it): N uneven water clusters in
+  cc-pVDZ as one batch -- batched Fock builds/s (default schedule and after the
+  batch autotuner), and the time to converged SCF of the whole set, one plain
+  FP64 GPU SCF per molecule against the batched SCF (with and without the
+  learned guess and the FP32 recursion).
+* other_configs: C40H82 6-31G** and the helical chain at CUTOFF 5/10 (build
+  rates; the chain also with its far cells in FP32).
+* mixed: the C20H42 build with the FP32 recursion below Schwarz x density
+  1e-6, its max|dF| and dE against the FP64 build.
 * N > 1 (torchrun): every rank computes its share of the quartet chunks and the
   J/K matrices are summed with one NCCL all-reduce -- the reference's
   MPI_ALLREDUCE of J/K; total work is fixed (strong scaling).
@@ -359,9 +365,11 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
     torch.cuda.synchronize(dev)
     ms = sum(a.elapsed_time(b) for a, b in evs) / steps
     ms_tuned, sched = None, fb.schedule()
-    if autotune:
+    if True:
         # the same builds after the batch autotuner picked each class's variant on them
+        t_tune = time.perf_counter()
         fb.autotune(pc)
+        t_tune = time.perf_counter() - t_tune
         for k in range(steps):
             flush.fill_(float(k))
             evs[k][0].record()
@@ -379,9 +387,9 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
            'build_ms': ms, 'builds_per_s': 1000.0 / ms, 'quartets_per_build': cen['quartets'],
            'quartets_per_s': cen['quartets'] / (ms * 1e-3), 'tflops': cen['flops'] / (ms * 1e-3) / 1e12,
            'launches_per_build': int(cen['kernel_launches']),
-           'build_ms_autotuned': ms_tuned,
+           'build_ms_autotuned': ms_tuned, 'autotune_s': t_tune,
            'variants': {x['cls']: x['variant'] for x in sched},
-           'schedule': 'autotuned on the batch' if autotune else 'default table',
+           'schedule': 'build_ms: default table; build_ms_autotuned: after pfe_batch_autotune on the batch',
            'l2': 'flushed before every timed build (256 MiB write)'}
     if not scf_runs:
         return out
@@ -437,7 +445,7 @@ def main():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-scf', action='store_true', help='skip the time-to-converged SCF leg')
-    ap.add_argument('--batch', type=int, default=32,
+    ap.add_argument('--batch', type=int, default=256,
                     help='water clusters in the batched leg (0: skip it)')
     ap.add_argument('--no-batch-scf', action='store_true',
                     help='batched leg: the batched builds only, no SCF of the set')

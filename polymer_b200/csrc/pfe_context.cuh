@@ -211,6 +211,8 @@ struct pfe_batch {
   pfe::ClassLaunch launches[64];    // joined chunk lists; ops/tables of the first instance with the class
   int nlaunch = 0;
   int* d_queue = nullptr;           // the joined launches' work queues (64 counters each)
+  long long* d_off = nullptr;       // off[] on the device (the batched symmetrisation)
+  bool all_contracted = false;      // every instance digests in contracted space
   void* d_insts = nullptr;          // the instances' launch records (MolLaunch) on the device
   void* h_insts = nullptr;          // ... and their pinned host copy, uploaded by every build (so a
                                     // captured graph re-reads it at each replay)

@@ -962,10 +962,13 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
         }
         PFE_CUDA(vv.allow(cl.smem_big, std::min<size_t>(cl.smem_warp, 220 * 1024)));
         if ((rc = size_wide(cl, ctx->kept_max, ctx->lower_kept)) != PFE_OK) return rc;
-        // default schedule (measured on B200): straight-line code where a class has it, else
-        // the wide warp variant where the working set fits, else one primitive quartet per
-        // warp up to 640 integrals, per block beyond
-        cl.variant = cl.has_straight ? 0 : (cl.has_wide ? 3 : ((h->nout <= 640 && cl.smem_warp <= 200 * 1024) ? 1 : 2));
+        // default schedule (measured on B200, C20H42 and the water batch): straight-line code
+        // where a class has it; (dd|dp) on the wide warp variant (3.2 ms against 4.9 ms per
+        // block on C20H42); (dd|dd) per block (1.2 ms against 2.2 ms wide)
+        cl.variant = cl.has_straight ? 0
+                                     : ((cl.has_wide && h->nout <= 4000)
+                                            ? 3
+                                            : ((h->nout <= 640 && cl.smem_warp <= 200 * 1024) ? 1 : 2));
       }
       if (!cl.has_straight && !cl.has_table) {
         set_error("no kernel for a quartet class");
@@ -1005,6 +1008,7 @@ static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   ql.gr_max = ctx->d_gr_max;
   ql.bk_list = ctx->d_bk_list;
   ql.blk = ctx->d_blk;
+  ql.tblk = ctx->d_tblk;
   ql.bmax = ctx->d_bmax;
   ql.nblk = ctx->nblk;
   ql.dtol = ctx->dtol;
@@ -1078,6 +1082,10 @@ static int tune_class(pfe_context* ctx, ClassLaunch& cl, const MolLaunch& ql, cu
   int bestv = cl.variant, bestg = cl.gmul;
   for (int v = 0; v < 4; ++v) {
     if (!variant_ok(cl, v)) continue;
+    // the one-quartet-per-warp/block interpreters lose to the straight-line code by
+    // 5-300x on every class that has it (measured on C20H42 and the water batch):
+    // not timed there, which keeps the autotuner to seconds
+    if ((v == 1 || v == 2) && cl.has_straight) continue;
     static const int kGmul[4] = {4, 8, 16, 32};
     const int ng = v == 0 ? 4 : 1;
     float tv = 1e30f;
@@ -1295,6 +1303,10 @@ int batch_setup(pfe_batch* b) {
       b->launches[b->nlaunch++] = cl;
     }
   PFE_CUDA(b->alloc(&b->d_insts, sizeof(MolLaunch) * b->inst.size()));
+  PFE_CUDA(b->alloc((void**)&b->d_off, sizeof(long long) * b->off.size()));
+  PFE_CUDA(cudaMemcpy(b->d_off, b->off.data(), sizeof(long long) * b->off.size(), cudaMemcpyHostToDevice));
+  b->all_contracted = true;
+  for (pfe_context* c : b->inst) b->all_contracted = b->all_contracted && c->contracted;
   PFE_CUDA(cudaMallocHost(&b->h_insts, sizeof(MolLaunch) * b->inst.size()));
   PFE_CUDA(cudaEventCreateWithFlags(&b->ev_insts, cudaEventDisableTiming));
   b->insts_for = nullptr;
@@ -1340,6 +1352,52 @@ static int batch_decontract(pfe_batch* b, const double* d_pc, cudaStream_t s) {
   return PFE_OK;
 }
 
+// The per-instance work around a batched build as three launches over every
+// instance (blockIdx.y = instance, the threads of its blocks stride over its
+// matrices) instead of seven small ones per instance: zero J'/K', the block
+// maxima and the FP32 counter; the block maxima of |P_T|; after the class
+// kernels, C_C = J' + J'^T and X_C = K' + K'^T at the packed offsets.
+__global__ void k_batch_zero(const MolLaunch* __restrict__ insts) {
+  const MolLaunch& q = insts[blockIdx.y];
+  const long long nt2 = (long long)q.nt * q.nt, nb2 = (long long)q.nblk * q.nblk;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt2; t += (long long)gridDim.x * blockDim.x) {
+    q.jt[t] = 0.0;
+    q.kt[t] = 0.0;
+    if (t < nb2) const_cast<double*>(q.bmax)[t] = 0.0;
+  }
+  for (long long t = nt2 + blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb2;
+       t += (long long)gridDim.x * blockDim.x)
+    const_cast<double*>(q.bmax)[t] = 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *q.n32 = 0ull;
+}
+
+__global__ void k_batch_dmax(const MolLaunch* __restrict__ insts) {
+  const MolLaunch& q = insts[blockIdx.y];
+  const long long nt2 = (long long)q.nt * q.nt;
+  unsigned long long* bm = reinterpret_cast<unsigned long long*>(const_cast<double*>(q.bmax));
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt2; t += (long long)gridDim.x * blockDim.x) {
+    const int b1 = q.tblk[t % q.nt], b2 = q.tblk[t / q.nt];
+    if (b1 < 0 || b2 < 0) continue;
+    const double v = fabs(q.dt[t]);
+    if (v > 0.0) atomicMax(bm + (size_t)b1 * q.nblk + b2, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+__global__ void k_batch_symmetrize(const MolLaunch* __restrict__ insts, const long long* __restrict__ off,
+                                   double* __restrict__ cc, double* __restrict__ xc) {
+  const MolLaunch& q = insts[blockIdx.y];
+  const int n = q.nt;
+  const long long nt2 = (long long)n * n;
+  double* c = cc + off[blockIdx.y];
+  double* x = xc + off[blockIdx.y];
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nt2; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % n), j = (int)(t / n);
+    const long long tt = i * (long long)n + j;   // (j, i)
+    c[t] = q.jt[t] + q.jt[tt];
+    x[t] = q.kt[t] + q.kt[tt];
+  }
+}
+
 // One build of every instance from the packed contracted densities d_pc.
 int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, cudaStream_t s) {
   const size_t n = b->inst.size();
@@ -1365,28 +1423,33 @@ int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, 
     PFE_CUDA(cudaEventRecord(b->ev_insts, s));
     b->ev_pending = true;
   }
-  for (size_t k = 0; k < n; ++k) {
-    pfe_context* c = b->inst[k];
-    // block maxima for every instance: its screening may change between graph replays
-    const int rc = prepare_build(c, c->contracted ? d_pc + b->off[k] : c->d_pt, s, true);
-    if (rc != PFE_OK) return rc;
-  }
+  // zero J'/K' and take the block maxima of every instance (its screening may
+  // change between graph replays), one launch each over the whole batch
+  const MolLaunch* di = static_cast<const MolLaunch*>(b->d_insts);
+  const dim3 gb(8, (unsigned)n);
+  k_batch_zero<<<gb, 256, 0, s>>>(di);
+  k_batch_dmax<<<gb, 256, 0, s>>>(di);
+  PFE_CUDA(cudaGetLastError());
   pfe_context* c0 = b->inst[0];
   MolLaunch lq = make_launch(c0, c0->d_pt);
-  lq.insts = static_cast<const MolLaunch*>(b->d_insts);
+  lq.insts = di;
   for (int i = 0; i < b->nlaunch; ++i) {
     const ClassLaunch& cl = b->launches[i];
     launch_class(c0, cl, lq, cl.variant, s, b->mixed);
     PFE_CUDA(cudaGetLastError());
   }
-  for (size_t k = 0; k < n; ++k) {
-    pfe_context* c = b->inst[k];
-    if (c->contracted) {
-      launch_symmetrize(c->d_jp, d_cc + b->off[k], c->ncgs, 1, s);
-      launch_symmetrize(c->d_kp, d_xc + b->off[k], c->ncgs, 1, s);
-    } else {
-      int rc = contract_outputs(c, c->d_jp, c->d_kp, d_cc + b->off[k], d_xc + b->off[k], true, 1, s);
-      if (rc != PFE_OK) return rc;
+  if (b->all_contracted) {
+    k_batch_symmetrize<<<gb, 256, 0, s>>>(di, b->d_off, d_cc, d_xc);
+  } else {
+    for (size_t k = 0; k < n; ++k) {
+      pfe_context* c = b->inst[k];
+      if (c->contracted) {
+        launch_symmetrize(c->d_jp, d_cc + b->off[k], c->ncgs, 1, s);
+        launch_symmetrize(c->d_kp, d_xc + b->off[k], c->ncgs, 1, s);
+      } else {
+        int rc = contract_outputs(c, c->d_jp, c->d_kp, d_cc + b->off[k], d_xc + b->off[k], true, 1, s);
+        if (rc != PFE_OK) return rc;
+      }
     }
   }
   PFE_CUDA(cudaGetLastError());

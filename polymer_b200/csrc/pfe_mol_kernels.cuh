@@ -61,6 +61,7 @@ struct MolLaunch {
   const double* gr_max;   // group -> largest bound
   const int* bk_list;     // ket groups by (class, bucket, group)
   const int* blk;         // shell -> contracted block
+  const int* tblk;        // target -> contracted block (-1: none)
   const double* bmax;     // block-pair maxima of |P_T| (density screening / mixed precision)
   int nblk;
   double dtol;            // skip quartets with bound * max|P| < dtol (0: the reference's screen only)
