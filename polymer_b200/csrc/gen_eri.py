@@ -167,17 +167,24 @@ class Gen:
 OPS_THRESHOLD = 1600  # classes with more integrals have no straight-line function (op tables only)
 
 
-def gen_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
+def gen_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False, compact=True):
     """Level-scheduled op table of one class for the block-cooperative interpreter.
 
-    Slot 0 holds zero, slots 1..L+1 the Boys values F[m]; every recursion node
-    gets its own slot, ordered by dependency level so that all ops of a level
-    can run in parallel.  Each op is six uint16: (kind<<12 | axis<<10 | cA<<5 |
-    cB, s1, s2, s3, s4, s5) computing
+    Slot 0 holds zero, slots 1..L+1 the Boys values F[m]; the recursion nodes
+    are ordered by dependency level so that all ops of a level can run in
+    parallel.  Each op is seven uint16: (kind<<12 | axis<<10 | cA<<5 | cB, s1,
+    s2, s3, s4, s5, dest) computing into slot dest
       v = G1*s1 + G2*s2 + cA*X*(s3 - Y*s4) + cB*Z*s5
     with (G1, G2, X, Y, Z) = (PA, WP, 1/2z, rho/z, 0) for kind 0 (VRR on A),
     (QC, WQ, 1/2h, rho/h, 1/2(z+h)) for kind 1 (VRR on C), (1, AB, 0, 0, 0)
     for kind 2 (bra HRR) and (1, CD, 0, 0, 0) for kind 3 (ket HRR).
+
+    With `compact` a node's slot is reused once every reader of its value has
+    run: a value last read at level l frees its slot for the writers of levels
+    l+1 and later (the readers of one level run concurrently with its writers,
+    so a slot never changes hands inside a level), and the outputs keep theirs
+    to the end.  That halves the slots of the large classes (the interpreters'
+    shared memory); without it every node has a slot of its own.
     """
     L = LA + LB + LC + LD
     nodes = {}     # key -> (kind, axis, cA, cB, [src keys]) ; leaves are ('F', m)
@@ -261,21 +268,45 @@ def gen_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
     sorted_keys = sorted(order, key=lambda k: level[k])
     slot = {('F', m): 1 + m for m in range(L + 1)}
     base = L + 2
-    for n, k in enumerate(sorted_keys):
-        slot[k] = base + n
+    nlev = (max(level.values()) + 1) if level else 0
+    if compact:
+        last = {k: -1 for k in sorted_keys}   # level of the last reader of each node
+        for k in sorted_keys:
+            for sk in nodes[k][4]:
+                if sk is not None and sk[0] != 'F':
+                    last[sk] = max(last[sk], level[k])
+        for o in outs:
+            if o is not None and o[0] != 'F':
+                last[o] = nlev   # read after the last level
+        free, used, release = [], 0, {}
+        for k in sorted_keys:   # level by level
+            lv = level[k]
+            for r in release.pop(lv, []):
+                free.append(r)
+            if free:
+                sl = free.pop()
+            else:
+                sl = base + used
+                used += 1
+            slot[k] = sl
+            release.setdefault(max(last[k], lv) + 1, []).append(sl)
+        nslots = base + used
+    else:
+        for n, k in enumerate(sorted_keys):
+            slot[k] = base + n
+        nslots = base + len(sorted_keys)
     ops = []
     for k in sorted_keys:
         kind, ax, cA, cB, srcs = nodes[k]
-        ops.append([(kind << 12) | (ax << 10) | (cA << 5) | cB] + [slot[sk] if sk is not None else 0 for sk in srcs])
-    nlev = (max(level.values()) + 1) if level else 0
+        ops.append([(kind << 12) | (ax << 10) | (cA << 5) | cB] + [slot[sk] if sk is not None else 0 for sk in srcs]
+                   + [slot[k]])
     lev_start = [0] * (nlev + 1)
     for k in sorted_keys:
         lev_start[level[k] + 1] += 1
     for i in range(nlev):
         lev_start[i + 1] += lev_start[i]
     out_slots = [slot[o] if o is not None else 0 for o in outs]
-    nslots = base + len(sorted_keys)
-    assert nslots < 65536
+    assert nslots < 32768   # slot indices share 15 bits with other fields in the wide kernel's output list
     return ops, lev_start, out_slots, nslots
 
 
@@ -290,7 +321,7 @@ def emit_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
     ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD, pure_bra, pure_ket)
     name = 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure2' if pure_ket else ('_pure' if pure_bra else ''))
     lines = ['// (%d%d|%d%d): %d ops in %d levels, %d slots' % (LA, LB, LC, LD, len(ops), len(lev) - 1, nslots)]
-    flat = [v for op in ops for v in op] or [0] * 6
+    flat = [v for op in ops for v in op] or [0] * 7
     lines.append('static const unsigned short %s_ops[%d] = {%s};' % (name, len(flat), ','.join(map(str, flat))))
     lines.append('static const int %s_levels[%d] = {%s};' % (name, len(lev), ','.join(map(str, lev))))
     lines.append('static const unsigned short %s_out[%d] = {%s};' % (name, len(outs), ','.join(map(str, outs))))

@@ -152,10 +152,10 @@ int upload_optable(pfe_context* ctx, const OpTableHost* h, OpTableDev* d) {
   PFE_CUDA(cudaMalloc((void**)&ops, sizeof(unsigned short) * 8 * (h->nops + 1)));
   PFE_CUDA(cudaMalloc((void**)&out, sizeof(unsigned short) * (h->nout ? h->nout : 1)));
   PFE_CUDA(cudaMalloc((void**)&lev, sizeof(int) * (h->nlevels + 1)));
-  {  // 16-byte records: the six generated fields and two zero pads
+  {  // 16-byte records: the seven generated fields (header, five sources, destination) and a zero pad
     std::vector<unsigned short> rec((size_t)8 * (h->nops + 1), 0);
     for (int o = 0; o < h->nops; ++o)
-      for (int k = 0; k < 6; ++k) rec[(size_t)8 * o + k] = h->ops[(size_t)6 * o + k];
+      for (int k = 0; k < 7; ++k) rec[(size_t)8 * o + k] = h->ops[(size_t)7 * o + k];
     PFE_CUDA(cudaMemcpy(ops, rec.data(), sizeof(unsigned short) * rec.size(), cudaMemcpyHostToDevice));
   }
   PFE_CUDA(cudaMemcpy(out, h->out, sizeof(unsigned short) * h->nout, cudaMemcpyHostToDevice));

@@ -26,6 +26,7 @@ struct OpTableDev {
   const int* levels_p2;
   const unsigned short* out_p2;
   int nlevels_p2;
+  int nslots_p, nslots_p2;   // slots of the two variants (0 where absent)
 };
 
 // Geometry multipliers of the four op kinds, in shared memory.
@@ -35,8 +36,10 @@ struct OpGeom {
 };
 
 // Value of an op of a table: each op is one 16-byte record of eight uint16,
-// (kind<<12 | axis<<10 | cA<<5 | cB, s1, s2, s3, s4, s5, 0, 0), read with one
-// vector load:  G1*v[s1] + G2*v[s2] + cA*X*(v[s3] - Y*v[s4]) + cB*Z*v[s5].
+// (kind<<12 | axis<<10 | cA<<5 | cB, s1, s2, s3, s4, s5, dest, 0), read with
+// one vector load:  v[dest] = G1*v[s1] + G2*v[s2] + cA*X*(v[s3] - Y*v[s4]) +
+// cB*Z*v[s5] (slots are reused once their value's last reader has run, so the
+// destination is part of the record).
 __device__ __forceinline__ double eval_rec(const uint4 r, const double* v, const OpGeom& geo) {
   const int h = r.x & 0xffff;
   const int kind = h >> 12, ax = (h >> 10) & 3, cA = (h >> 5) & 31, cB = h & 31;
@@ -62,20 +65,23 @@ struct EvalD {
 // records before evaluating any of them (four record loads in flight instead
 // of one load-use chain per op).
 template <typename T, typename Geo, typename Eval>
-__device__ __forceinline__ void run_level(const unsigned short* __restrict__ ops, int o0, int o1, T* v, int base,
-                                          const Geo& geo, int tid, int team, Eval eval) {
+__device__ __forceinline__ void run_level(const unsigned short* __restrict__ ops, int o0, int o1, T* v, const Geo& geo,
+                                          int tid, int team, Eval eval) {
   const uint4* rec = reinterpret_cast<const uint4*>(ops);
   int o = o0 + tid;
   for (; o + 3 * team < o1; o += 4 * team) {
     const uint4 r0 = __ldg(rec + o), r1 = __ldg(rec + o + team), r2 = __ldg(rec + o + 2 * team),
                 r3 = __ldg(rec + o + 3 * team);
     const T a0 = eval(r0, v, geo), a1 = eval(r1, v, geo), a2 = eval(r2, v, geo), a3 = eval(r3, v, geo);
-    v[base + o] = a0;
-    v[base + o + team] = a1;
-    v[base + o + 2 * team] = a2;
-    v[base + o + 3 * team] = a3;
+    v[r0.w & 0xffff] = a0;
+    v[r1.w & 0xffff] = a1;
+    v[r2.w & 0xffff] = a2;
+    v[r3.w & 0xffff] = a3;
   }
-  for (; o < o1; o += team) v[base + o] = eval(__ldg(rec + o), v, geo);
+  for (; o < o1; o += team) {
+    const uint4 r = __ldg(rec + o);
+    v[r.w & 0xffff] = eval(r, v, geo);
+  }
 }
 
 // The same op in FP32 (the mixed-precision lattice path): slots hold F_m/pref
@@ -112,11 +118,10 @@ __device__ __forceinline__ void geom_to_float(const OpGeom& g, OpGeomF& f) {
   f.Z = (float)g.Z;
 }
 
-__device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restrict__ v, const OpGeom& geo,
-                                            int base) {
+__device__ __forceinline__ void run_optable(const OpTableDev& t, double* __restrict__ v, const OpGeom& geo) {
   for (int l = 0; l < t.nlevels; ++l) {
     const int o0 = t.levels[l], o1 = t.levels[l + 1];
-    run_level(t.ops, o0, o1, v, base, geo, (int)threadIdx.x, (int)blockDim.x, EvalD{});
+    run_level(t.ops, o0, o1, v, geo, (int)threadIdx.x, (int)blockDim.x, EvalD{});
     __syncthreads();
   }
 }
@@ -198,7 +203,7 @@ __global__ void __launch_bounds__(256) k_schwarz_big(PairArrays pr, const int* _
       set_geom(geo, PA, Z0, PA, Z0, AB, AB, 0.5 / z, 0.5 / z, 0.25 / z, 0.5, 0.5);
     }
     __syncthreads();
-    run_optable(tab, v, geo, 2 * (LA + LB) + 2);
+    run_optable(tab, v, geo);
     const int I = pr.si[t], J = pr.sj[t];
     double b = 0.0;
     for (int x = threadIdx.x; x < NA * NB; x += blockDim.x) {

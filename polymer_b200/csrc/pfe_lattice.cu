@@ -241,7 +241,6 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
   const LatGeom& g = R.g;
   const int nchunks = *R.nchunks;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  const int base = LT + 2;
   const int h3 = g.c2[0] + g.c1[0];
   const bool helix = R.pph != nullptr;
   for (int c = blockIdx.x * wpb + wid; c < nchunks; c += gridDim.x * wpb) {
@@ -343,13 +342,13 @@ __global__ void __launch_bounds__(256) k_lattice(LatticeRun R, OpTableDev tab, i
           ++n32;
           for (int l = 0; l < tab.nlevels; ++l) {
             const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-            run_level(tab.ops, o0, o1, vf, base, geof, lane, 32, EvalF{});
+            run_level(tab.ops, o0, o1, vf, geof, lane, 32, EvalF{});
             __syncwarp();
           }
         } else {
           for (int l = 0; l < tab.nlevels; ++l) {
             const int o0 = tab.levels[l], o1 = tab.levels[l + 1];
-            run_level(tab.ops, o0, o1, v, base, geo, lane, 32, EvalD{});
+            run_level(tab.ops, o0, o1, v, geo, lane, 32, EvalD{});
             __syncwarp();
           }
         }

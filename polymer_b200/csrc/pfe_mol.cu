@@ -421,7 +421,6 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
   const double* __restrict__ scoef = ql.scoef;   // held in registers (ql may live in global memory)
   const double* __restrict__ boys = ql.boys;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  const int base = LT + 2;
   const int G = ch.x;
   const int g0 = ql.gr_start[G], gn = ql.gr_n[G];
   {
@@ -521,7 +520,7 @@ __device__ __forceinline__ void gq_team(const MolLaunch& ql, const OpTableDev& t
         sync();
         for (int l = 0; l < t_nlevels; ++l) {
           const int o0 = t_levels[l], o1 = t_levels[l + 1];
-          run_level(t_ops, o0, o1, v, base, geo, tid, team, EvalD{});
+          run_level(t_ops, o0, o1, v, geo, tid, team, EvalD{});
           sync();
         }
         const double w = sw[0];
@@ -695,13 +694,17 @@ static int size_wide(ClassLaunch& cl, const int kept_max[3], const bool lower_ke
   auto km = [&](int L) { return std::max(kept_max[L], 1); };
   const int xmax = km(la) * km(lb) * km(lc) * km(ld);
   const size_t pw = sizeof(double) * (size_t)wv.doubles(vmax, xmax);
-  const size_t cap = 227 * 1024;
+  // at most 160 KB of shared memory per SM: the rest of the SM's 256 KB stays
+  // L1, which then holds the op table the warps read their op records from
+  // (61 KB for the pure-bra (dd|dp) table)
+  const size_t cap = 160 * 1024;
   int best = 0, best_w = 0;
   for (int w = 1; w <= 8; ++w) {
     if (w * pw > cap) break;
-    const int resident = w * (int)((228 * 1024) / (w * pw + 1024));
+    const int resident = w * (int)(cap / (w * pw));
     if (resident > best_w) { best_w = resident; best = w; }
   }
+  if (best == 0 && pw <= 227 * 1024) best = 1;   // one warp per block where 160 KB is too little
   if (best == 0) return PFE_OK;   // does not fit: the class keeps its other variants
   cl.wide_vmax = vmax;
   cl.wide_xmax = xmax;
@@ -1034,9 +1037,10 @@ static void launch_class(pfe_context* ctx, const ClassLaunch& cl, MolLaunch ql, 
     return;
   }
   OpTableDev t{cl.ops,   cl.levels,   cl.out,     cl.nlevels,   cl.nout,   cl.nslots,     cl.ops_p,
-               cl.levels_p, cl.out_p, cl.nlevels_p, cl.ops_p2, cl.levels_p2, cl.out_p2, cl.nlevels_p2};
+               cl.levels_p, cl.out_p, cl.nlevels_p, cl.ops_p2, cl.levels_p2, cl.out_p2, cl.nlevels_p2,
+               cl.nslots_p, cl.nslots_p2};
   if (variant == 3 && cl.has_wide) {
-    const int per_sm = std::max(1, (int)((228 * 1024) / (cl.smem_wide + 1024)));   // resident blocks per SM
+    const int per_sm = std::max(1, (int)((160 * 1024) / cl.smem_wide));   // resident blocks per SM
     const int grid = std::min((work + cl.wide_wpb - 1) / cl.wide_wpb, ctx->num_sms * per_sm);
     wide_variant(cl.cb, cl.ck).launch(ql, t, std::max(grid, 1), cl.wide_wpb, cl.wide_per_warp, cl.wide_vmax,
                                       cl.wide_xmax, cl.smem_wide, s);

@@ -91,7 +91,6 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
     geo.Y[2] = geo.Y[3] = 0.0;
   }
   __syncwarp();
-  const int base = LT + 2;
   const double c2pi = 2.0 / sqrt(REF_PI);
   const int nchunks = *lq.nchunks;
   for (;;) {   // chunks from the launch's work queue, costliest first
@@ -145,7 +144,8 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
       const int* __restrict__ levels = two ? tab.levels_p2 : (bra_top ? tab.levels_p : tab.levels);
       const unsigned short* __restrict__ outs = two ? tab.out_p2 : (bra_top ? tab.out_p : tab.out);
       const int nlev = two ? tab.nlevels_p2 : (bra_top ? tab.nlevels_p : tab.nlevels);
-      if (nx > xmax || base + levels[nlev] > vmax) {
+      const int tslots = two ? tab.nslots_p2 : (bra_top ? tab.nslots_p : tab.nslots);
+      if (nx > xmax || tslots > vmax) {
         // the host sized the working set for every table and kept-component count
         // of this molecule; anything else is refused loudly in the result
         if (lane == 0) atomicAdd(ql.jt, __longlong_as_double(0x7ff8000000000000ll));
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
           __syncwarp();
           for (int l = 0; l < nlev; ++l) {
             const int o1 = levels[l + 1];
-            run_level(ops, levels[l], o1, v, base, geo, lane, 32, EvalD{});
+            run_level(ops, levels[l], o1, v, geo, lane, 32, EvalD{});
             __syncwarp();
           }
           for (int i = lane; i < nx; i += 32) {
@@ -279,7 +279,12 @@ void launch_wide(const MolLaunch& ql, const OpTableDev& t, int grid, int wpb, in
 
 template <int LA, int LB, int LC, int LD>
 cudaError_t allow_wide(size_t smem) {
-  return cudaFuncSetAttribute(k_gq_wide<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const cudaError_t e =
+      cudaFuncSetAttribute(k_gq_wide<LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // ask for no more shared memory than the blocks use: the rest of the SM's
+  // 256 KB is L1, where the op table the warps read stays resident
+  return cudaFuncSetAttribute(k_gq_wide<LA, LB, LC, LD>, cudaFuncAttributePreferredSharedMemoryCarveout, 70);
 }
 
 template <int LA, int LB, int LC, int LD>

@@ -38,24 +38,36 @@ def _geometry(rng):
 
 
 def _run(table, L, geo, F):
+    """Evaluate a table level by level as the interpreters do: every op of a
+    level reads the slots as they were when the level began (a level's ops run
+    concurrently), then the level's results are written to their destinations."""
     ops, lev, outs, nslots = table
     G1, G2, X, Y, Z = geo
     v = np.full(nslots, np.nan)
     v[0] = 0.0
     v[1:L + 2] = F
-    base = L + 2
     for lv in range(len(lev) - 1):
+        snap = v.copy()
+        written = set()
         for o in range(lev[lv], lev[lv + 1]):
-            h, s1, s2, s3, s4, s5 = ops[o]
+            h, s1, s2, s3, s4, s5, dest = ops[o]
             kind, ax, cA, cB = h >> 12, (h >> 10) & 3, (h >> 5) & 31, h & 31
             srcs = [s1, s2] + ([s3, s4] if cA else []) + ([s5] if cB else [])
-            assert all(not np.isnan(v[x]) for x in srcs), 'op reads a slot of a later level'
-            val = G1[kind][ax] * v[s1] + G2[kind][ax] * v[s2]
+            assert all(not np.isnan(snap[x]) for x in srcs), 'op reads a slot no earlier level wrote'
+            val = G1[kind][ax] * snap[s1] + G2[kind][ax] * snap[s2]
             if cA:
-                val += cA * X[kind] * (v[s3] - Y[kind] * v[s4])
+                val += cA * X[kind] * (snap[s3] - Y[kind] * snap[s4])
             if cB:
-                val += cB * Z * v[s5]
-            v[base + o] = val
+                val += cB * Z * snap[s5]
+            assert dest > L + 1 and dest not in written, 'two ops of a level write one slot'
+            written.add(dest)
+            v[dest] = val
+        # no op of this level read a slot this level overwrites
+        for o in range(lev[lv], lev[lv + 1]):
+            h, s1, s2, s3, s4, s5, dest = ops[o]
+            cA, cB = (h >> 5) & 31, h & 31
+            srcs = [s1, s2] + ([s3, s4] if cA else []) + ([s5] if cB else [])
+            assert not (set(srcs) & written), 'a slot is read and rewritten within one level'
     return np.array([v[x] for x in outs])
 
 
@@ -187,3 +199,24 @@ def test_table_lookups_match_the_generator():
         assert tuple(int(v) for v in m.groups()[1:]) == cls[cb] + cls[ck], m.group(0)
         got.add((cb, ck))
     assert got == every
+
+
+@pytest.mark.parametrize('cls', CLASSES + [(2, 2, 2, 1)])
+def test_slot_reuse_keeps_every_output(cls):
+    """Slots reused after their value's last reader (compact tables, what the
+    kernels run) give every output bit for bit as tables with one slot per
+    node, in fewer slots."""
+    L = sum(cls)
+    rng = np.random.default_rng(7 + L)
+    geo = _geometry(rng)
+    F = rng.uniform(0.1, 1.0, size=L + 1)
+    for pb, pk in ((False, False), (True, False), (True, True)):
+        if (pb and cls[0] == 0) or (pk and cls[2] == 0):
+            continue
+        loose = gen_eri.gen_optable(*cls, pure_bra=pb, pure_ket=pk, compact=False)
+        tight = gen_eri.gen_optable(*cls, pure_bra=pb, pure_ket=pk)
+        a, b = _run(loose, L, geo, F), _run(tight, L, geo, F)
+        assert np.array_equal(a, b)
+        assert tight[3] <= loose[3]
+        if len(tight[0]) > 1000:   # the large classes: a half to two thirds of the slots
+            assert tight[3] < 0.75 * loose[3]
