@@ -173,8 +173,9 @@ def cpu_baseline(sysm, p_p_np, budget_s: float = 15.0):
         t_s, sampled = sample(stride)
     t_full = t_fixed + max(t_s, 0.0) * n / sampled
     return {'value': 1.0 / t_full, 'unit': 'Fock builds/s', 'cores': 1, 'kind': 'port',
-            'sample': 'oracle FOURINDEX_ERI restatement over bra shells I = 0 mod %d (%d of %d), '
-                      'extrapolated: %.1f s per full build' % (stride, sampled, n, t_full),
+            'sample': 'oracle FOURINDEX_ERI restatement (the reference loop: no permutational symmetry) over bra '
+                      'shells I = 0 mod %d (%d of %d), extrapolated to a full build: %.1f s; one core, as the '
+                      'reference runs a molecule on one busy rank' % (stride, sampled, n, t_full),
             'seconds_per_build': t_full}
 
 
@@ -245,7 +246,10 @@ def run_reference(args):
             'cpu_baseline': {'value': value, 'unit': 'Fock builds/s', 'cores': cores, 'kind': 'port',
                              'sample': 'per step %d bra shells of %d on %d processes (stride %d), extrapolated '
                                        'to one full build (%.1f s); the Fortran reference cannot be compiled here '
-                                       '(no gfortran/mpif90)' % (walls[0][2], n, cores, stride, t_full)},
+                                       '(no gfortran/mpif90). The oracle port splits the bra shells over the '
+                                       'processes, which the reference cannot do for a molecule (one (Q1,Q2) '
+                                       'ticket: one busy MPI rank), so this rate is an upper bound on the '
+                                       "reference's" % (walls[0][2], n, cores, stride, t_full)},
             'e2e': {'value': value, 'unit': 'Fock builds/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line))
     return 0

@@ -48,6 +48,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     # its source or a header is newer than its object
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith('.cuh')]
     headers += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
+                os.path.join(CSRC, 'generated', 'eri_grad_tables.cuh'),
                 os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h'),
                 os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h')]
     newest_header = max(os.path.getmtime(d) for d in headers if os.path.exists(d))

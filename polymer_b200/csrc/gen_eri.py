@@ -317,9 +317,9 @@ def pure_ket_gains(LA, LB, LC, LD):
             len(gen_optable(LA, LB, LC, LD, True, False)[0]))
 
 
-def emit_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False):
+def emit_optable(LA, LB, LC, LD, pure_bra=False, pure_ket=False, name=None):
     ops, lev, outs, nslots = gen_optable(LA, LB, LC, LD, pure_bra, pure_ket)
-    name = 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure2' if pure_ket else ('_pure' if pure_bra else ''))
+    name = name or 'op_%d%d%d%d%s' % (LA, LB, LC, LD, '_pure2' if pure_ket else ('_pure' if pure_bra else ''))
     lines = ['// (%d%d|%d%d): %d ops in %d levels, %d slots' % (LA, LB, LC, LD, len(ops), len(lev) - 1, nslots)]
     flat = [v for op in ops for v in op] or [0] * 7
     lines.append('static const unsigned short %s_ops[%d] = {%s};' % (name, len(flat), ','.join(map(str, flat))))
@@ -434,6 +434,14 @@ struct EriGeom {
 '''
 
 
+GRAD_HEADER = '''// Generated by polymer_b200/csrc/gen_eri.py -- do not edit.
+// Op tables of the derivative integrals: class (LA LB|LC LD) with centre A, C
+// or D raised by one (cumulative), opg_<LA><LB><LC><LD>_<centre>.
+#pragma once
+#include "eri_classes.cuh"
+'''
+
+
 def main():
     out = sys.argv[1]
     lmax = int(sys.argv[2]) if len(sys.argv) > 2 else 2
@@ -485,6 +493,18 @@ def main():
     pieces.append('    default: return 0.0;\n  }\n}\n')
     with open(out, 'w') as fh:
         fh.write('\n'.join(pieces))
+    # gradient tables: every class with one centre raised by one (A, C or D; B by
+    # translational invariance), for the derivative integrals of
+    # FOURINDEX_ERI_GRADIENT; a header of their own, read by the gradient unit only
+    grad = [GRAD_HEADER]
+    for LA, LB in classes:
+        for LC, LD in classes:
+            if (LC, LD) > (LA, LB) or classes.index((LC, LD)) > classes.index((LA, LB)):
+                continue
+            for c, cls in (('a', (LA + 1, LB, LC, LD)), ('c', (LA, LB, LC + 1, LD)), ('d', (LA, LB, LC, LD + 1))):
+                grad.append(emit_optable(*cls, name='opg_%d%d%d%d_%s' % (LA, LB, LC, LD, c)))
+    with open(out.replace('eri_classes.cuh', 'eri_grad_tables.cuh'), 'w') as fh:
+        fh.write('\n'.join(grad) + '\n')
     with open(out.replace('.cuh', '_flops.json'), 'w') as fh:
         json.dump(table, fh, indent=1, sort_keys=True)
 

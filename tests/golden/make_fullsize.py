@@ -44,7 +44,7 @@ def density(sysm, seed):
     n = sysm.basis.ncgs
     a = rng.normal(size=(n, n)) * 0.3
     pc = a + a.T
-    return pc, np.einsum('ai,cab,bj->cij', sysm.basis.cc, pc[None], sysm.basis.cc)
+    return pc, np.einsum('ai,cab,bj->cij', sysm.basis.cc, pc[None], sysm.basis.cc, optimize=True)
 
 
 def projector(n):

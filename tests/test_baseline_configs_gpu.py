@@ -63,7 +63,7 @@ def _mol_density(sysm, seed):
     rng = np.random.default_rng(seed)
     n = sysm.basis.ncgs
     a = rng.normal(size=(n, n)) * 0.3
-    return np.einsum('ai,cab,bj->cij', sysm.basis.cc, (a + a.T)[None], sysm.basis.cc)
+    return np.einsum('ai,cab,bj->cij', sysm.basis.cc, (a + a.T)[None], sysm.basis.cc, optimize=True)
 
 
 def test_c10h22_at_full_size_matches_oracle():
@@ -138,7 +138,7 @@ def test_helical_chain_at_cutoff_5_10_matches_oracle():
             pc[c] = 0.5 * (pc[c] + pc[c].T)
         elif cm < c:
             pc[c] = pc[cm].T
-    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc, optimize=True)
     ph = scf.rotate(scf.HostState(s), torch.tensor(pp)).numpy()
     c_ref, x_ref = oracle_pool.fourindex_eri(s, pp, ph)
     c_gpu, x_gpu = fock.fourindex_eri(s, pp, ph)

@@ -31,7 +31,7 @@ def _random_density(sysm, seed=7):
             if cm < c:
                 pc[c] = pc[cm].T
     cc = sysm.basis.cc
-    return pc, np.einsum('ai,cab,bj->cij', cc, pc, cc)
+    return pc, np.einsum('ai,cab,bj->cij', cc, pc, cc, optimize=True)
 
 
 def _assert_close(got, ref, what):

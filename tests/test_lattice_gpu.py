@@ -28,7 +28,7 @@ def _density(sysm, seed=1):
             pc[c] = 0.5 * (pc[c] + pc[c].T)
         elif cm < c:
             pc[c] = pc[cm].T
-    pp = np.einsum('ai,cab,bj->cij', sysm.basis.cc, pc, sysm.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', sysm.basis.cc, pc, sysm.basis.cc, optimize=True)
     st = scf.HostState(sysm)
     ph = scf.rotate(st, torch.tensor(pp))
     return pp, (ph.numpy() if ph is not None else None)
@@ -84,7 +84,7 @@ def test_molecular_rank_shares_sum_to_the_full_build():
     rng = np.random.default_rng(4)
     n = s.basis.ncgs
     a = rng.normal(size=(n, n))
-    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, (a + a.T)[None], s.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, (a + a.T)[None], s.basis.cc, optimize=True)
     c_full, x_full = fock.fourindex_eri(s, pp)
     parts = [fock.fourindex_eri(s, pp, myid=r, numprocs=2) for r in range(2)]
     _close(parts[0][0] + parts[1][0], c_full, 'sum C_C')
@@ -97,7 +97,7 @@ def test_rotate_on_the_gpu_matches_oracle():
     s = system.build_system(geometry.polyethylene_deck('6-31G', cutoff1=5, cutoff2=10, kpoints=16), oracle.onee)
     rng = np.random.default_rng(9)
     n = s.basis.ncgs
-    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, rng.normal(size=(s.ncell1, n, n)) * 0.1, s.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, rng.normal(size=(s.ncell1, n, n)) * 0.1, s.basis.cc, optimize=True)
     ref = oracle.rotate_density(s, pp)
     got = scf.rotate(scf.HostState(s, 'cuda'), torch.tensor(pp, device='cuda')).cpu().numpy()
     assert np.abs(got - ref).max() <= 1e-13 * np.abs(ref).max()

@@ -14,7 +14,7 @@ def test_molecule_pieces_sum_to_the_whole_build():
     rng = np.random.default_rng(2)
     n = s.basis.ncgs
     a = rng.normal(size=(n, n))
-    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, (a + a.T)[None], s.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, (a + a.T)[None], s.basis.cc, optimize=True)
     c1, x1 = oracle.fourindex_eri(s, pp)
     c2, x2 = oracle_pool.fourindex_eri(s, pp, nproc=2)
     assert np.abs(c1 - c2).max() <= 1e-12 * np.abs(c1).max()
@@ -32,7 +32,7 @@ def test_lattice_tickets_sum_to_the_whole_build():
             pc[c] = 0.5 * (pc[c] + pc[c].T)
         elif cm < c:
             pc[c] = pc[cm].T
-    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc)
+    pp = np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc, optimize=True)
     ph = scf.rotate(scf.HostState(s), torch.tensor(pp)).numpy()
     c1, x1 = oracle.fourindex_eri(s, pp, ph)
     c2, x2 = oracle_pool.fourindex_eri(s, pp, ph, nproc=2)

@@ -23,7 +23,7 @@ def _density(s, seed):
     rng = np.random.default_rng(seed)
     n = s.basis.ncgs
     pc = rng.normal(size=(s.ncell1, n, n)) * 0.1
-    return np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc)
+    return np.einsum('ai,cab,bj->cij', s.basis.cc, pc, s.basis.cc, optimize=True)
 
 
 CASES = [('STO-3G', 1, 2), ('6-31G', 2, 3), ('6-31Gss', 1, 2)]
