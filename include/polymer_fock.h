@@ -211,6 +211,19 @@ int32_t pfe_context_autotune(pfe_context *ctx, const double *d_p_p, const double
  * class that has it; the others keep theirs (diagnostics and tests). */
 int32_t pfe_context_force_variant(pfe_context *ctx, int32_t variant);
 
+/* Replaces the molecular branch of FOURINDEX_ERI_GRADIENT
+ * (src/pfourindexgradient.f90:1-1478), which adds the two-electron part of the
+ * nuclear gradient to FORCEX/Y/Z(NATOM) (module GRADIENT).  Same argument
+ * block as pfe_fourindex_eri (P_P the density; molecules only: a lattice or
+ * helix returns PFE_EUNSUPPORTED) plus PGS_ATOM(npgs) (1-based atom of every
+ * primitive) and natom.  grad_j and grad_k (natom x 3, column-major: the x
+ * derivatives of all atoms, then y, then z) are overwritten with
+ *   grad_j = d/dR [ 1/2 sum (ij|kl) P_ij P_kl ],  grad_k = d/dR [ -1/4 sum (ij|kl) P_ik P_jl ]
+ * at fixed P; the reference's two-electron force is grad_j + HFX * grad_k
+ * (HFX = DOPTN(19)).  Host pointers; synchronous. */
+int32_t pfe_fourindex_eri_gradient(const pfe_args *a, const int32_t *pgs_atom, int32_t natom, double *grad_j,
+                                   double *grad_k);
+
 /* Measured FP64 FMA-pipe throughput of `device` in TFLOP/s (a dependent-chain
  * free DFMA loop over all SMs; diagnostics for the roofline denominator). */
 int32_t pfe_measure_fp64_peak(int32_t device, double *tflops);

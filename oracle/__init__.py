@@ -115,6 +115,12 @@ def _onee(sysm, with_v):
             from_fortran(n, (nc,), b.npgs).copy())
 
 
+def onee_overlap_only(sysm):
+    """(S_P, T_P, zeros) -- a system for the Fock build and energies of J/K only."""
+    s, t, _ = _onee(sysm, with_v=False)
+    return s, t, np.zeros_like(t)
+
+
 def onee_overlap(sysm):
     """(S_P, T_P) only -- what the Fock build needs from the one-electron set-up."""
     s, t, _ = _onee(sysm, with_v=False)

@@ -17,7 +17,7 @@ LIB = os.path.join(OUT, 'libpolymer_fock.so')
 # the largest units first: the pool starts them before the small ones
 SOURCES = ['pfe_mol_big2.cu', 'pfe_mol_big6.cu', 'pfe_mol_big4.cu', 'pfe_mol_big8.cu', 'pfe_mol_big3.cu',
            'pfe_mol_big7.cu', 'pfe_mol_big1.cu', 'pfe_mol_big5.cu', 'pfe_mol.cu', 'pfe_mol_batch.cu',
-           'pfe_mol_mixed.cu', 'pfe_mol_batch_mixed.cu', 'pfe_mol_wide.cu', 'pfe_api.cu', 'pfe_eri.cu', 'pfe_lattice.cu', 'pfe_lattice_sl.cu', 'pfe_onee.cu',
+           'pfe_mol_mixed.cu', 'pfe_mol_batch_mixed.cu', 'pfe_mol_wide.cu', 'pfe_api.cu', 'pfe_eri.cu', 'pfe_lattice.cu', 'pfe_lattice_sl.cu', 'pfe_grad.cu', 'pfe_onee.cu',
            'pfe_mlp.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
@@ -35,8 +35,9 @@ def _run(cmd):
 def generate():
     gen = os.path.join(CSRC, 'gen_eri.py')
     out = os.path.join(CSRC, 'generated', 'eri_classes.cuh')
+    grad = os.path.join(CSRC, 'generated', 'eri_grad_tables.cuh')   # made at build time, not committed
     os.makedirs(os.path.dirname(out), exist_ok=True)
-    if (not os.path.exists(out)) or os.path.getmtime(out) < os.path.getmtime(gen):
+    if any((not os.path.exists(f)) or os.path.getmtime(f) < os.path.getmtime(gen) for f in (out, grad)):
         _run([sys.executable, gen, out, '2'])
 
 

@@ -100,6 +100,8 @@ def lib(path: str = LIB_PATH):
     L = ctypes.CDLL(path)
     L.pfe_fourindex_eri.argtypes = [ctypes.POINTER(PfeArgs), _dp, _dp]
     L.pfe_fourindex_eri.restype = ctypes.c_int32
+    L.pfe_fourindex_eri_gradient.argtypes = [ctypes.POINTER(PfeArgs), _ip, ctypes.c_int32, _dp, _dp]
+    L.pfe_fourindex_eri_gradient.restype = ctypes.c_int32
     L.pfe_last_error.argtypes = [ctypes.c_char_p, ctypes.c_int32]
     L.pfe_last_error.restype = ctypes.c_int32
     L.pfe_context_create.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
@@ -194,7 +196,8 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_version', 'pfe_overlap_kinetic_noalloc', 'pfe_context_fock_pc',
            'pfe_context_primitive_targets', 'pfe_context_set_screening', 'pfe_batch_create', 'pfe_batch_setup',
            'pfe_batch_set_screening', 'pfe_batch_set_instance_screening', 'pfe_batch_offsets', 'pfe_batch_refresh',
-           'pfe_batch_autotune', 'pfe_batch_schedule', 'pfe_batch_fock_pc', 'pfe_batch_census', 'pfe_batch_destroy']
+           'pfe_batch_autotune', 'pfe_batch_schedule', 'pfe_batch_fock_pc', 'pfe_batch_census', 'pfe_batch_destroy',
+           'pfe_fourindex_eri_gradient']
 
 # Exported symbols declared in include/polymer_guess.h (checked by the CPU tests).
 GUESS_EXPORTS = ['pfe_mlp_gemm', 'pfe_mlp_bias_act', 'pfe_mlp_act_grad', 'pfe_mlp_colsum', 'pfe_mlp_mse',

@@ -851,4 +851,70 @@ int32_t pfe_fourindex_eri(const pfe_args* a, double* c_c, double* x_c) {
   return PFE_OK;
 }
 
+int32_t pfe_fourindex_eri_gradient(const pfe_args* a, const int32_t* pgs_atom, int32_t natom, double* grad_j,
+                                   double* grad_k) {
+  std::lock_guard<std::mutex> lock(g_default_mu);
+  if (!grad_j || !grad_k || !pgs_atom || natom <= 0) { set_error("invalid gradient arguments"); return PFE_EINVAL; }
+  int dev = 0;
+  PFE_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_error("device index out of range"); return PFE_EINVAL; }
+  if (!g_default[dev]) {
+    int rc = pfe_context_create(dev, &g_default[dev]);
+    if (rc != PFE_OK) return rc;
+  }
+  pfe_context* ctx = g_default[dev];
+  HostShells hs;
+  int rc = build_host_shells(a, &hs);
+  if (rc != PFE_OK) return rc;
+  if (!a->p_p) { set_error("P_P is null"); return PFE_EINVAL; }
+  const bool molecule = a->cel1[0] == 0 && a->cel1[1] == 0 && a->cel1[2] == 0 && a->cel2[0] == 0 &&
+                        a->cel2[1] == 0 && a->cel2[2] == 0 && a->helix == 0.0;
+  if (!molecule) {
+    set_error("the two-electron gradient is implemented for molecules (no lattice, no helix)");
+    return PFE_EUNSUPPORTED;
+  }
+  std::vector<int> satom(a->npshell);
+  for (int sh = 0; sh < a->npshell; ++sh) {
+    const int at = pgs_atom[hs.head[sh]] - 1;
+    if (at < 0 || at >= natom) { set_error("PGS_ATOM outside 1..natom"); return PFE_EINVAL; }
+    satom[sh] = at;
+  }
+  const size_t npp = (size_t)a->npgs * a->npgs;
+  if ((rc = check_density(a->p_p, npp)) != PFE_OK) return rc;
+  const uint64_t key = static_key(a, hs);
+  if (!(ctx->ready && ctx->key == key)) {
+    if ((rc = setup_impl(ctx, a, hs, key)) != PFE_OK) { ctx->ready = false; return rc; }
+  }
+  cudaStream_t s = ctx->stream;
+  if (ctx->pp_bytes < npp * sizeof(double)) {
+    ctx->free_now(ctx->d_pp);
+    PFE_CUDA(ctx->alloc((void**)&ctx->d_pp, npp * sizeof(double)));
+    ctx->pp_bytes = npp * sizeof(double);
+  }
+  PFE_CUDA(cudaMemcpyAsync(ctx->d_pp, a->p_p, npp * sizeof(double), cudaMemcpyHostToDevice, s));
+  int* d_satom = nullptr;
+  double* d_g = nullptr;
+  PFE_CUDA(ctx->alloc((void**)&d_satom, sizeof(int) * a->npshell));
+  PFE_CUDA(ctx->alloc((void**)&d_g, sizeof(double) * 6 * (size_t)natom));
+  PFE_CUDA(cudaMemcpyAsync(d_satom, satom.data(), sizeof(int) * a->npshell, cudaMemcpyHostToDevice, s));
+  rc = molecular_gradient_pp(ctx, ctx->d_pp, d_satom, natom, d_g, d_g + 3 * (size_t)natom, s);
+  bool ok = true;
+  if (rc == PFE_OK) rc = molecular_density_ok(ctx, s, &ok);
+  if (rc == PFE_OK && !ok) {
+    set_error("pfe_fourindex_eri_gradient: P_P is not CC^T P_C CC (the gradient reads contracted targets)");
+    rc = PFE_EINVAL;
+  }
+  if (rc == PFE_OK) {
+    PFE_CUDA(cudaMemcpyAsync(grad_j, d_g, sizeof(double) * 3 * (size_t)natom, cudaMemcpyDeviceToHost, s));
+    PFE_CUDA(cudaMemcpyAsync(grad_k, d_g + 3 * (size_t)natom, sizeof(double) * 3 * (size_t)natom,
+                             cudaMemcpyDeviceToHost, s));
+    PFE_CUDA(cudaStreamSynchronize(s));
+  }
+  PFE_CUDA(cudaStreamSynchronize(s));
+  ctx->free_now(d_satom);
+  ctx->free_now(d_g);
+  return rc;
+}
+
+
 }  // extern "C"

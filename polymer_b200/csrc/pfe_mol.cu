@@ -1211,6 +1211,20 @@ int molecular_fock_pc(pfe_context* ctx, const double* d_pc, double* d_cc, double
   return run_build(ctx, ctx->d_pt, d_cc, d_xc, s);
 }
 
+MolLaunch molecular_launch(pfe_context* ctx, const double* d_dt) { return make_launch(ctx, d_dt); }
+
+int molecular_gradient(pfe_context* ctx, const double* d_dt, const int* d_satom, int natom, double* d_gj,
+                       double* d_gk, cudaStream_t s);
+
+// The two-electron gradient (pfe_grad.cu) for P_P: read as the target-space density as the
+// Fock build does (molecules only).
+int molecular_gradient_pp(pfe_context* ctx, const double* d_pp, const int* d_satom, int natom, double* d_gj,
+                          double* d_gk, cudaStream_t s) {
+  const double* d_dt = target_density(ctx, d_pp, s);
+  PFE_CUDA(cudaGetLastError());
+  return molecular_gradient(ctx, d_dt, d_satom, natom, d_gj, d_gk, s);
+}
+
 // Whether the last build's P_P was the decontraction of a contracted density
 // (always true for primitive targets).  Synchronises the stream.
 int molecular_density_ok(pfe_context* ctx, cudaStream_t s, bool* ok) {

@@ -76,6 +76,9 @@ struct MolLaunch {
   const MolLaunch* insts;   // batches: the launch record of every instance (chunk .w), else null
 };
 
+// The launch record of a set-up molecular context for target-space density d_dt.
+MolLaunch molecular_launch(pfe_context* ctx, const double* d_dt);
+
 // max|P_T| over the six density blocks a group quartet's digestion reads
 __device__ __forceinline__ double quartet_pmax(const MolLaunch& ql, int I, int J, int K, int L) {
   const int bI = ql.blk[I], bJ = ql.blk[J], bK = ql.blk[K], bL = ql.blk[L], nb = ql.nblk;

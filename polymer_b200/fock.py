@@ -78,6 +78,20 @@ def fourindex_eri(sysm: System, p_p: np.ndarray, p_p_helix: Optional[np.ndarray]
     return from_fortran(c, (nc,), n).copy(), from_fortran(x, (nc,), n).copy()
 
 
+def fourindex_eri_gradient(sysm: System, p_p: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """The two-electron nuclear gradient for the density P_P (molecules) through
+    the C ABI: (grad_J, grad_K), each (natom, 3), the derivatives of
+    1/2 sum (ij|kl) P_ij P_kl and of -1/4 sum (ij|kl) P_ik P_jl at fixed P."""
+    L = lib()
+    a, keep = sysm.pfe_args(p_p, None)
+    natom = sysm.deck.natom
+    atom = np.ascontiguousarray(sysm.basis.pgs_atom.astype(np.int32))
+    gj = np.zeros(3 * natom)
+    gk = np.zeros(3 * natom)
+    check(L, L.pfe_fourindex_eri_gradient(ctypes.byref(a), capi.iptr(atom), natom, capi.dptr(gj), capi.dptr(gk)))
+    return gj.reshape(3, natom).T.copy(), gk.reshape(3, natom).T.copy()
+
+
 class DeviceFock:
     """A pfe_context bound to one System; callable as the SCF's FockBuilder."""
 
