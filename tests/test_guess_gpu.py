@@ -1,6 +1,7 @@
 """The learned initial guess (polymer_b200/guess.py, network in
-polymer_b200/data/guess_water_ccpvdz.pt, trained on clusters of 2-6 waters) on
-held-out water clusters of 8 waters: against the reference's nuclear-charge
+polymer_b200/data/guess_water_ccpvdz.pt, trained on 768 clusters of 1-16
+waters converged by the batched GPU SCF) on held-out water clusters of 8
+waters: against the reference's nuclear-charge
 guess it must start the SCF much closer to self-consistency (first commutator
 error below a fifth), need no more iterations, trigger no fallback, and reach
 the same energy (1e-8 Eh).
