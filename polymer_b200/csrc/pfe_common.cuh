@@ -107,4 +107,48 @@ __device__ __forceinline__ void boys_tab(double T, double pref, const double* __
   boys_eval<L>(T, pref, gv, F);
 }
 
+// The part of IGAMMA a Boys evaluation of orders 0..L can read -- rows 0..20*TF(L)
+// (the Taylor branch is taken below TF(L)), BoysRow<L>::N columns -- staged in
+// shared memory by a kernel, so that the per-lane row gathers of the quartet
+// loops hit shared memory instead of L1.  `use`: it fits next to the other
+// blocks of an SM (at most 96 KB).
+constexpr int kTF[22] = {33, 37, 41, 43, 46, 49, 51, 54, 56, 58, 61, 63, 66, 68, 70, 72, 74, 76, 78, 80, 82, 84};
+
+template <int L>
+struct BoysSmem {
+  static constexpr int ROWS = 20 * kTF[L] + 1;
+  static constexpr int COLS = BoysRow<L>::N;
+  static constexpr size_t BYTES = sizeof(double) * (size_t)ROWS * COLS;
+  static constexpr bool use = BYTES <= 96 * 1024;
+};
+
+// Copy the rows and columns of BoysSmem<L> from the row-major table (all threads of the block).
+template <int L>
+__device__ __forceinline__ void boys_stage(const double* __restrict__ tab, double* __restrict__ s) {
+  using B = BoysSmem<L>;
+  for (int i = threadIdx.x; i < B::ROWS * B::COLS / 2; i += blockDim.x) {
+    const int r = i / (B::COLS / 2), c = i % (B::COLS / 2);
+    reinterpret_cast<double2*>(s)[i] = __ldg(reinterpret_cast<const double2*>(tab + (size_t)r * NIG_M) + c);
+  }
+}
+
+// boys_tab with the row read from the staged copy.
+template <int L>
+__device__ __forceinline__ void boys_tab_smem(double T, double pref, const double* __restrict__ s,
+                                              double* __restrict__ F) {
+  using B = BoysSmem<L>;
+  double gv[B::COLS];
+  if (T < c_TF[L]) {
+    const int ts = (int)floor(T * 20.0 + 0.5);   // <= 20*TF(L) = ROWS-1
+    const double2* r2 = reinterpret_cast<const double2*>(s + (size_t)ts * B::COLS);
+#pragma unroll
+    for (int k = 0; k < B::COLS / 2; ++k) {
+      const double2 v = r2[k];
+      gv[2 * k] = v.x;
+      gv[2 * k + 1] = v.y;
+    }
+  }
+  boys_eval<L>(T, pref, gv, F);
+}
+
 }  // namespace pfe

@@ -224,6 +224,14 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   const int lane = threadIdx.x & 31;
   const int nchunks = *lq.nchunks;
   const double c2pi = 2.0 / sqrt(REF_PI);
+  // classes of total angular momentum up to 4 read their Boys rows from a copy
+  // of the table's first rows in shared memory (the launch passes its size)
+  constexpr bool SBOYS = BoysSmem<LT>::use;
+  extern __shared__ double s_boys[];
+  if constexpr (SBOYS) {
+    boys_stage<LT>(lq.boys, s_boys);
+    __syncthreads();
+  }
   // the warp takes the next chunk of this rank's share (every numprocs-th,
   // starting at myid) from the pass's work queue: chunks are sorted costliest
   // first, so the launch ends with the cheap ones
@@ -323,7 +331,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
         if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < mcut);
         n32 += f32 ? 1u : 0u;
         double F[LT + 1];
-        boys_tab<LT>(T, f32 ? 1.0 : pref, boys, F);
+        if constexpr (SBOYS) boys_tab_smem<LT>(T, f32 ? 1.0 : pref, s_boys, F);
+        else boys_tab<LT>(T, f32 ? 1.0 : pref, boys, F);
         double out[NI];
         if constexpr (LT == 0) {
           out[0] = F[0];
@@ -472,7 +481,24 @@ using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 struct Passes {
   static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
-    k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED, BATCH><<<grid, 128, 0, s>>>(ql);
+    constexpr int LT = LA + LB + LC + LD;
+    auto kern = k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED, BATCH>;
+    if constexpr (BoysSmem<LT>::use) {
+      // the staged Boys rows: allow them once, and launch no more blocks than can be
+      // resident (each block copies the rows once; the work queue spreads the chunks)
+      static int resident = 0;
+      if (resident == 0) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BoysSmem<LT>::BYTES);
+        int per_sm = 0, dev = 0, nsm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, BoysSmem<LT>::BYTES);
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        resident = std::max(1, per_sm) * std::max(1, nsm);
+      }
+      kern<<<std::min(grid, resident), 128, BoysSmem<LT>::BYTES, s>>>(ql);
+    } else {
+      kern<<<grid, 128, 0, s>>>(ql);
+    }
     if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1, MIXED, BATCH>::run(ql, grid, s);
   }
 };
