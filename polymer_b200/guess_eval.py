@@ -22,6 +22,7 @@ Run: python -m polymer_b200.guess_eval [n_train] [n_heldout] [out.pt] [out.json]
 from __future__ import annotations
 
 import json
+import os
 import sys
 import time
 
@@ -29,6 +30,8 @@ import numpy as np
 import torch
 
 KMIN, KMAX = 8, 32
+# the network trained by train(600, ...) on this configuration
+MODEL = os.path.join(os.path.dirname(__file__), 'data', 'guess_water_k8_32.pt')
 
 
 def cluster_sizes(seeds, kmin: int = KMIN, kmax: int = KMAX):

@@ -58,3 +58,31 @@ def test_guess_is_rotation_covariant(learned):
         e.append(scf.energy(st2, pt, c, x, 1.0, sysm.e_nuc, 0.0, None, 0.0, sysm.deck.nelectrons)[0])
         df.close()
     assert abs(e[0] - e[1]) < 1e-3
+
+
+def test_learned_guess_saves_wall_time_on_large_clusters():
+    """(H2O)k with k >= 16 from the held-out seeds of the large-cluster
+    experiment (polymer_b200/guess_eval.py): the batched SCF from the learned
+    guess (data/guess_water_k8_32.pt; its features, network, assembly and
+    purification inside the timed region) needs fewer iterations and less wall
+    time than from the nuclear-charge guess, with the same energies."""
+    import time
+    from polymer_b200 import batch_scf, guess_eval
+    seeds = [sd for sd in guess_eval.heldout_seeds(200) if guess_eval.cluster_sizes([sd])[0] >= 16][:8]
+    sizes = guess_eval.cluster_sizes(seeds)
+    systems = [system.build_system(guess.sample_cluster(k, sd), fock.onee) for k, sd in zip(sizes, seeds)]
+    lg = guess.LearnedGuess.load(guess_eval.MODEL)
+    res, wall = {}, {}
+    for name, opts in (('nuclear', batch_scf.BatchOptions()), ('learned', batch_scf.BatchOptions(guess=lg))):
+        batch_scf.run_batch_scf(systems, opts, device=0, graph=True)   # untimed: pools, lazy kernels
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res[name] = batch_scf.run_batch_scf(systems, opts, device=0, graph=True)
+        torch.cuda.synchronize()
+        wall[name] = time.perf_counter() - t0
+    print('k >= 16 batch: nuclear %.2f s (%.1f iterations), learned %.2f s (%.1f iterations)' % (
+        wall['nuclear'], res['nuclear'].iterations.mean(), wall['learned'], res['learned'].iterations.mean()))
+    assert res['learned'].converged.all() and not res['learned'].fallback.any()
+    assert res['learned'].iterations.mean() < res['nuclear'].iterations.mean()
+    assert wall['learned'] < wall['nuclear']
+    assert np.abs(res['learned'].energy - res['nuclear'].energy).max() < 1e-8
