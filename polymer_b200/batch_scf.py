@@ -35,6 +35,7 @@ import torch
 from torch.cuda import nvtx
 
 from . import fock as fock_mod
+from . import scf_ops
 from .scf import SCFError, guess_density, incremental_tol
 from .system import System
 
@@ -78,10 +79,6 @@ class BatchResult:
     p_c: List[torch.Tensor]     # converged contracted densities, input order
     sp2_steps: int              # SP2 products over the run (per group, summed)
     phases: Optional[dict] = None   # seconds per phase when profiled (see run_batch_scf)
-
-
-def _trace(x: torch.Tensor) -> torch.Tensor:
-    return x.diagonal(dim1=-2, dim2=-1).sum(-1)
 
 
 class _Group:
@@ -134,82 +131,38 @@ class _Group:
 
 
 def sp2_projector(f: torch.Tensor, nocc: int, pad: torch.Tensor, tol: float = 1e-12, max_steps: int = 200,
-                  first_check: int = 12, fixed_steps: Optional[int] = None):
+                  first_check: int = 12, fixed_steps: Optional[int] = None, ops=None):
     """Projector on the `nocc` lowest eigenvectors of each symmetric f [B, n, n]
     (slots marked in `pad` [B, n] are decoupled and left empty), by SP2.
 
     Gershgorin bounds [lo, hi] of the spectrum map f to X0 = (hi - f)/(hi - lo)
     with eigenvalues in [0, 1], occupied ones nearest 1; each step replaces X by
     X^2 or 2X - X^2, whichever brings tr X^2 closer to nocc.  Adaptive mode runs
-    until the idempotency defect tr(X - X^2) is below `tol` for every matrix
-    (checked after `first_check` steps, then every other step); with
-    `fixed_steps` it runs exactly that many steps and reads nothing back (the
-    form a CUDA graph can hold).  Returns (X, steps, defect per matrix)."""
-    B, n, _ = f.shape
-    d = f.diagonal(dim1=-2, dim2=-1)
-    r = f.abs().sum(-1) - d.abs()
-    big = torch.finfo(F64).max
-    lo = torch.where(pad, torch.full_like(d, big), d - r).amin(-1)
-    hi = torch.where(pad, torch.full_like(d, -big), d + r).amax(-1)
-    hi = torch.maximum(hi, lo + 1e-8)
-    eye = torch.eye(n, dtype=F64, device=f.device)
-    x = (hi[:, None, None] * eye - f) / (hi - lo)[:, None, None]
-    # padded slots: X0 = 0 there, a fixed point of both maps
-    x = torch.where(pad[:, :, None] | pad[:, None, :], torch.zeros_like(x), x)
+    until the idempotency defect tr(X - X^2) before a step is below `tol` for
+    every matrix (checked after `first_check` steps, then every other step);
+    with `fixed_steps` it runs exactly that many steps and reads nothing back
+    (the form a CUDA graph can hold).  `ops`: scf_ops implementation (default:
+    the one for f's device).  Returns (X, steps, defect per matrix)."""
+    ops = ops or scf_ops.ops_for(f.device)
+    x = ops.sp2_init(f, pad)
     steps = 0
     while True:
         x2 = torch.bmm(x, x)
-        t1, t2 = _trace(x), _trace(x2)
+        defect = ops.sp2_step(x, x2, nocc)
         steps += 1
-        defect = (t1 - t2).abs()
-        if fixed_steps is None and steps >= first_check and steps % 2 == 0:
-            if float(defect.max()) < tol:
+        if fixed_steps is not None:
+            if steps >= fixed_steps:
                 return x, steps, defect
-        if fixed_steps is None and steps >= max_steps:
-            raise SCFError('SP2 projection did not converge')
-        up = (t2 - nocc).abs() < (2.0 * t1 - t2 - nocc).abs()
-        x = torch.where(up[:, None, None], x2, 2.0 * x - x2)
-        if fixed_steps is not None and steps >= fixed_steps:
+            continue
+        if steps >= first_check and steps % 2 == 0 and float(defect.max()) < tol:
             return x, steps, defect
+        if steps >= max_steps:
+            raise SCFError('SP2 projection did not converge')
 
 
-def _spd_solve(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
-    """Solve a x = b for a batch of small symmetric positive definite a [B, m, m]
-    (Cholesky, unrolled over m in tensor operations: no host synchronisation,
-    no solver workspace -- usable inside a CUDA graph)."""
-    m = a.shape[-1]
-    L = torch.zeros_like(a)
-    for j in range(m):
-        s = a[:, j, j] - (L[:, j, :j] ** 2).sum(-1)
-        ljj = torch.sqrt(s.clamp_min(1e-300))
-        L[:, j, j] = ljj
-        if j + 1 < m:
-            L[:, j + 1:, j] = (a[:, j + 1:, j] - (L[:, j + 1:, :j] * L[:, j:j + 1, :j]).sum(-1)) / ljj[:, None]
-    y = torch.zeros_like(b)
-    for j in range(m):
-        y[:, j] = (b[:, j] - (L[:, j, :j] * y[:, :j]).sum(-1)) / L[:, j, j]
-    x = torch.zeros_like(b)
-    for j in reversed(range(m)):
-        x[:, j] = (y[:, j] - (L[:, j + 1:, j] * x[:, j + 1:]).sum(-1)) / L[:, j, j]
-    return x
-
-
-def _diis(hist_e: torch.Tensor, valid: torch.Tensor, slot: torch.Tensor) -> torch.Tensor:
-    """Pulay coefficients per molecule over the valid history slots [B, D]:
-    c = G^-1 1 / (1^T G^-1 1) with G the (scaled, slightly regularised) Gram
-    matrix of the commutators; the newest slot alone when that fails."""
-    B, D = valid.shape
-    e = hist_e.view(B, D, -1)
-    g = torch.bmm(e, e.transpose(1, 2))
-    vm = valid.to(F64)
-    scale = (g.diagonal(dim1=-2, dim2=-1) * vm).amax(-1).clamp_min(1e-300)
-    g = g / scale[:, None, None]
-    a = g * vm[:, :, None] * vm[:, None, :] + torch.diag_embed(1.0 - vm + vm * 1e-12)
-    y = _spd_solve(a, vm)
-    c = y / y.sum(-1, keepdim=True)
-    ok = torch.isfinite(c).all(-1)
-    newest = torch.nn.functional.one_hot(slot.expand(B), D).to(F64)
-    return torch.where(ok[:, None], c, newest)
+def pulay_coefficients(hist_e: torch.Tensor, valid: torch.Tensor, slot: torch.Tensor) -> torch.Tensor:
+    """Pulay coefficients of the valid history slots (scf_ops.pulay_coefficients)."""
+    return scf_ops.pulay_coefficients(hist_e, valid, slot)
 
 
 def _check_system(sysm: System) -> None:
@@ -230,14 +183,14 @@ def sorted_order(systems: Sequence[System]) -> List[int]:
     return sorted(range(len(systems)), key=lambda k: _key(systems[k]))
 
 
-def _projector_density(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions, fixed: Optional[int] = None):
-    """P_C = 2 W D W^T with D the SP2 projector of f_ortho; adaptive steps unless `fixed`."""
+def _projector(g: _Group, f_ortho: torch.Tensor, opts: BatchOptions, ops, fixed: Optional[int] = None):
+    """W D W^T with D the SP2 projector of f_ortho (P_C is twice it); adaptive steps unless `fixed`."""
     d, steps, defect = sp2_projector(f_ortho, g.nocc, g.pad, opts.sp2_tol, opts.sp2_max,
-                                     first_check=max(8, g.sp2_last - 2), fixed_steps=fixed)
+                                     first_check=max(8, g.sp2_last - 2), fixed_steps=fixed, ops=ops)
     if fixed is None:
         g.sp2_last = steps
         g.sp2_seen = max(g.sp2_seen, steps)
-    return 2.0 * g.w @ d @ g.w.transpose(1, 2), steps, defect
+    return torch.bmm(torch.bmm(g.w, d), g.w.transpose(1, 2)), steps, defect
 
 
 def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None, device=0,
@@ -283,6 +236,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         g.sp2_fixed = None
         groups.append(g)
         k = k1
+    ops = scf_ops.ops_for(dev)
     conv = np.array([s.deck.scfconv if scfconv is None else scfconv for s in ssys])
     ncycles = max_cycles or max(s.deck.scfcycles for s in ssys)
     total = fb.off[-1]
@@ -318,8 +272,8 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             fb.view(p, kk).copy_(nuclear(kk))
     elif opts.guess == 'core':
         for g in groups:
-            pv, st, _ = _projector_density(g, g.w.transpose(1, 2) @ g.h @ g.w, opts)
-            g.view(p).copy_(pv)
+            q, st, _ = _projector(g, g.w.transpose(1, 2) @ g.h @ g.w, opts, ops)
+            g.view(p).copy_(2.0 * q)
             sp2_steps[0] += st
     elif learned:
         # occupied natural orbitals of the predicted density: the projector on the
@@ -329,8 +283,8 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
             fb.view(p, kk).copy_(torch.tensor(np.asarray(raws[kk]), **f64))
         for g in groups:
             dm = 0.5 * g.ws @ g.view(p) @ g.ws.transpose(1, 2)
-            pv, st, _ = _projector_density(g, -0.5 * (dm + dm.transpose(1, 2)), opts)
-            g.view(p).copy_(pv)
+            q, st, _ = _projector(g, -0.5 * (dm + dm.transpose(1, 2)), opts, ops)
+            g.view(p).copy_(2.0 * q)
             sp2_steps[0] += st
     else:
         raise SCFError('unknown guess %r' % (opts.guess,))
@@ -346,6 +300,7 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         g.hist_f = torch.zeros((g.B, D, g.n, g.n), **f64)
         g.hist_e = torch.zeros((g.B, D, g.n, g.n), **f64)
         g.valid = torch.zeros((g.B, D), dtype=torch.bool, device=dev)
+        ops.prepare(g)
     # device-side inputs of an iteration (fixed addresses: a captured graph reads them)
     take_t = torch.zeros(nmol, dtype=torch.bool, device=dev)
     restart_t = torch.zeros(nmol, dtype=torch.bool, device=dev)
@@ -358,13 +313,8 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         """The device part of one iteration (no host synchronisation when `fixed`)."""
         for g in groups:
             sl = g.sl
-            pv = g.view(p)
-            upd = torch.where(take_t[sl][:, None, None], g.view(p_new), pv)
-            if p_nuc is not None:
-                upd = torch.where(restart_t[sl][:, None, None], g.view(p_nuc), upd)
-                g.valid &= ~restart_t[sl][:, None]
-            pv.copy_(upd)
-            g.view(dp).copy_((pv - g.view(p_ref) * incr_t[sl][:, None, None]) * live_t[sl][:, None, None])
+            ops.next_density(g, g.view(p), g.view(p_new), g.view(p_nuc) if p_nuc is not None else None, take_t[sl],
+                             restart_t[sl], incr_t[sl], live_t[sl], g.view(p_ref), g.view(dp))
         mark('host')
         nvtx.range_push('batched Fock build')
         fb.run_packed(dp, dc, dx)
@@ -373,30 +323,18 @@ def run_batch_scf(systems: Sequence[System], opts: Optional[BatchOptions] = None
         nvtx.range_push('Fock assembly, DIIS, SP2 projector')
         for g in groups:
             sl = g.sl
-            im = incr_t[sl][:, None, None]
-            cv = g.view(dc) + g.view(c_ref) * im
-            xv = g.view(dx) + g.view(x_ref) * im
-            g.view(c_ref).copy_(cv)
-            g.view(x_ref).copy_(xv)
             pv = g.view(p)
-            g.view(p_ref).copy_(pv)
-            f = g.h + cv - 0.5 * g.hfx * xv
-            f = 0.5 * (f + f.transpose(1, 2))
-            fo = g.w.transpose(1, 2) @ f @ g.w
-            po = g.ws @ pv @ g.ws.transpose(1, 2)
-            err = fo @ po - po @ fo
-            e = (pv * (g.h + 0.5 * cv - 0.25 * g.hfx * xv)).sum((1, 2)) + g.e_nuc
-            fe = err.abs().amax((1, 2))
-            g.hist_f.index_copy_(1, slot_t, fo.unsqueeze(1))
-            g.hist_e.index_copy_(1, slot_t, err.unsqueeze(1))
-            g.valid.index_fill_(1, slot_t, True)
-            c = _diis(g.hist_e, g.valid, slot_t)
-            fx = torch.einsum('bd,bdij->bij', c, g.hist_f)
-            pn, st, defect = _projector_density(g, fx, opts, g.sp2_fixed if fixed else None)
+            f, e = ops.fock_assemble(g, g.view(dc), g.view(dx), g.view(c_ref), g.view(x_ref), pv, g.view(p_ref),
+                                     incr_t[sl])
+            wt = g.w.transpose(1, 2)
+            fo = torch.bmm(torch.bmm(wt, f), g.w)
+            po = torch.bmm(torch.bmm(g.ws, pv), g.ws.transpose(1, 2))
+            # commutator F_o P_o - P_o F_o = A - A^T with A = F_o P_o (both symmetric)
+            fe = ops.commutator(g, torch.bmm(fo, po), fo, slot_t)
+            fx = ops.diis(g, slot_t)
+            q, st, defect = _projector(g, fx, opts, ops, g.sp2_fixed if fixed else None)
             sp2_steps[0] += st
-            g.view(p_new).copy_(pn)
-            dchg = torch.sqrt(((pn - pv) ** 2).sum((1, 2)) / float(g.n * g.n))
-            stats_t[sl] = torch.stack([e, fe, dchg, defect], 1)
+            ops.finish(g, 2.0, q, pv, g.view(p_new), e, fe, defect, stats_t[sl])
         slot_t.add_(1).remainder_(D)
         nvtx.range_pop()
 

@@ -18,7 +18,7 @@ LIB = os.path.join(OUT, 'libpolymer_fock.so')
 SOURCES = ['pfe_mol_big2.cu', 'pfe_mol_big6.cu', 'pfe_mol_big4.cu', 'pfe_mol_big8.cu', 'pfe_mol_big3.cu',
            'pfe_mol_big7.cu', 'pfe_mol_big1.cu', 'pfe_mol_big5.cu', 'pfe_mol.cu', 'pfe_mol_batch.cu',
            'pfe_mol_mixed.cu', 'pfe_mol_batch_mixed.cu', 'pfe_mol_wide.cu', 'pfe_api.cu', 'pfe_eri.cu', 'pfe_lattice.cu', 'pfe_lattice_sl.cu', 'pfe_grad.cu', 'pfe_onee.cu',
-           'pfe_mlp.cu']
+           'pfe_mlp.cu', 'pfe_scf.cu']
 NVCC = os.environ.get('NVCC', 'nvcc')
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-diag-suppress', '177,550'] + \
@@ -51,7 +51,8 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     headers += [os.path.join(CSRC, 'generated', 'eri_classes.cuh'),
                 os.path.join(CSRC, 'generated', 'eri_grad_tables.cuh'),
                 os.path.join(os.path.dirname(HERE), 'include', 'polymer_fock.h'),
-                os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h')]
+                os.path.join(os.path.dirname(HERE), 'include', 'polymer_guess.h'),
+                os.path.join(os.path.dirname(HERE), 'include', 'polymer_scf.h')]
     newest_header = max(os.path.getmtime(d) for d in headers if os.path.exists(d))
     srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
 

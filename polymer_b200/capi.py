@@ -170,9 +170,18 @@ def lib(path: str = LIB_PATH):
                        ('pfe_mlp_colsum', [_vp, _vp, _i32, _i32, _vp]),
                        ('pfe_mlp_mse', [_vp, _vp, _vp, _f32, _vp, _vp, _i64, _vp]),
                        ('pfe_mlp_adam', [_vp, _vp, _vp, _vp, _vp, _i64, _f32, _f32, _f32, _f32, _i32, _f32, _vp]),
-                       ('pfe_mlp_to_bf16', [_vp, _vp, _i64, _vp])):
+                       ('pfe_mlp_to_bf16', [_vp, _vp, _i64, _vp]),
+                       ('pfe_scf_next_density', [_i32, _i32, _i32] + [_vp] * 11),
+                       ('pfe_scf_fock_assemble', [_i32, _i32] + [_vp] * 14),
+                       ('pfe_scf_commutator', [_i32, _i32, _i32] + [_vp] * 9),
+                       ('pfe_scf_diis', [_i32, _i32, _i32] + [_vp] * 9),
+                       ('pfe_scf_sp2_init', [_i32, _i32, _vp, _vp, _vp, _vp]),
+                       ('pfe_scf_sp2_step', [_i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+                       ('pfe_scf_finish', [_i32, _i32, ctypes.c_double] + [_vp] * 9)):
         getattr(L, name).argtypes = args
         getattr(L, name).restype = ctypes.c_int32
+    L.pfe_scf_workspace.argtypes = [_i32, _i32, _i32]
+    L.pfe_scf_workspace.restype = ctypes.c_int64
     _LIB = L
     return L
 
@@ -202,3 +211,7 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
 # Exported symbols declared in include/polymer_guess.h (checked by the CPU tests).
 GUESS_EXPORTS = ['pfe_mlp_gemm', 'pfe_mlp_bias_act', 'pfe_mlp_act_grad', 'pfe_mlp_colsum', 'pfe_mlp_mse',
                  'pfe_mlp_adam', 'pfe_mlp_to_bf16']
+
+# Exported symbols declared in include/polymer_scf.h (checked by the CPU tests).
+SCF_EXPORTS = ['pfe_scf_workspace', 'pfe_scf_next_density', 'pfe_scf_fock_assemble', 'pfe_scf_commutator',
+               'pfe_scf_diis', 'pfe_scf_sp2_init', 'pfe_scf_sp2_step', 'pfe_scf_finish']

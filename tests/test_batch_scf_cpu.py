@@ -51,7 +51,7 @@ def test_diis_coefficients_match_the_pulay_system():
     valid[2, :] = False
     valid[2, 3] = True
     slot = torch.tensor([3])
-    c = batch_scf._diis(e, valid, slot).numpy()
+    c = batch_scf.pulay_coefficients(e, valid, slot).numpy()
     for b in range(B):
         idx = np.nonzero(valid[b].numpy())[0]
         m = len(idx)

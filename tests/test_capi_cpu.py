@@ -28,6 +28,7 @@ HEADER = os.path.join(ROOT, 'include', 'polymer_fock.h')
 
 
 GUESS_HEADER = os.path.join(ROOT, 'include', 'polymer_guess.h')
+SCF_HEADER = os.path.join(ROOT, 'include', 'polymer_scf.h')
 
 
 def _declared(path=HEADER):
@@ -38,13 +39,14 @@ def _declared(path=HEADER):
 def test_header_declares_the_exports():
     assert _declared() == sorted(capi.EXPORTS)
     assert _declared(GUESS_HEADER) == sorted(capi.GUESS_EXPORTS)
+    assert _declared(SCF_HEADER) == sorted(capi.SCF_EXPORTS)
 
 
 def test_library_exports_every_symbol():
     lib = build.build()
     out = subprocess.run(['nm', '-D', '--defined-only', lib], capture_output=True, text=True, check=True).stdout
     exported = set(ln.split()[-1] for ln in out.splitlines() if ln.strip())
-    missing = [s for s in capi.EXPORTS + capi.GUESS_EXPORTS if s not in exported]
+    missing = [s for s in capi.EXPORTS + capi.GUESS_EXPORTS + capi.SCF_EXPORTS if s not in exported]
     assert not missing, missing
 
 
