@@ -27,9 +27,14 @@ extern "C" {
 #define PFE_EINVAL (-1)      /* malformed arguments (sizes, shell map, cutoffs) */
 #define PFE_ECUDA (-2)       /* a CUDA runtime / cuBLAS call failed */
 #define PFE_EUNSUPPORTED (-3)/* valid input outside what the kernels implement */
-#define PFE_ERANGE (-4)      /* Boys argument/order outside the IGAMMA table (reference: PABORT 'FMT CANNOT BE EVALUATED') */
+#define PFE_ERANGE (-4)      /* Boys order outside the IGAMMA table (reference: PABORT 'FMT CANNOT BE EVALUATED',
+                                src/pfourindexdirect.f90:537-538).  Not reachable in this version: shells up to d
+                                need orders <= 8 (9 for the gradient) of the table's 0..21, and higher shells are
+                                refused with PFE_EUNSUPPORTED; the code is kept so that callers can map the abort. */
 #define PFE_ENOMEM (-5)      /* device allocation failed */
-#define PFE_ETIMEOUT (-6)    /* a bounded device wait gave up */
+#define PFE_ETIMEOUT (-6)    /* a bounded device wait gave up.  Not reachable in this version: no kernel waits on
+                                another block, kernel or rank (work is handed out by atomic tickets), so there is
+                                no device wait to bound. */
 #define PFE_ENAN (-7)        /* non-finite density on input */
 
 #define PFE_PREC_FP64 0      /* every quartet in FP64 (parity path) */
