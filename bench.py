@@ -331,6 +331,32 @@ def extra_legs(device: int, peak: float):
     return out
 
 
+class _EventTimedFock:
+    """A DeviceFock whose calls (Fock builds) are bracketed by CUDA events on the
+    current stream, so that the device time of a whole SCF's builds can be summed."""
+
+    def __init__(self, df, dev):
+        self._df, self._dev, self._ev = df, dev, []
+
+    def __call__(self, *a, **kw):
+        import torch
+        s = torch.cuda.current_stream(self._dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        r = self._df(*a, **kw)
+        e1.record(s)
+        self._ev.append((e0, e1))
+        return r
+
+    def __getattr__(self, name):
+        return getattr(self._df, name)
+
+    def device_s(self) -> float:
+        import torch
+        torch.cuda.synchronize(self._dev)
+        return sum(a.elapsed_time(b) for a, b in self._ev) * 1e-3
+
+
 def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: bool = False, scf_runs: bool = True):
     """Uneven water clusters (cc-pVDZ, k ~ U{1..16} as geometry.water_batch_decks
     draws them) as one batch: batched full FP64 Fock builds per second, and the
@@ -399,13 +425,15 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
         return out
     # plain: the reference's loop with full FP64 builds, one molecule after another
     e_plain, it_plain = [], []
+    t_plain_builds = 0.0
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     for s in systems:
-        df = fock.DeviceFock(s, device)
+        df = _EventTimedFock(fock.DeviceFock(s, device), dev)
         r = scf.run_scf(s, df, device=dev, variational=True)
         e_plain.append(r.energy_variational)
         it_plain.append(len(r.iterations))
+        t_plain_builds += df.device_s()
         df.close()
     torch.cuda.synchronize(dev)
     t_plain = time.perf_counter() - t0
@@ -435,7 +463,12 @@ def batch_leg(n_clusters: int, device: int, steps: int, warmup: int, autotune: b
                                   'mixed_cutoff': opts.mixed_cutoff, 'reset_every': opts.reset_every,
                                   'guess': opts.guess if isinstance(opts.guess, str) else 'learned',
                                   'cuda_graph': 'each iteration from the third on is one graph replay'}}
-    out['scf'] = {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)), **runs,
+    out['scf'] = {'plain_fp64_s': t_plain, 'plain_iterations_mean': float(np.mean(it_plain)),
+                  'plain_fp64_build_s': t_plain_builds,
+                  'plain_fp64_build_note': 'CUDA-event time of the plain loop\'s Fock builds alone (the rest of '
+                                           'plain_fp64_s is its host loop, eigensolver and transfers)',
+                  'batched_vs_plain_builds_only': {k: t_plain_builds / v['s'] for k, v in runs.items()},
+                  **runs,
                   'wall_clock': 'host time around each whole set, GPU synchronised; one-electron set-up excluded; '
                                 'batched: best of two runs after one untimed run'}
     return out
