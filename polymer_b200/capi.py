@@ -14,7 +14,9 @@ from typing import Optional
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, '_build', 'libpolymer_fock.so')
+# PFE_LIBRARY names another build of the library to load instead (a variant
+# compiled with other tuning macros); by default the in-tree build.
+LIB_PATH = os.environ.get('PFE_LIBRARY') or os.path.join(HERE, '_build', 'libpolymer_fock.so')
 
 PFE_OK = 0
 PFE_PREC_FP64 = 0

@@ -23,11 +23,12 @@ struct __align__(16) PairRec {
 static_assert(sizeof(PairRec) == 128, "PairRec layout");
 
 struct PairView {
-  double P[3], PA[3], AB[3], zeta, S, oz;
+  double P[3], PA[3], AB[3], zeta, S, oz, bound;
   int si, sj;
 };
 
-// the record of pair t after its bound (already loaded) passed the screen
+// the record of pair t with its Schwarz bound (the quartet loops load the whole
+// record before screening on the bound: one load latency per pair, not two)
 __device__ __forceinline__ PairView load_pair(const PairRec* __restrict__ rec, int t) {
   const double2* r = reinterpret_cast<const double2*>(rec + t);
   const double2 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3), e = __ldg(r + 4),
@@ -36,7 +37,7 @@ __device__ __forceinline__ PairView load_pair(const PairRec* __restrict__ rec, i
   v.P[0] = a.x; v.P[1] = a.y; v.P[2] = b.x;
   v.PA[0] = b.y; v.PA[1] = c.x; v.PA[2] = c.y;
   v.AB[0] = d.x; v.AB[1] = d.y; v.AB[2] = e.x;
-  v.zeta = e.y; v.S = f.x;
+  v.zeta = e.y; v.S = f.x; v.bound = f.y;
   v.si = __double2loint(g.x); v.sj = __double2hiint(g.x);
   v.oz = g.y;
   return v;
@@ -200,6 +201,15 @@ struct GqOccupancy {
 #endif
 };
 
+// Largest class (integrals per quartet) whose bra loop prefetches the next pair record.
+struct GqPrefetch {
+#ifdef PFE_GQ_PREFETCH
+  static constexpr int ni = PFE_GQ_PREFETCH;
+#else
+  static constexpr int ni = 0;
+#endif
+};
+
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch lq) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
@@ -286,10 +296,10 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
     for (int qi = 0;; ++qi) {
       const bool lv = qi < hn;
       const int q = h0 + (lv ? qi : 0);
-      const double sq = lv ? pair_bound(rec, q) : 0.0;
+      const PairView kq = load_pair(rec, q);
+      const double sq = lv ? kq.bound : 0.0;
       const bool qok = lv && sq * gmax >= thr;
       if (!__any_sync(0xffffffffu, qok)) break;
-      const PairView kq = load_pair(rec, q);
       const double ze = kq.zeta;
       const double Qx = kq.P[0], Qy = kq.P[1], Qz = kq.P[2];
       const double Sq = kq.S;
@@ -309,13 +319,24 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
 #pragma unroll
           for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = wKL * sK[cc] * sL[d];
       }
+      // classes with at most GqPrefetch::ni integrals load the next bra record while
+      // the current quartet is evaluated (its load latency leaves the chain)
+      constexpr bool PF = NI <= GqPrefetch::ni;
+      PairView nx;
+      if constexpr (PF) nx = load_pair(rec, g0);
       for (int p = g0; p < g0 + gn; ++p) {
-        const double sp = pair_bound(rec, p);
+        PairView bp;
+        if constexpr (PF) {
+          bp = nx;
+          if (p + 1 < g0 + gn) nx = load_pair(rec, p + 1);
+        } else {
+          bp = load_pair(rec, p);
+        }
+        const double sp = bp.bound;
         const bool pass = qok && sp * sq >= thr;
         if (!__any_sync(0xffffffffu, pass)) break;   // later bra pairs fail for every lane
         // a group paired with itself: each unordered pair of pairs once (p >= q)
         if (!pass || (G == H && p < q)) continue;
-        const PairView bp = load_pair(rec, p);
         const int I = bp.si, J = bp.sj;
         const double zb = bp.zeta;
         const double Px = bp.P[0], Py = bp.P[1], Pz = bp.P[2];

@@ -166,17 +166,17 @@ __global__ void __launch_bounds__(256) k_gq_wide(MolLaunch lq, OpTableDev tab, i
       for (int t = lane; t < nb * nd; t += 32) P[W::OBD + t] = dt_at(D, nt, tB[t / nd], tD[t % nd]);
       bool any = false;   // warp-uniform
       for (int p = g0; p < g0 + gn; ++p) {
-        const double sp = pair_bound(rec, p);
-        if (sp * hmax < thr) break;
         const PairView bp = load_pair(rec, p);
+        const double sp = bp.bound;
+        if (sp * hmax < thr) break;
         const int I = bp.si, J = bp.sj;
         const double zb = bp.zeta;
         const int qe = (G == H) ? p + 1 : h0 + hn;
         bool cab_ready = false;
         for (int q = h0; q < qe; ++q) {
-          const double sq = pair_bound(rec, q);
-          if (sp * sq < thr) break;   // the reference's screen (warp-uniform)
           const PairView kq = load_pair(rec, q);
+          const double sq = kq.bound;
+          if (sp * sq < thr) break;   // the reference's screen (warp-uniform)
           const int K = kq.si, L = kq.sj;
           const double ze = kq.zeta;
           const double zz = zb + ze, rzz = 1.0 / zz, rho = zb * ze * rzz;
