@@ -201,6 +201,15 @@ struct GqOccupancy {
 #endif
 };
 
+template <int LT>
+struct GqSmemBoys {
+#ifdef PFE_GQ_SMEM_BOYS
+  static constexpr bool use = BoysSmem<LT>::use;
+#else
+  static constexpr bool use = false;
+#endif
+};
+
 // Largest class (integrals per quartet) whose bra loop prefetches the next pair record.
 struct GqPrefetch {
 #ifdef PFE_GQ_PREFETCH
@@ -234,9 +243,12 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   const int lane = threadIdx.x & 31;
   const int nchunks = *lq.nchunks;
   const double c2pi = 2.0 / sqrt(REF_PI);
-  // classes of total angular momentum up to 4 read their Boys rows from a copy
-  // of the table's first rows in shared memory (the launch passes its size)
-  constexpr bool SBOYS = BoysSmem<LT>::use;
+  // with PFE_GQ_SMEM_BOYS, classes of total angular momentum up to 4 read their
+  // Boys rows from a copy of the table's first rows in shared memory (the launch
+  // passes its size); off by default: measured on C20H42 it cost 10-16 % on the
+  // low classes (fewer resident blocks, the per-block copy), the L1-cached
+  // gathers of the global table are as fast
+  constexpr bool SBOYS = GqSmemBoys<LT>::use;
   extern __shared__ double s_boys[];
   if constexpr (SBOYS) {
     boys_stage<LT>(lq.boys, s_boys);
@@ -504,7 +516,7 @@ struct Passes {
   static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
     constexpr int LT = LA + LB + LC + LD;
     auto kern = k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED, BATCH>;
-    if constexpr (BoysSmem<LT>::use) {
+    if constexpr (GqSmemBoys<LT>::use) {
       // the staged Boys rows: allow them once, and launch no more blocks than can be
       // resident (each block copies the rows once; the work queue spreads the chunks)
       static int resident = 0;
