@@ -107,6 +107,54 @@ __device__ __forceinline__ void boys_tab(double T, double pref, const double* __
   boys_eval<L>(T, pref, gv, F);
 }
 
+// Coefficients 1/(k! (2L+2k+1)), k = 0..17, of the Maclaurin series
+// F_L(T) = sum_k (-T)^k / (k! (2L+2k+1)); at T <= 1 the omitted terms are below 1e-17.
+template <int L>
+struct BoysSeries {
+  double c[18];
+  constexpr BoysSeries() : c() {
+    double f = 1.0;   // k!
+    for (int k = 0; k < 18; ++k) {
+      if (k > 0) f *= (double)k;
+      c[k] = 1.0 / (f * (double)(2 * L + 2 * k + 1));
+    }
+  }
+};
+
+// F_m(T)*pref for m = 0..L (L <= 2) without reading the table, for kernels whose
+// per-lane table-row gathers are what their L1 spends its wavefronts on:
+//  * T >= 1: F_0 = F1(0) erf(sqrt T)/sqrt T (F1(0) = sqrt(PI)/2, the constant of the
+//    asymptotic form) and upward recursion F_{m+1} = ((2m+1) F_m - e^-T)/(2T), whose
+//    error grows by at most (2m+1)/(2T) <= 3/2 per step here;
+//  * T < 1: the series above for F_L and downward recursion
+//    F_{m-1} = (2T F_m + e^-T)/(2m-1), which is stable.
+// The reference tabulates and Taylor-expands every order (boys_eval); the two agree to
+// the table's own accuracy (about 1e-14 relative), far inside the build's tolerance.
+template <int L>
+__device__ __forceinline__ void boys_direct(double T, double pref, double* __restrict__ F) {
+  static_assert(L <= 2, "boys_direct: orders 0..2");
+  if (T >= 1.0) {
+    const double r = rsqrt(T);
+    F[0] = pref * PFE_F1_0 * erf(T * r) * r;
+    if (L >= 1) {
+      const double e = pref * exp(-T), h = 0.5 * r * r;
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = ((double)(2 * m + 1) * F[m] - e) * h;
+    }
+  } else {
+    constexpr BoysSeries<L> S{};
+    double v = S.c[17];
+#pragma unroll
+    for (int k = 16; k >= 0; --k) v = fma(v, -T, S.c[k]);
+    F[L] = pref * v;
+    if (L >= 1) {
+      const double e = pref * exp(-T);
+#pragma unroll
+      for (int m = L; m > 0; --m) F[m - 1] = (2.0 * T * F[m] + e) * (1.0 / (double)(2 * m - 1));
+    }
+  }
+}
+
 // The part of IGAMMA a Boys evaluation of orders 0..L can read -- rows 0..20*TF(L)
 // (the Taylor branch is taken below TF(L)), BoysRow<L>::N columns -- staged in
 // shared memory by a kernel, so that the per-lane row gathers of the quartet

@@ -61,7 +61,7 @@ struct LatticeState {
   double* d_quirk = nullptr;   // ntk * npl bra bounds (sorted order of the Q1 list)
   LatticeLaunch launches[36];
   int nlaunch = 0;
-  int* d_queue = nullptr;      // one chunk counter per launch (straight-line kernels)
+  int* d_queue = nullptr;      // kLatQueueSlots chunk counters per launch (straight-line kernels, per pass)
   bool interpret_only = false; // every class on the op-table interpreter (tests)
   double quartets = 0.0, flops = 0.0;
 };
@@ -547,7 +547,7 @@ int lattice_setup(pfe_context* ctx, const pfe_args* a) {
   cudaStream_t s = ctx->stream;
   LatticeState* L = new LatticeState();
   ctx->lattice = L;
-  PFE_CUDA(ctx->alloc((void**)&L->d_queue, sizeof(int) * 64));
+  PFE_CUDA(ctx->alloc((void**)&L->d_queue, sizeof(int) * 64 * kLatQueueSlots));
   if (!ctx->d_n32) {   // FP32 quartet counter of the mixed-precision path
     PFE_CUDA(ctx->alloc((void**)&ctx->d_n32, sizeof(unsigned long long)));
     PFE_CUDA(cudaMemset(ctx->d_n32, 0, sizeof(unsigned long long)));
@@ -773,12 +773,12 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
   R.far32 = ctx->mcut > 0.0 ? 1 : 0;
   R.n32 = ctx->d_n32;
   PFE_CUDA(cudaMemsetAsync(ctx->d_n32, 0, sizeof(unsigned long long), s));
-  PFE_CUDA(cudaMemsetAsync(L->d_queue, 0, sizeof(int) * 64, s));
+  PFE_CUDA(cudaMemsetAsync(L->d_queue, 0, sizeof(int) * 64 * kLatQueueSlots, s));
   for (int i = 0; i < L->nlaunch; ++i) {
     const LatticeLaunch& ll = L->launches[i];
     R.chunks = ll.chunks;
     R.nchunks = ll.d_nchunks;
-    R.queue = L->d_queue + i;
+    R.queue = L->d_queue + kLatQueueSlots * i;
     const int e1 = std::max(ll.cb, ll.ck), e2 = std::min(ll.cb, ll.ck);
     if (LatSlFn f = L->interpret_only ? nullptr : lattice_sl_launcher(e1, e2, ll.cb < ll.ck)) {
       // straight-line: one chunk per warp from the queue, a persistent grid of 16 blocks per SM

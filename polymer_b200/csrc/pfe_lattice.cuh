@@ -43,6 +43,8 @@ struct LatticeRun {
 // The straight-line kernel of evaluated class (e1|e2) (e1 >= e2, swap: the
 // chunk's bra class is e2) on `grid` blocks of 128 threads, or null where the
 // class has more than 64 integrals (it keeps the op-table interpreter).
+// work-queue counters per lattice class launch (one per register pass)
+constexpr int kLatQueueSlots = 4;
 using LatSlFn = void (*)(const LatticeRun&, int grid, cudaStream_t);
 LatSlFn lattice_sl_launcher(int e1, int e2, bool sw);
 

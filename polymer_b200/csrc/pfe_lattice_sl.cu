@@ -14,7 +14,11 @@
 // stay in registers and are digested as they are produced): the J sums of the
 // bra's components accumulate in registers over the chunk's kets and cells and
 // are reduced over the warp once, the K contributions go straight to the
-// atomics.  Classes of up to 64 integrals; larger ones keep the interpreter.
+// atomics.  Classes of up to 64 integrals in one launch; (11|11) in four
+// register passes, pass p keeping the chunk bra's first component a = p (64
+// integrals each; the K sums of a pass are partial sums over the kept
+// components, so the passes' atomics add up to the full digestion).  Larger
+// classes keep the interpreter.
 // With mixed precision the cells Q3 outside the CUTOFF1 box (the far cells)
 // run the recursion in FP32 on F_m/pref, the rest in FP64.
 
@@ -30,8 +34,9 @@ namespace {
 
 // K digestion of one quartet: X(i,l,cell) += sum_{j,k} D(k,j) (ij|kl), with the
 // bra's (SWB) and the ket's (SWK) centre order fixed at compile time so that
-// every integral index is a constant (the integrals stay in registers).
-template <int N1, int N2, int M1, int M2, bool SWAP, bool SWB, bool SWK>
+// every integral index is a constant (the integrals stay in registers); only the
+// integrals whose chunk-bra first component lies in [A0, A1) (this pass's).
+template <int N1, int N2, int M1, int M2, bool SWAP, bool SWB, bool SWK, int A0, int A1>
 __device__ __forceinline__ void lat_k(const double* out, const int* b1, const int* b2, const int* k1, const int* k2,
                                       const double* __restrict__ Dk, size_t ck, double* __restrict__ xp, size_t cx,
                                       int npgs) {
@@ -47,12 +52,14 @@ __device__ __forceinline__ void lat_k(const double* out, const int* b1, const in
       dk[kc * nJ + jc] = (kp >= 0 && jp >= 0) ? __ldg(Dk + kp + (size_t)npgs * jp + ck) : 0.0;
     }
 #pragma unroll
-  for (int ic = 0; ic < nI; ++ic)
+  for (int ic = 0; ic < nI; ++ic) {
+    if (!SWB && (ic < A0 || ic >= A1)) continue;
 #pragma unroll
     for (int lc = 0; lc < nL; ++lc) {
       double acc = 0.0;
 #pragma unroll
-      for (int jc = 0; jc < nJ; ++jc)
+      for (int jc = 0; jc < nJ; ++jc) {
+        if (SWB && (jc < A0 || jc >= A1)) continue;
 #pragma unroll
         for (int kc = 0; kc < nK; ++kc) {
           const int a = SWB ? jc : ic, b = SWB ? ic : jc;
@@ -60,15 +67,18 @@ __device__ __forceinline__ void lat_k(const double* out, const int* b1, const in
           const int idx = SWAP ? ((cc * M2 + d) * N1 + a) * N2 + b : ((a * N2 + b) * M1 + cc) * M2 + d;
           acc = fma(dk[kc * nJ + jc], out[idx], acc);
         }
+      }
       const int ip = SWB ? b2[ic] : b1[ic];
       const int lp = SWK ? k1[lc] : k2[lc];
       if (ip >= 0 && lp >= 0 && acc != 0.0) atomicAdd(xp + ip + (size_t)npgs * lp + cx, acc);
     }
+  }
 }
 
 // (LA LB|LC LD) is the evaluated canonical class; SWAP: the chunk's bra pair is
-// its ket pair (the chunk's bra class is the lower one).
-template <int LA, int LB, int LC, int LD, bool SWAP>
+// its ket pair (the chunk's bra class is the lower one).  Register pass PASS of
+// NPASS keeps the chunk bra's first components [A0, A1).
+template <int LA, int LB, int LC, int LD, bool SWAP, int NPASS = 1, int PASS = 0>
 __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
   constexpr int LT = LA + LB + LC + LD;
@@ -76,6 +86,8 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
   constexpr int N1 = SWAP ? NC : NA, N2 = SWAP ? ND : NB;   // the chunk's bra: first, second centre
   constexpr int M1 = SWAP ? NA : NC, M2 = SWAP ? NB : ND;   // the lane's ket: first, second centre
   constexpr int NBRA = N1 * N2;
+  constexpr int A0 = PASS * N1 / NPASS, A1 = (PASS + 1) * N1 / NPASS;
+  static_assert(A0 < A1, "every pass keeps a component");
   const int lane = threadIdx.x & 31;
   const PairArrays pr = R.pairs;
   const int npgs = R.npgs;
@@ -157,7 +169,8 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
       const double dx = Pb[0] - Q[0], dy = Pb[1] - Q[1], dz = Pb[2] - Q[2];
       const double T = rho * (dx * dx + dy * dy + dz * dz);
       double F[LT + 1];
-      boys_tab<LT>(T, f32 ? 1.0 : pref, R.boys, F);
+      if constexpr (LT <= GqBoysDirect::maxl) boys_direct<LT>(T, f32 ? 1.0 : pref, F);
+      else boys_tab<LT>(T, f32 ? 1.0 : pref, R.boys, F);
       double out[NI];
       if constexpr (LT == 0) {
         out[0] = F[0];
@@ -184,7 +197,7 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
         if (f32) eri_prec<float, LA, LB, LC, LD>(F, pref, e, out);
         else eri_prec<double, LA, LB, LC, LD>(F, pref, e, out);
       }
-      n32 += f32 ? 1u : 0u;
+      n32 += (f32 && PASS == 0) ? 1u : 0u;
       // integral of the bra's components (a first, b second) and the ket's (c, d)
       auto E = [&](int a, int b, int cc, int d) -> double {
         return out[SWAP ? ((cc * M2 + d) * N1 + a) * N2 + b : ((a * N2 + b) * M1 + cc) * M2 + d];
@@ -200,7 +213,7 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
       }
       // J: sum over the ket's components, accumulated over cells and kets
 #pragma unroll
-      for (int a = 0; a < N1; ++a)
+      for (int a = A0; a < A1; ++a)
 #pragma unroll
         for (int b = 0; b < N2; ++b) {
           double acc = 0.0;
@@ -216,16 +229,16 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
                                 : pp2 * cell1_index(g, q1[0] - q3x, q1[1] - q3y, q1[2] - q3z);
         const double* __restrict__ Dk = helix ? R.pph : R.pp;
         const size_t cx = pp2 * cell1_index(g, q3x + q2[0], q3y + q2[1], q3z + q2[2]);
-        if (!swb && !swk) lat_k<N1, N2, M1, M2, SWAP, false, false>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
-        else if (!swb) lat_k<N1, N2, M1, M2, SWAP, false, true>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
-        else if (!swk) lat_k<N1, N2, M1, M2, SWAP, true, false>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
-        else lat_k<N1, N2, M1, M2, SWAP, true, true>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
+        if (!swb && !swk) lat_k<N1, N2, M1, M2, SWAP, false, false, A0, A1>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
+        else if (!swb) lat_k<N1, N2, M1, M2, SWAP, false, true, A0, A1>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
+        else if (!swk) lat_k<N1, N2, M1, M2, SWAP, true, false, A0, A1>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
+        else lat_k<N1, N2, M1, M2, SWAP, true, true, A0, A1>(out, b1, b2, k1, k2, Dk, ck, R.xp, cx, npgs);
       }
     }
     // J of this chunk: reduce the lanes' sums, one atomic per bra component pair
     const size_t c1q1 = pp2 * cell1_index(g, q1[0], q1[1], q1[2]);
 #pragma unroll
-    for (int a = 0; a < N1; ++a)
+    for (int a = A0; a < A1; ++a)
 #pragma unroll
       for (int b = 0; b < N2; ++b) {
         const double v = warp_sum(jacc[a * N2 + b]);
@@ -243,6 +256,17 @@ void launch_sl(const LatticeRun& r, int grid, cudaStream_t s) {
   k_lat_sl<LA, LB, LC, LD, SW><<<grid, 128, 0, s>>>(r);
 }
 
+// The register passes of a class, one launch each on its own work-queue counter
+// (r.queue + PASS: the lattice build zeroes kLatQueueSlots counters per class).
+template <int LA, int LB, int LC, int LD, bool SW, int NPASS, int PASS = 0>
+void launch_sl_passes(const LatticeRun& r, int grid, cudaStream_t s) {
+  static_assert(NPASS <= kLatQueueSlots, "a counter per pass");
+  LatticeRun rp = r;
+  rp.queue = r.queue + PASS;
+  k_lat_sl<LA, LB, LC, LD, SW, NPASS, PASS><<<grid, 128, 0, s>>>(rp);
+  if constexpr (PASS + 1 < NPASS) launch_sl_passes<LA, LB, LC, LD, SW, NPASS, PASS + 1>(r, grid, s);
+}
+
 }  // namespace
 
 // evaluated class (e1 >= e2) and swap flag -> straight-line launcher, or null
@@ -254,6 +278,7 @@ LatSlFn lattice_sl_launcher(int e1, int e2, bool sw) {
     case 9: return L2(1, 0, 1, 0);
     case 16: return L2(1, 1, 0, 0);
     case 17: return L2(1, 1, 1, 0);
+    case 18: return sw ? &launch_sl_passes<1, 1, 1, 1, true, 4> : &launch_sl_passes<1, 1, 1, 1, false, 4>;
     case 24: return L2(2, 0, 0, 0);
     case 25: return L2(2, 0, 1, 0);
     case 32: return L2(2, 1, 0, 0);

@@ -210,6 +210,16 @@ struct GqSmemBoys {
 #endif
 };
 
+// Classes of total angular momentum up to maxl evaluate the Boys function without
+// the table (boys_direct): their lanes' table-row gathers fill the L1 data pipe.
+struct GqBoysDirect {
+#ifdef PFE_BOYS_DIRECT_MAXL
+  static constexpr int maxl = PFE_BOYS_DIRECT_MAXL;
+#else
+  static constexpr int maxl = -1;
+#endif
+};
+
 // Largest class (integrals per quartet) whose bra loop prefetches the next pair record.
 struct GqPrefetch {
 #ifdef PFE_GQ_PREFETCH
@@ -364,7 +374,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
         if constexpr (MIXED && LT > 0) f32 = __all_sync(__activemask(), sp * sq * pmax < mcut);
         n32 += f32 ? 1u : 0u;
         double F[LT + 1];
-        if constexpr (SBOYS) boys_tab_smem<LT>(T, f32 ? 1.0 : pref, s_boys, F);
+        if constexpr (LT <= GqBoysDirect::maxl) boys_direct<LT>(T, f32 ? 1.0 : pref, F);
+        else if constexpr (SBOYS) boys_tab_smem<LT>(T, f32 ? 1.0 : pref, s_boys, F);
         else boys_tab<LT>(T, f32 ? 1.0 : pref, boys, F);
         double out[NI];
         if constexpr (LT == 0) {
