@@ -737,7 +737,7 @@ int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
     n += (ctx->contracted ? 2 : 0) + 2 + ((ctx->dtol > 0.0 || ctx->mcut > 0.0) ? 1 : 0);
     out->kernel_launches = n;
   } else {
-    out->kernel_launches = ctx->nlaunch + 3;
+    out->kernel_launches = lattice_class_launches(ctx) + 3;
   }
   return PFE_OK;
 }

@@ -280,6 +280,7 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
                  cudaStream_t s);
 void lattice_release(pfe_context* ctx);
 void lattice_force_interpreter(pfe_context* ctx, bool on);
+int lattice_class_launches(pfe_context* ctx);
 int molecular_gradient_pp(pfe_context* ctx, const double* d_pp, const int* d_satom, int natom, double* d_gj,
                           double* d_gk, cudaStream_t s);
 const char* last_error_cstr();

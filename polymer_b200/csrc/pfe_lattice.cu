@@ -811,6 +811,20 @@ int lattice_fock(pfe_context* ctx, const double* d_pp, const double* d_pph, doub
   return PFE_OK;
 }
 
+// Class kernel launches of one lattice build: a straight-line class's register
+// passes, one launch for an interpreted class.
+int lattice_class_launches(pfe_context* ctx) {
+  const LatticeState* L = (const LatticeState*)ctx->lattice;
+  if (!L) return 0;
+  int n = 0;
+  for (int i = 0; i < L->nlaunch; ++i) {
+    const LatticeLaunch& ll = L->launches[i];
+    const int e1 = std::max(ll.cb, ll.ck), e2 = std::min(ll.cb, ll.ck);
+    n += L->interpret_only ? 1 : std::max(1, lattice_sl_passes(e1, e2));
+  }
+  return n;
+}
+
 void lattice_force_interpreter(pfe_context* ctx, bool on) {
   if (ctx->lattice) ((LatticeState*)ctx->lattice)->interpret_only = on;
 }

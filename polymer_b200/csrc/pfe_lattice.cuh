@@ -47,5 +47,7 @@ struct LatticeRun {
 constexpr int kLatQueueSlots = 4;
 using LatSlFn = void (*)(const LatticeRun&, int grid, cudaStream_t);
 LatSlFn lattice_sl_launcher(int e1, int e2, bool sw);
+// launches (register passes) of a straight-line class, 0 where the class has none
+int lattice_sl_passes(int e1, int e2);
 
 }  // namespace pfe

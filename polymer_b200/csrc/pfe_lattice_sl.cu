@@ -169,8 +169,7 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
       const double dx = Pb[0] - Q[0], dy = Pb[1] - Q[1], dz = Pb[2] - Q[2];
       const double T = rho * (dx * dx + dy * dy + dz * dz);
       double F[LT + 1];
-      if constexpr (LT <= GqBoysDirect::maxl) boys_direct<LT>(T, f32 ? 1.0 : pref, F);
-      else boys_tab<LT>(T, f32 ? 1.0 : pref, R.boys, F);
+      boys_tab<LT>(T, f32 ? 1.0 : pref, R.boys, F);
       double out[NI];
       if constexpr (LT == 0) {
         out[0] = F[0];
@@ -268,6 +267,11 @@ void launch_sl_passes(const LatticeRun& r, int grid, cudaStream_t s) {
 }
 
 }  // namespace
+
+int lattice_sl_passes(int e1, int e2) {
+  if (!lattice_sl_launcher(e1, e2, false)) return 0;
+  return (e1 == 2 && e2 == 2) ? 4 : 1;
+}
 
 // evaluated class (e1 >= e2) and swap flag -> straight-line launcher, or null
 LatSlFn lattice_sl_launcher(int e1, int e2, bool sw) {

@@ -211,12 +211,17 @@ struct GqSmemBoys {
 };
 
 // Classes of total angular momentum up to maxl evaluate the Boys function without
-// the table (boys_direct): their lanes' table-row gathers fill the L1 data pipe.
+// the table (boys_direct): their lanes' per-quartet table-row gathers were half of
+// their L1 wavefronts.  Measured on the 32-cluster water batch: (10|00) 55.8 ->
+// 53.0 ms (long-scoreboard stalls halved, instructions +60 % for erf and exp), the
+// batched build 295.8 -> 287.5 ms; C20H42 unchanged.  The lattice kernels keep the
+// table (their classes ran 12 % slower on it: they already spend the FP64 pipe on
+// the screw rotations of every image cell).
 struct GqBoysDirect {
 #ifdef PFE_BOYS_DIRECT_MAXL
   static constexpr int maxl = PFE_BOYS_DIRECT_MAXL;
 #else
-  static constexpr int maxl = -1;
+  static constexpr int maxl = 2;
 #endif
 };
 
