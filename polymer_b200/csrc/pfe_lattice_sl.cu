@@ -98,6 +98,19 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
   const int h3 = g.c2[0] + g.c1[0];
   const bool helix = R.pph != nullptr;
   unsigned long long n32 = 0;
+  // cos and sin of the screw angle of every image cell along x, once per block
+  // (the same functions of the same arguments the lanes would evaluate per cell)
+  constexpr int kMaxRot = 257;
+  __shared__ double s_cs[kMaxRot], s_sn[kMaxRot];
+  const int nrot = 2 * g.c2[0] + 1;
+  const bool rot_tab = nrot <= kMaxRot;
+  if (rot_tab)
+    for (int i = threadIdx.x; i < nrot; i += blockDim.x) {
+      const double ang = (i - g.c2[0]) * g.helix;
+      s_cs[i] = cos(ang);
+      s_sn[i] = sin(ang);
+    }
+  __syncthreads();
   for (;;) {
     int tk = 0;
     if (lane == 0) tk = atomicAdd(R.queue, 1);
@@ -160,7 +173,15 @@ __global__ void __launch_bounds__(128) k_lat_sl(LatticeRun R) {
                (q1[k] - q3[k] <= g.c1[k]);
       const bool f32 = R.far32 && LT > 0 && (abs(q3x) > g.c1[0] || abs(q3y) > g.c1[1] || abs(q3z) > g.c1[2]);
       if (!act) continue;
-      const double ang = q3x * g.helix, cs = cos(ang), sn = sin(ang);
+      double cs, sn;
+      if (rot_tab) {
+        cs = s_cs[q3x + g.c2[0]];
+        sn = s_sn[q3x + g.c2[0]];
+      } else {
+        const double ang = q3x * g.helix;
+        cs = cos(ang);
+        sn = sin(ang);
+      }
       // screw image of the ket pair: rotate about x, then translate
       const double Q[3] = {Qb[0] + q3x * g.period[0], Qb[1] * cs - Qb[2] * sn + q3y * g.period[1],
                            Qb[1] * sn + Qb[2] * cs + q3z * g.period[2]};
