@@ -699,7 +699,7 @@ int32_t pfe_batch_census(pfe_batch* b, pfe_census* out) {
   }
   int n = 0;
   for (int i = 0; i < b->nlaunch; ++i)
-    n += (b->launches[i].variant == 0 && b->launches[i].has_straight) ? b->launches[i].npass : 1;
+    n += (b->launches[i].variant == 0 && b->launches[i].has_straight) ? b->launches[i].npass_live : 1;
   tot.kernel_launches = n;
   *out = tot;
   return PFE_OK;
@@ -733,7 +733,7 @@ int32_t pfe_context_census(pfe_context* ctx, pfe_census* out) {
     // maxima under density screening or mixed precision
     int n = 0;
     for (int i = 0; i < ctx->nlaunch; ++i)
-      n += (ctx->launches[i].variant == 0 && ctx->launches[i].has_straight) ? ctx->launches[i].npass : 1;
+      n += (ctx->launches[i].variant == 0 && ctx->launches[i].has_straight) ? ctx->launches[i].npass_live : 1;
     n += (ctx->contracted ? 2 : 0) + 2 + ((ctx->dtol > 0.0 || ctx->mcut > 0.0) ? 1 : 0);
     out->kernel_launches = n;
   } else {

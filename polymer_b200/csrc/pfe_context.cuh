@@ -72,7 +72,8 @@ struct ClassLaunch {
   size_t smem_wide;
   int* queue;                // device work queue: one chunk counter per launch (pass), zeroed before each
   unsigned int* cost;        // screened primitive quartets per chunk (chunks are sorted by it, descending)
-  int npass;                 // launches of the straight-line variant
+  int npass;                 // register passes of the straight-line variant
+  int npass_live;            // of which launched: the others keep no component with a coefficient
   int gmul = 32;             // straight-line variant: persistent grid of up to gmul blocks per SM
 };
 

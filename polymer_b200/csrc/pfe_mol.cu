@@ -683,6 +683,13 @@ static int exclusive_sum(pfe_context* ctx, const int* in, int* out, int n, cudaS
 // (the pure-bra or bra-and-ket table when no shell of the bra or ket kind has a
 // target on a lower component) and the kept outputs of its largest group
 // quartet; warps per block chosen for the most resident warps per SM.
+// bit L: some shell of top angular momentum L has a coefficient on a lower component
+static int lower_kept_bits(const pfe_context* ctx) {
+  int bits = 0;
+  for (int L = 0; L < 3; ++L) bits |= ctx->lower_kept[L] ? (1 << L) : 0;
+  return bits;
+}
+
 static int size_wide(ClassLaunch& cl, const int kept_max[3], const bool lower_kept[3]) {
   cl.has_wide = false;
   const WideVariant wv = wide_variant(cl.cb, cl.ck);
@@ -913,6 +920,12 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
       cl.quartets = (double)nq;
       cl.has_straight = straight_launcher(cb, ck) != nullptr;
       cl.npass = cl.has_straight ? straight_npass(cb, ck) : 0;
+      cl.npass_live = 0;   // register passes actually launched (the rest keep no coefficient)
+      for (int p = 0; p < cl.npass; ++p)
+        cl.npass_live += (cl.npass == 1 || pass_live(kCL[cb][0], kCL[cb][1], kCL[ck][0], kCL[ck][1], cl.npass, p,
+                                                     lower_kept_bits(ctx)))
+                             ? 1
+                             : 0;
       cl.has_table = false;
       cl.variant = 0;
       cl.xg = nullptr;
@@ -997,6 +1010,7 @@ int molecular_setup(pfe_context* ctx, const pfe_args* a) {
 
 static MolLaunch make_launch(pfe_context* ctx, const double* d_dt) {
   MolLaunch ql{};
+  ql.lower_kept_bits = lower_kept_bits(ctx);
   ql.pairs = ctx->pairs;
   ql.rec = (const PairRec*)ctx->d_prec;
   ql.prim = ctx->shells.prim;
@@ -1272,6 +1286,14 @@ int batch_setup(pfe_batch* b) {
       if (!tmpl || total == 0) continue;
       if (total >= (1LL << 31)) { set_error("batch: too many chunks in one quartet class"); return PFE_EINVAL; }
       ClassLaunch cl = *tmpl;
+      {  // launched passes over the whole batch: a pass is skipped only if no instance needs it
+        int bits = 0;
+        for (pfe_context* c : b->inst) bits |= lower_kept_bits(c);
+        cl.npass_live = 0;
+        for (int p = 0; p < cl.npass; ++p)
+          cl.npass_live +=
+              (cl.npass == 1 || pass_live(kCL[cb][0], kCL[cb][1], kCL[ck][0], kCL[ck][1], cl.npass, p, bits)) ? 1 : 0;
+      }
       if (cl.has_wide) {   // the wide variant's working set must cover every instance
         int km[3] = {1, 1, 1};
         bool lk[3] = {false, false, false};
@@ -1451,6 +1473,7 @@ int batch_fock_pc(pfe_batch* b, const double* d_pc, double* d_cc, double* d_xc, 
   pfe_context* c0 = b->inst[0];
   MolLaunch lq = make_launch(c0, c0->d_pt);
   lq.insts = di;
+  for (pfe_context* c : b->inst) lq.lower_kept_bits |= lower_kept_bits(c);   // a pass is skipped only if dead everywhere
   for (int i = 0; i < b->nlaunch; ++i) {
     const ClassLaunch& cl = b->launches[i];
     launch_class(c0, cl, lq, cl.variant, s, b->mixed);
@@ -1490,6 +1513,7 @@ int batch_autotune(pfe_batch* b, const double* d_pc, cudaStream_t s) {
   pfe_context* c0 = b->inst[0];
   MolLaunch lq = make_launch(c0, c0->d_pt);
   lq.insts = static_cast<const MolLaunch*>(b->d_insts);
+  for (pfe_context* c : b->inst) lq.lower_kept_bits |= lower_kept_bits(c);
   cudaEvent_t e0, e1;
   PFE_CUDA(cudaEventCreate(&e0));
   PFE_CUDA(cudaEventCreate(&e1));

@@ -75,6 +75,7 @@ struct MolLaunch {
   int nt;
   int myid, numprocs;
   const MolLaunch* insts;   // batches: the launch record of every instance (chunk .w), else null
+  int lower_kept_bits;      // bit L: some shell of top L has a coefficient on a lower component
 };
 
 // The launch record of a set-up molecular context for target-space density d_dt.
@@ -155,39 +156,75 @@ __host__ __device__ constexpr int comp_tot(int L, int i) {
 // Bra component pairs ab = a*NB + b ordered by (|a|, |b|): the passes of a
 // class then keep the lower (for pure shells coefficient-free) components
 // together, and such passes skip their chunks.
+__host__ __device__ constexpr void ab_order_fill(int LA, int LB, int* ab, int* pos) {
+  const int NB = ncum(LB), N = ncum(LA) * NB;
+  for (int i = 0; i < N; ++i) ab[i] = i;
+  for (int i = 1; i < N; ++i)   // stable insertion sort by (|a|, |b|)
+    for (int j = i; j > 0; --j) {
+      const int x = ab[j - 1], y = ab[j];
+      const int kx = comp_tot(LA, x / NB) * 8 + comp_tot(LB, x % NB);
+      const int ky = comp_tot(LA, y / NB) * 8 + comp_tot(LB, y % NB);
+      if (kx <= ky) break;
+      ab[j - 1] = y;
+      ab[j] = x;
+    }
+  for (int i = 0; i < N; ++i) pos[ab[i]] = i;
+}
+
 template <int LA, int LB>
 struct AbOrder {
   static constexpr int NA = ncum(LA), NB = ncum(LB), N = NA * NB;
   int ab[N];    // k-th pair
   int pos[N];   // position of pair ab
-  __host__ __device__ constexpr AbOrder() : ab(), pos() {
-    for (int i = 0; i < N; ++i) ab[i] = i;
-    for (int i = 1; i < N; ++i)   // stable insertion sort by (|a|, |b|)
-      for (int j = i; j > 0; --j) {
-        const int x = ab[j - 1], y = ab[j];
-        const int kx = comp_tot(LA, x / NB) * 8 + comp_tot(LB, x % NB);
-        const int ky = comp_tot(LA, y / NB) * 8 + comp_tot(LB, y % NB);
-        if (kx <= ky) break;
-        ab[j - 1] = y;
-        ab[j] = x;
-      }
-    for (int i = 0; i < N; ++i) pos[ab[i]] = i;
-  }
+  __host__ __device__ constexpr AbOrder() : ab(), pos() { ab_order_fill(LA, LB, ab, pos); }
 };
 
 // Bra component pairs below the top level (|a| < LA or |b| < LB): in AbOrder
 // they come first.
+__host__ __device__ constexpr int lower_pairs(int LA, int LB) {
+  int c = 0;
+  for (int a = 0; a < ncum(LA); ++a)
+    for (int b = 0; b < ncum(LB); ++b)
+      if (comp_tot(LA, a) < LA || comp_tot(LB, b) < LB) ++c;
+  return c;
+}
+
 template <int LA, int LB>
 struct LowerPairs {
-  static constexpr int count() {
-    int c = 0;
-    for (int a = 0; a < ncum(LA); ++a)
-      for (int b = 0; b < ncum(LB); ++b)
-        if (comp_tot(LA, a) < LA || comp_tot(LB, b) < LB) ++c;
-    return c;
-  }
-  static constexpr int n = count();
+  static constexpr int n = lower_pairs(LA, LB);
 };
+
+// The bra component pairs [ab0, ab1) (positions in AbOrder) register pass `pass`
+// of `npass` keeps.  Two-pass (d s| classes split at the level boundary: the
+// lower components of the d shell first, the top-level ones second, so that a
+// pure d shell (lower components coefficient-free) skips the first pass entirely.
+__host__ __device__ constexpr void pass_range(int LA, int LB, int LC, int LD, int npass, int pass, int& ab0, int& ab1) {
+  const int NAB = ncum(LA) * ncum(LB), NCD = ncum(LC) * ncum(LD);
+  const int abp = (NAB + npass - 1) / npass;
+  const int nlow = lower_pairs(LA, LB);
+  const bool lsplit = npass == 2 && LA == 2 && LB == 0 && nlow * NCD <= 40 && (NAB - nlow) * NCD <= 40;
+  ab0 = lsplit ? (pass == 0 ? 0 : nlow) : pass * abp;
+  ab1 = lsplit ? (pass == 0 ? nlow : NAB) : ((ab0 + abp < NAB) ? ab0 + abp : NAB);
+}
+
+// Whether register pass `pass` keeps a bra component pair that can carry a
+// coefficient: a component below its shell's top level has none unless bit L of
+// lower_kept_bits is set (the kernel skips such chunks anyway; a pass that keeps
+// none of them is not launched at all).
+inline bool pass_live(int LA, int LB, int LC, int LD, int npass, int pass, int lower_kept_bits) {
+  int ab[MAXCOMP * MAXCOMP] = {}, pos[MAXCOMP * MAXCOMP] = {};
+  ab_order_fill(LA, LB, ab, pos);
+  int ab0 = 0, ab1 = 0;
+  pass_range(LA, LB, LC, LD, npass, pass, ab0, ab1);
+  const int NB = ncum(LB);
+  for (int k = ab0; k < ab1; ++k) {
+    const int a = ab[k] / NB, b = ab[k] % NB;
+    const bool ka = comp_tot(LA, a) == LA || ((lower_kept_bits >> LA) & 1);
+    const bool kb = comp_tot(LB, b) == LB || ((lower_kept_bits >> LB) & 1);
+    if (ka && kb) return true;
+  }
+  return false;
+}
 
 // resident blocks of 128 threads the register allocation aims at: 4 (at most
 // 128 registers) for the classes whose working set fits, else the compiler's choice
@@ -242,14 +279,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
   constexpr int NCD = NC * ND;
   constexpr int LT = LA + LB + LC + LD;
   constexpr AbOrder<LA, LB> ORD{};
-  constexpr int ABP = (NAB + NPASS - 1) / NPASS;
-  // two-pass (d s| classes split at the level boundary: the lower components of
-  // the d shell first, the top-level ones second, so that a pure d shell (lower
-  // components coefficient-free) skips the first pass entirely
-  constexpr int NLOW = LowerPairs<LA, LB>::n;
-  constexpr bool LSPLIT = NPASS == 2 && LA == 2 && LB == 0 && NLOW * NCD <= 40 && (NAB - NLOW) * NCD <= 40;
-  constexpr int AB0 = LSPLIT ? (PASS == 0 ? 0 : NLOW) : PASS * ABP;
-  constexpr int AB1 = LSPLIT ? (PASS == 0 ? NLOW : NAB) : ((AB0 + ABP < NAB) ? AB0 + ABP : NAB);
+  constexpr int AB0 = [] { int a = 0, b = 0; pass_range(LA, LB, LC, LD, NPASS, PASS, a, b); return a; }();
+  constexpr int AB1 = [] { int a = 0, b = 0; pass_range(LA, LB, LC, LD, NPASS, PASS, a, b); return b; }();
   constexpr int XN = (AB1 - AB0) * NCD;
   static_assert(AB0 < NAB, "every pass keeps at least one bra component pair");
   // the pass keeps the pairs ab at positions [AB0, AB1) of ORD; X(k, cd) is pair ORD.ab[AB0 + k]
@@ -530,6 +561,10 @@ using LaunchFn = void (*)(const MolLaunch&, int grid, cudaStream_t);
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 struct Passes {
   static void run(const MolLaunch& ql, int grid, cudaStream_t s) {
+    if (NPASS > 1 && !pass_live(LA, LB, LC, LD, NPASS, PASS, ql.lower_kept_bits)) {
+      if constexpr (PASS + 1 < NPASS) Passes<LA, LB, LC, LD, NPASS, PASS + 1, MIXED, BATCH>::run(ql, grid, s);
+      return;
+    }
     constexpr int LT = LA + LB + LC + LD;
     auto kern = k_gq<LA, LB, LC, LD, NPASS, PASS, MIXED, BATCH>;
     if constexpr (GqSmemBoys<LT>::use) {
