@@ -65,21 +65,29 @@ def test_learned_guess_saves_wall_time_on_large_clusters():
     experiment (polymer_b200/guess_eval.py): the batched SCF from the learned
     guess (data/guess_water_k8_32.pt; its features, network, assembly and
     purification inside the timed region) needs fewer iterations and less wall
-    time than from the nuclear-charge guess, with the same energies."""
+    time than from the nuclear-charge guess, with the same energies.  The
+    batch's set-up (pair lists and chunk lists of every molecule, the same for
+    both guesses and the noisiest part of a run at about a second) is done once
+    outside the timed runs; each guess is timed twice and its better run kept."""
     import time
     from polymer_b200 import batch_scf, guess_eval
     seeds = [sd for sd in guess_eval.heldout_seeds(200) if guess_eval.cluster_sizes([sd])[0] >= 16][:8]
     sizes = guess_eval.cluster_sizes(seeds)
     systems = [system.build_system(guess.sample_cluster(k, sd), fock.onee) for k, sd in zip(sizes, seeds)]
     lg = guess.LearnedGuess.load(guess_eval.MODEL)
+    fb = fock.DeviceBatch([systems[k] for k in batch_scf.sorted_order(systems)], 0)
     res, wall = {}, {}
     for name, opts in (('nuclear', batch_scf.BatchOptions()), ('learned', batch_scf.BatchOptions(guess=lg))):
-        batch_scf.run_batch_scf(systems, opts, device=0, graph=True)   # untimed: pools, lazy kernels
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res[name] = batch_scf.run_batch_scf(systems, opts, device=0, graph=True)
-        torch.cuda.synchronize()
-        wall[name] = time.perf_counter() - t0
+        batch_scf.run_batch_scf(systems, opts, device=0, graph=True, batch=fb)   # untimed: pools, lazy kernels
+        times = []
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res[name] = batch_scf.run_batch_scf(systems, opts, device=0, graph=True, batch=fb)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        wall[name] = min(times)
+    fb.close()
     print('k >= 16 batch: nuclear %.2f s (%.1f iterations), learned %.2f s (%.1f iterations)' % (
         wall['nuclear'], res['nuclear'].iterations.mean(), wall['learned'], res['learned'].iterations.mean()))
     assert res['learned'].converged.all() and not res['learned'].fallback.any()
