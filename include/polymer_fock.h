@@ -270,6 +270,14 @@ int32_t pfe_overlap_kinetic_noalloc(const pfe_onee_args *a, double *s_p, double 
 /* Library version string. */
 const char *pfe_version(void);
 
+/* Testing aid, no reference counterpart: the `after`-th device allocation that a
+ * context or batch set-up asks for from now on (0: the next one) fails as if the
+ * device were out of memory, so that callers can exercise their PFE_ENOMEM
+ * paths; the failing call returns PFE_ENOMEM and leaves its context or batch not
+ * set up (a later set-up starts afresh).  Negative `after`: no injection (the
+ * default).  Process-wide; nothing is attempted on the device. */
+int32_t pfe_debug_fail_allocation(int32_t after);
+
 #ifdef __cplusplus
 }
 #endif

@@ -165,6 +165,8 @@ def lib(path: str = LIB_PATH):
     L.pfe_measure_fp64_peak.restype = ctypes.c_int32
     L.pfe_version.argtypes = []
     L.pfe_version.restype = ctypes.c_char_p
+    L.pfe_debug_fail_allocation.argtypes = [ctypes.c_int32]
+    L.pfe_debug_fail_allocation.restype = ctypes.c_int32
     _vp, _i32, _i64, _f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
     for name, args in (('pfe_mlp_gemm', [_vp, _vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _vp]),
                        ('pfe_mlp_bias_act', [_vp, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
@@ -208,7 +210,7 @@ EXPORTS = ['pfe_fourindex_eri', 'pfe_last_error', 'pfe_context_create', 'pfe_con
            'pfe_context_primitive_targets', 'pfe_context_set_screening', 'pfe_batch_create', 'pfe_batch_setup',
            'pfe_batch_set_screening', 'pfe_batch_set_instance_screening', 'pfe_batch_offsets', 'pfe_batch_refresh',
            'pfe_batch_autotune', 'pfe_batch_schedule', 'pfe_batch_fock_pc', 'pfe_batch_census', 'pfe_batch_destroy',
-           'pfe_fourindex_eri_gradient']
+           'pfe_fourindex_eri_gradient', 'pfe_debug_fail_allocation']
 
 # Exported symbols declared in include/polymer_guess.h (checked by the CPU tests).
 GUESS_EXPORTS = ['pfe_mlp_gemm', 'pfe_mlp_bias_act', 'pfe_mlp_act_grad', 'pfe_mlp_colsum', 'pfe_mlp_mse',

@@ -454,6 +454,11 @@ extern "C" {
 
 const char* pfe_version(void) { return "polymer_fock 0.1 (sm_100a, cumulative s/p/d shells)"; }
 
+int32_t pfe_debug_fail_allocation(int32_t after) {
+  pfe::g_fail_alloc_after.store(after < 0 ? -1 : (long long)after);
+  return PFE_OK;
+}
+
 int32_t pfe_last_error(char* buf, int32_t len) {
   const char* m = last_error_cstr();
   const int32_t n = (int32_t)strlen(m);

@@ -1,6 +1,8 @@
 // Device-side state of one Fock-build context (struct pfe_context of the C ABI).
 #pragma once
 
+#include <atomic>
+
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 
@@ -10,6 +12,20 @@
 #include "pfe_common.cuh"
 
 namespace pfe {
+
+// Allocation-failure injection for tests of the error paths: the n-th device
+// allocation a context or batch asks for from now on fails as out of memory
+// (pfe_debug_fail_allocation); negative: never.  Nothing reaches the GPU: the
+// allocation is simply not attempted.
+inline std::atomic<long long> g_fail_alloc_after{-1};
+
+inline cudaError_t injected_alloc_failure() {
+  long long v = g_fail_alloc_after.load();
+  while (v >= 0)
+    if (g_fail_alloc_after.compare_exchange_weak(v, v - 1)) return v == 0 ? cudaErrorMemoryAllocation : cudaSuccess;
+  return cudaSuccess;
+}
+
 
 // Primitive-shell table, struct of arrays (n shells).
 struct DevShells {
@@ -176,6 +192,7 @@ struct pfe_context {
   std::vector<void*> pending;  // scratch freed at the end of setup
 
   cudaError_t alloc(void** p, size_t bytes) {
+    if (cudaError_t f = pfe::injected_alloc_failure()) return f;
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
     if (e == cudaSuccess) owned.push_back(*p);
     return e;
@@ -224,6 +241,7 @@ struct pfe_batch {
   bool ready = false;               // set by a pfe_batch_setup that succeeded
   std::vector<void*> owned;
   cudaError_t alloc(void** p, size_t bytes) {
+    if (cudaError_t f = pfe::injected_alloc_failure()) return f;
     cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
     if (e == cudaSuccess) owned.push_back(*p);
     return e;
