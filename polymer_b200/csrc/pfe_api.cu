@@ -480,6 +480,9 @@ int32_t pfe_context_create(int32_t device, pfe_context** out) {
   ctx->device = device;
   PFE_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
   PFE_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  PFE_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+  PFE_CUDA(cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+  PFE_CUDA(cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
   *out = ctx;   // the cuBLAS handle comes with the first call that needs it (ensure_blas)
   return PFE_OK;
 }
@@ -490,6 +493,12 @@ int32_t pfe_context_destroy(pfe_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   reset_context(ctx);
   if (ctx->blas) cublasDestroy(ctx->blas);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return PFE_OK;

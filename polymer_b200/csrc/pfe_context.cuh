@@ -100,6 +100,10 @@ struct pfe_context {
   int device = 0;
   int num_sms = 148;
   cudaStream_t stream = nullptr;
+  // the interpreter classes' launches run on `side`, beside the straight-line
+  // classes on the caller's stream (forked and joined with the two events)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cublasHandle_t blas = nullptr;
   bool ready = false;
   uint64_t key = 0;
