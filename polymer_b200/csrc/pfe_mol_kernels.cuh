@@ -262,15 +262,6 @@ struct GqBoysDirect {
 #endif
 };
 
-// Largest class (integrals per quartet) whose bra loop prefetches the next pair record.
-struct GqPrefetch {
-#ifdef PFE_GQ_PREFETCH
-  static constexpr int ni = PFE_GQ_PREFETCH;
-#else
-  static constexpr int ni = 0;
-#endif
-};
-
 template <int LA, int LB, int LC, int LD, int NPASS, int PASS, bool MIXED, bool BATCH>
 __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq(MolLaunch lq) {
   constexpr int NA = ncum(LA), NB = ncum(LB), NC = ncum(LC), ND = ncum(LD);
@@ -377,19 +368,8 @@ __global__ void __launch_bounds__(128, GqOccupancy<LA, LB, LC, LD>::blocks) k_gq
 #pragma unroll
           for (int d = 0; d < ND; ++d) ccd[cc * ND + d] = wKL * sK[cc] * sL[d];
       }
-      // classes with at most GqPrefetch::ni integrals load the next bra record while
-      // the current quartet is evaluated (its load latency leaves the chain)
-      constexpr bool PF = NI <= GqPrefetch::ni;
-      PairView nx;
-      if constexpr (PF) nx = load_pair(rec, g0);
       for (int p = g0; p < g0 + gn; ++p) {
-        PairView bp;
-        if constexpr (PF) {
-          bp = nx;
-          if (p + 1 < g0 + gn) nx = load_pair(rec, p + 1);
-        } else {
-          bp = load_pair(rec, p);
-        }
+        const PairView bp = load_pair(rec, p);
         const double sp = bp.bound;
         const bool pass = qok && sp * sq >= thr;
         if (!__any_sync(0xffffffffu, pass)) break;   // later bra pairs fail for every lane
